@@ -1,0 +1,208 @@
+/*
+ * qk_api.h -- C ABI of the B200 batch Monte Carlo pricing library
+ * (libqk_b200.so).
+ *
+ * Part 1 is a drop-in for the Monte Carlo subset of yluoc/Quant-Kernel's
+ * cpp/include/quantkernel/qk_api.h: the same names, argument order, types,
+ * return codes and NaN-per-bad-element behaviour.  Each declaration cites the
+ * reference declaration it replaces.  All pointers are host pointers; calls
+ * are synchronous and thread-safe (one CUDA stream and one error buffer per
+ * calling thread).  There is no CPU fallback: when CUDA is unusable the batch
+ * calls return QK_ERR_RUNTIME_INIT and the scalar calls return NaN, both with
+ * a message in qk_get_last_error().
+ *
+ * Part 2 (ABI 2.13) adds calls with no reference counterpart: price + standard
+ * error batches, a mixed-model batch, and device-resident "plans".
+ */
+#ifndef QK_API_H
+#define QK_API_H
+
+#include "qk_abi.h"
+
+#ifdef _WIN32
+#define QK_EXPORT __declspec(dllexport)
+#else
+#define QK_EXPORT __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ======================================================================= *
+ * Part 1 -- reference-compatible entry points
+ * ======================================================================= */
+
+/* qk_api.h:16 */
+QK_EXPORT void qk_abi_version(int32_t* major, int32_t* minor);
+/* qk_api.h:17-19 */
+QK_EXPORT int32_t qk_plugin_get_api(int32_t host_abi_major, int32_t host_abi_minor,
+                                    const QKPluginAPI** out_api);
+/* qk_api.h:20 */
+QK_EXPORT const char* qk_get_last_error(void);
+/* qk_api.h:21 */
+QK_EXPORT void qk_clear_last_error(void);
+
+/* qk_api.h:259-261 (estimate_terminal_antithetic, zero-vol forward branch) */
+QK_EXPORT double qk_mcm_standard_monte_carlo_price(double spot, double strike, double t, double vol,
+                                                   double r, double q, int32_t option_type,
+                                                   int32_t paths, uint64_t seed);
+/* qk_api.h:262-268 */
+QK_EXPORT int32_t qk_mcm_standard_monte_carlo_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices);
+
+/* qk_api.h:269-271 (estimate_stepwise + make_bsm_euler_step) */
+QK_EXPORT double qk_mcm_euler_maruyama_price(double spot, double strike, double t, double vol,
+                                             double r, double q, int32_t option_type,
+                                             int32_t paths, int32_t steps, uint64_t seed);
+/* qk_api.h:300-305 */
+QK_EXPORT int32_t qk_mcm_euler_maruyama_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices);
+
+/* qk_api.h:272-274 (estimate_stepwise + make_bsm_milstein_step) */
+QK_EXPORT double qk_mcm_milstein_price(double spot, double strike, double t, double vol, double r,
+                                       double q, int32_t option_type, int32_t paths,
+                                       int32_t steps, uint64_t seed);
+/* qk_api.h:306-311 */
+QK_EXPORT int32_t qk_mcm_milstein_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices);
+
+/* qk_api.h:294-296 (estimate_terminal_antithetic) */
+QK_EXPORT double qk_mcm_antithetic_variates_price(double spot, double strike, double t, double vol,
+                                                  double r, double q, int32_t option_type,
+                                                  int32_t paths, uint64_t seed);
+/* qk_api.h:347-352 */
+QK_EXPORT int32_t qk_mcm_antithetic_variates_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices);
+
+/* qk_api.h:359-364 (estimate_stepwise_2d + make_heston_euler_step) */
+QK_EXPORT double qk_mcm_heston_monte_carlo_price(double spot, double strike, double t, double r,
+                                                 double q, double v0, double kappa, double theta,
+                                                 double sigma, double rho, int32_t option_type,
+                                                 int32_t paths, int32_t steps, uint64_t seed);
+/* qk_api.h:365-374 */
+QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices);
+
+/* qk_api.h:393-396 (local_vol_price_impl, constant sigma) */
+QK_EXPORT double qk_mcm_local_vol_monte_carlo_price(double spot, double strike, double t,
+                                                    double vol, double r, double q,
+                                                    int32_t option_type, int32_t paths,
+                                                    int32_t steps, uint64_t seed);
+/* qk_api.h:397-403 */
+QK_EXPORT int32_t qk_mcm_local_vol_monte_carlo_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices);
+
+/* ======================================================================= *
+ * Part 2 -- additions in ABI 2.13 (no counterpart in the reference)
+ * ======================================================================= */
+
+/* Device selection for the calling thread (the library links its own CUDA
+ * runtime, so a host framework's current device is not seen here).  Every
+ * later call from this thread runs on `device`.  Returns QK_ERR_RUNTIME_INIT
+ * for a device that does not exist. */
+QK_EXPORT int32_t qk_set_device(int32_t device);
+QK_EXPORT int32_t qk_get_device(int32_t* device);
+
+/* Model codes for the mixed-model batch and for plans. */
+#define QK_MC_STANDARD       0 /* terminal GBM, antithetic pairs, zero-vol forward branch */
+#define QK_MC_ANTITHETIC     1 /* terminal GBM, antithetic pairs */
+#define QK_MC_EULER          2 /* BSM Euler-Maruyama */
+#define QK_MC_MILSTEIN       3 /* BSM Milstein */
+#define QK_MC_LOCAL_VOL      4 /* constant local-vol Euler */
+#define QK_MC_TERMINAL_PLAIN 5 /* terminal GBM, independent paths */
+#define QK_MC_HESTON         6 /* Heston full-truncation Euler */
+
+/* Plan flags. */
+#define QK_PLAN_PERSISTENT    0x1 /* one persistent work-stealing launch over all tiles */
+#define QK_PLAN_GRAPH         0x2 /* replay execute() from a captured CUDA graph */
+#define QK_PLAN_NO_ANTITHETIC 0x4 /* stepwise models: independent paths, not pairs */
+#define QK_PLAN_TIMING        0x8 /* record CUDA events around the simulate kernel */
+#define QK_PLAN_AUTOTUNE      0x10 /* choose block size / units per thread by timing */
+
+/* Price + standard error batches.  Same inputs as the Part 1 batch calls;
+ * out_stderr[i] is the standard error of out_prices[i] (NaN where no
+ * simulation ran: invalid input, t <= 1e-12, the zero-vol branch). */
+QK_EXPORT int32_t qk_mcm_standard_monte_carlo_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_antithetic_variates_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_euler_maruyama_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_milstein_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_local_vol_monte_carlo_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+
+/* Mixed-model batch: option i is priced with model[i] (QK_MC_*).  Fields a
+ * model does not use are ignored and may hold anything (vol for Heston;
+ * v0..rho for the BSM models; steps for the terminal models).  Runs as one
+ * persistent work-stealing launch.  out_stderr may be NULL. */
+QK_EXPORT int32_t qk_mcm_mixed_price_batch(
+    const int32_t* model, const double* spot, const double* strike, const double* t,
+    const double* vol, const double* r, const double* q, const double* v0, const double* kappa,
+    const double* theta, const double* sigma, const double* rho, const int32_t* option_type,
+    const int32_t* paths, const int32_t* steps, const uint64_t* seed, int32_t n,
+    double* out_prices, double* out_stderr);
+
+/* Plans: validate and upload a batch once, then run it many times with the
+ * inputs resident in GPU memory.  A plan belongs to the device that was
+ * current when it was created.  execute() is asynchronous on `stream` (a
+ * cudaStream_t; NULL = the plan's own stream); results() synchronises that
+ * stream and copies prices (and standard errors, if out_stderr != NULL) to
+ * host memory.  Plans are not thread-safe: one thread per plan at a time. */
+typedef struct qk_mc_plan qk_mc_plan;
+
+QK_EXPORT int32_t qk_mcm_plan_create(
+    const int32_t* model, const double* spot, const double* strike, const double* t,
+    const double* vol, const double* r, const double* q, const double* v0, const double* kappa,
+    const double* theta, const double* sigma, const double* rho, const int32_t* option_type,
+    const int32_t* paths, const int32_t* steps, const uint64_t* seed, int32_t n, int32_t flags,
+    qk_mc_plan** out_plan);
+QK_EXPORT int32_t qk_mcm_plan_execute(qk_mc_plan* plan, void* stream);
+QK_EXPORT int32_t qk_mcm_plan_results(qk_mc_plan* plan, double* out_prices, double* out_stderr);
+/* Device pointers to the plan's result arrays (n doubles each). */
+QK_EXPORT int32_t qk_mcm_plan_device_results(qk_mc_plan* plan, double** d_prices,
+                                             double** d_stderr);
+/* Milliseconds of the last execute()'s simulate kernel (QK_PLAN_TIMING), and
+ * the number of kernels one execute() launches. */
+QK_EXPORT int32_t qk_mcm_plan_stats(qk_mc_plan* plan, double* simulate_ms, int32_t* launches,
+                                    int64_t* path_steps);
+/* The launch shape in use: block size, units per thread, persistent CTAs. */
+QK_EXPORT int32_t qk_mcm_plan_config(qk_mc_plan* plan, int32_t* block, int32_t* units_per_thread,
+                                     int32_t* ctas);
+QK_EXPORT int32_t qk_mcm_plan_destroy(qk_mc_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QK_API_H */

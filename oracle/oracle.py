@@ -1,0 +1,232 @@
+"""ctypes binding of the CPU oracle (libqk_oracle.so) and of the reference
+library compiled from its own sources (oracle/_ref/libquantkernel.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, always as the checker or the timed CPU baseline,
+never as a product path.
+"""
+
+import ctypes as ct
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "libqk_oracle.so"
+REF_SO = HERE / "_ref" / "libquantkernel.so"
+
+D = ct.c_double
+I32 = ct.c_int32
+U32 = ct.c_uint32
+U64 = ct.c_uint64
+PD = ct.POINTER(D)
+PI32 = ct.POINTER(I32)
+PU64 = ct.POINTER(U64)
+PU32 = ct.POINTER(U32)
+
+# Model codes shared with the GPU library (QK_MC_* in include/qk_api.h).
+STANDARD, ANTITHETIC, EULER, MILSTEIN, LOCAL_VOL, TERMINAL_PLAIN, HESTON = range(7)
+
+
+def _pd(a):
+    return a.ctypes.data_as(PD)
+
+
+class Oracle:
+    """The C restatement: bit-exact reference pricers + SE, closed forms, Philox replay."""
+
+    def __init__(self, path: Path = ORACLE_SO):
+        if not path.exists():
+            raise OSError(f"{path} missing; run `make -C oracle`")
+        lib = ct.CDLL(str(path))
+        term = [D, D, D, D, D, D, I32, I32, U64, PD]
+        step = [D, D, D, D, D, D, I32, I32, I32, U64, PD]
+        sig = {
+            "qko_standard_mc": (D, term), "qko_antithetic": (D, term),
+            "qko_terminal_plain": (D, term), "qko_euler": (D, step),
+            "qko_milstein": (D, step), "qko_local_vol": (D, step),
+            "qko_heston": (D, [D] * 10 + [I32, I32, I32, U64, PD]),
+            "qko_heston_batch": (None, [PD] * 10 + [PI32, PI32, PI32, PU64, I32, PD, PD]),
+            "qko_bsm_family_batch": (None, [I32] + [PD] * 6 + [PI32, PI32, PI32, PU64, I32, PD, PD]),
+            "qko_bsm_price": (D, [D] * 6 + [I32]),
+            "qko_heston_cf_price": (D, [D] * 10 + [I32, I32, D]),
+            "qko_normals": (None, [U64, I32, PD]),
+            "qko_philox4x32_10": (None, [PU32, PU32, PU32]),
+            "qko_philox_normals4": (None, [U64, U32, U32, U32, PD]),
+            "qko_philox_price": (D, [I32] + [D] * 11 + [I32, I32, I32, U64, I32, PD]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        self.lib = lib
+
+    # -- reference pricers (bit-exact) -------------------------------------------
+    def price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps, seed,
+              v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0):
+        se = D()
+        L = self.lib
+        if model == STANDARD:
+            p = L.qko_standard_mc(spot, strike, t, vol, r, q, option_type, paths, seed, ct.byref(se))
+        elif model == ANTITHETIC:
+            p = L.qko_antithetic(spot, strike, t, vol, r, q, option_type, paths, seed, ct.byref(se))
+        elif model == TERMINAL_PLAIN:
+            p = L.qko_terminal_plain(spot, strike, t, vol, r, q, option_type, paths, seed, ct.byref(se))
+        elif model == EULER:
+            p = L.qko_euler(spot, strike, t, vol, r, q, option_type, paths, steps, seed, ct.byref(se))
+        elif model == MILSTEIN:
+            p = L.qko_milstein(spot, strike, t, vol, r, q, option_type, paths, steps, seed, ct.byref(se))
+        elif model == LOCAL_VOL:
+            p = L.qko_local_vol(spot, strike, t, vol, r, q, option_type, paths, steps, seed, ct.byref(se))
+        elif model == HESTON:
+            p = L.qko_heston(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                             paths, steps, seed, ct.byref(se))
+        else:
+            raise ValueError(model)
+        return p, se.value
+
+    def heston_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                     paths, steps, seed):
+        a = [np.ascontiguousarray(x, np.float64) for x in (spot, strike, t, r, q, v0, kappa, theta, sigma, rho)]
+        ot = np.ascontiguousarray(option_type, np.int32)
+        pp = np.ascontiguousarray(paths, np.int32)
+        st = np.ascontiguousarray(steps, np.int32)
+        sd = np.ascontiguousarray(seed, np.uint64)
+        n = a[0].shape[0]
+        out = np.empty(n)
+        se = np.empty(n)
+        self.lib.qko_heston_batch(*[_pd(x) for x in a], ot.ctypes.data_as(PI32), pp.ctypes.data_as(PI32),
+                                  st.ctypes.data_as(PI32), sd.ctypes.data_as(PU64), n, _pd(out), _pd(se))
+        return out, se
+
+    def bsm_family_batch(self, model, spot, strike, t, vol, r, q, option_type, paths, steps, seed):
+        a = [np.ascontiguousarray(x, np.float64) for x in (spot, strike, t, vol, r, q)]
+        ot = np.ascontiguousarray(option_type, np.int32)
+        pp = np.ascontiguousarray(paths, np.int32)
+        st = np.ascontiguousarray(steps if steps is not None else np.ones(len(pp)), np.int32)
+        sd = np.ascontiguousarray(seed, np.uint64)
+        n = a[0].shape[0]
+        out = np.empty(n)
+        se = np.empty(n)
+        self.lib.qko_bsm_family_batch(int(model), *[_pd(x) for x in a], ot.ctypes.data_as(PI32),
+                                      pp.ctypes.data_as(PI32), st.ctypes.data_as(PI32),
+                                      sd.ctypes.data_as(PU64), n, _pd(out), _pd(se))
+        return out, se
+
+    # -- closed forms -------------------------------------------------------------
+    def bsm(self, spot, strike, t, vol, r, q, option_type):
+        return self.lib.qko_bsm_price(spot, strike, t, vol, r, q, option_type)
+
+    def heston_cf(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                  integration_steps=1024, integration_limit=120.0):
+        return self.lib.qko_heston_cf_price(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                            option_type, integration_steps, integration_limit)
+
+    # -- streams ------------------------------------------------------------------
+    def normals(self, seed, n):
+        out = np.empty(n)
+        self.lib.qko_normals(seed, n, _pd(out))
+        return out
+
+    def philox(self, ctr, key):
+        c = (U32 * 4)(*ctr)
+        k = (U32 * 2)(*key)
+        o = (U32 * 4)()
+        self.lib.qko_philox4x32_10(c, k, o)
+        return list(o)
+
+    def philox_normals4(self, seed, c0, c1, c3):
+        z = np.empty(4)
+        self.lib.qko_philox_normals4(seed, c0, c1, c3, _pd(z))
+        return z
+
+    def philox_price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps, seed,
+                     v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0, antithetic=True):
+        se = D()
+        p = self.lib.qko_philox_price(model, spot, strike, t, vol, r, q, v0, kappa, theta, sigma,
+                                      rho, option_type, paths, steps, seed, 1 if antithetic else 0,
+                                      ct.byref(se))
+        return p, se.value
+
+
+class Reference:
+    """The reference library (compiled from its sources by `make -C oracle ref`)."""
+
+    def __init__(self, path: Path = REF_SO):
+        if not path.exists():
+            raise OSError(f"{path} missing; run `make -C oracle ref` where the reference is present")
+        lib = ct.CDLL(str(path))
+        term = [D, D, D, D, D, D, I32, I32, U64]
+        step = [D, D, D, D, D, D, I32, I32, I32, U64]
+        sig = {
+            "qk_mcm_standard_monte_carlo_price": (D, term),
+            "qk_mcm_antithetic_variates_price": (D, term),
+            "qk_mcm_euler_maruyama_price": (D, step),
+            "qk_mcm_milstein_price": (D, step),
+            "qk_mcm_local_vol_monte_carlo_price": (D, step),
+            "qk_mcm_heston_monte_carlo_price": (D, [D] * 10 + [I32, I32, I32, U64]),
+            "qk_mcm_heston_monte_carlo_price_batch": (I32, [PD] * 10 + [PI32, PI32, PI32, PU64, I32, PD]),
+            "qk_mcm_standard_monte_carlo_price_batch": (I32, [PD] * 6 + [PI32, PI32, PU64, I32, PD]),
+            "qk_mcm_euler_maruyama_price_batch": (I32, [PD] * 6 + [PI32, PI32, PI32, PU64, I32, PD]),
+            "qk_cf_black_scholes_merton_price": (D, [D] * 6 + [I32]),
+            "qk_cf_heston_price_cf": (D, [D] * 10 + [I32, I32, D]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        self.lib = lib
+
+    def price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps, seed,
+              v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0):
+        L = self.lib
+        if model == STANDARD:
+            return L.qk_mcm_standard_monte_carlo_price(spot, strike, t, vol, r, q, option_type, paths, seed)
+        if model == ANTITHETIC:
+            return L.qk_mcm_antithetic_variates_price(spot, strike, t, vol, r, q, option_type, paths, seed)
+        if model == EULER:
+            return L.qk_mcm_euler_maruyama_price(spot, strike, t, vol, r, q, option_type, paths, steps, seed)
+        if model == MILSTEIN:
+            return L.qk_mcm_milstein_price(spot, strike, t, vol, r, q, option_type, paths, steps, seed)
+        if model == LOCAL_VOL:
+            return L.qk_mcm_local_vol_monte_carlo_price(spot, strike, t, vol, r, q, option_type, paths, steps, seed)
+        if model == HESTON:
+            return L.qk_mcm_heston_monte_carlo_price(spot, strike, t, r, q, v0, kappa, theta, sigma,
+                                                     rho, option_type, paths, steps, seed)
+        raise ValueError(model)
+
+    def heston_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                     paths, steps, seed):
+        a = [np.ascontiguousarray(x, np.float64) for x in (spot, strike, t, r, q, v0, kappa, theta, sigma, rho)]
+        ot = np.ascontiguousarray(option_type, np.int32)
+        pp = np.ascontiguousarray(paths, np.int32)
+        st = np.ascontiguousarray(steps, np.int32)
+        sd = np.ascontiguousarray(seed, np.uint64)
+        n = a[0].shape[0]
+        out = np.empty(n)
+        rc = self.lib.qk_mcm_heston_monte_carlo_price_batch(
+            *[_pd(x) for x in a], ot.ctypes.data_as(PI32), pp.ctypes.data_as(PI32),
+            st.ctypes.data_as(PI32), sd.ctypes.data_as(PU64), n, _pd(out))
+        if rc != 0:
+            raise RuntimeError(f"reference batch rc={rc}")
+        return out
+
+    def bsm(self, spot, strike, t, vol, r, q, option_type):
+        return self.lib.qk_cf_black_scholes_merton_price(spot, strike, t, vol, r, q, option_type)
+
+    def heston_cf(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                  integration_steps=1024, integration_limit=120.0):
+        return self.lib.qk_cf_heston_price_cf(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                              option_type, integration_steps, integration_limit)
+
+
+def reference_available() -> bool:
+    return REF_SO.exists()
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1

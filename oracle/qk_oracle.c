@@ -1,0 +1,678 @@
+/*
+ * qk_oracle.c -- CPU oracle for the batch Monte Carlo pricing path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see qk_oracle.h).  Compiled with
+ * -ffp-contract=off so that every expression rounds exactly as written, the
+ * way the reference's x86-64 build (no FMA) evaluates it.
+ *
+ * Citations are into yluoc/Quant-Kernel.
+ */
+#include "qk_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stddef.h>
+#include <string.h>
+
+#define QKO_CALL 0
+#define QKO_PUT 1
+#define QKO_EPS 1e-12 /* monte_carlo_methods/common/internal_util.h:13 */
+
+static double qko_nan(void) {
+    /* math_util.h:12-16 writes the quiet NaN bit pattern 0x7FF8000000000000. */
+    uint64_t bits = UINT64_C(0x7FF8000000000000);
+    double out;
+    memcpy(&out, &bits, sizeof out);
+    return out;
+}
+
+static int qko_finite(double x) {
+    /* math_util.h:18-23: finite iff the exponent field is not all ones. */
+    uint64_t bits;
+    memcpy(&bits, &x, sizeof bits);
+    return (bits & UINT64_C(0x7FF0000000000000)) != UINT64_C(0x7FF0000000000000);
+}
+
+/* std::max(a, b) is (a < b) ? b : a.  The reference's NaN behaviour follows
+ * from this exact form, so the oracle keeps it rather than fmax(). */
+static double smax(double a, double b) { return (a < b) ? b : a; }
+
+/* option_util.h:33-38: payoff, NaN for an unknown option type. */
+static double intrinsic(double x, double y, int32_t option_type) {
+    if (option_type == QKO_CALL) return smax(0.0, x - y);
+    if (option_type == QKO_PUT) return smax(0.0, y - x);
+    return qko_nan();
+}
+
+static int valid_option_type(int32_t ot) { return ot == QKO_CALL || ot == QKO_PUT; }
+
+/* option_util.h:42-50. */
+static int valid_common_inputs(double spot, double strike, double t, double vol, double r,
+                               double q, int32_t ot) {
+    if (!valid_option_type(ot)) return 0;
+    if (!qko_finite(spot) || !qko_finite(strike) || !qko_finite(t) || !qko_finite(vol) ||
+        !qko_finite(r) || !qko_finite(q))
+        return 0;
+    return spot > 0.0 && strike > 0.0 && t >= 0.0 && vol >= 0.0;
+}
+
+/* monte_carlo_methods/common/internal_util.h:24-26. */
+static int valid_mc_counts(int32_t paths, int32_t steps) { return paths > 1 && steps > 0; }
+
+/* ===================================================================== *
+ * MT19937-64 (Matsumoto & Nishimura, "Mersenne Twister 64-bit", 2000),
+ * with the parameters that the C++ standard fixes for std::mt19937_64.
+ * ===================================================================== */
+#define MT_N 312
+#define MT_M 156
+#define MT_UPPER UINT64_C(0xFFFFFFFF80000000)
+#define MT_LOWER UINT64_C(0x000000007FFFFFFF)
+
+static void mt_seed(qko_normal_gen* g, uint64_t seed) {
+    g->mt[0] = seed;
+    for (int i = 1; i < MT_N; ++i) {
+        uint64_t prev = g->mt[i - 1];
+        g->mt[i] = UINT64_C(6364136223846793005) * (prev ^ (prev >> 62)) + (uint64_t)i;
+    }
+    g->idx = MT_N;
+}
+
+static void mt_twist(qko_normal_gen* g) {
+    for (int k = 0; k < MT_N; ++k) {
+        uint64_t x = (g->mt[k] & MT_UPPER) | (g->mt[(k + 1) % MT_N] & MT_LOWER);
+        uint64_t xa = x >> 1;
+        if (x & 1u) xa ^= UINT64_C(0xB5026F5AA96619E9);
+        g->mt[k] = g->mt[(k + MT_M) % MT_N] ^ xa;
+    }
+    g->idx = 0;
+}
+
+uint64_t qko_mt64_next(qko_normal_gen* g) {
+    if (g->idx >= MT_N) mt_twist(g);
+    uint64_t y = g->mt[g->idx++];
+    y ^= (y >> 29) & UINT64_C(0x5555555555555555);
+    y ^= (y << 17) & UINT64_C(0x71D67FFFEDA60000);
+    y ^= (y << 37) & UINT64_C(0xFFF7EEE000000000);
+    y ^= y >> 43;
+    return y;
+}
+
+void qko_gen_init(qko_normal_gen* g, uint64_t seed) {
+    /* mc_engine.h:15-23: one engine + one normal_distribution per option. */
+    mt_seed(g, seed);
+    g->has_saved = 0;
+    g->saved = 0.0;
+}
+
+/* libstdc++ (GCC 13) generate_canonical<double, 53> over a 64-bit engine:
+ * one draw, double(x) / 2^64, and a result that rounds up to 1 replaced by
+ * the largest double below 1. */
+double qko_gen_canonical(qko_normal_gen* g) {
+    double u = (double)qko_mt64_next(g) / 18446744073709551616.0;
+    if (u >= 1.0) u = nextafter(1.0, 0.0);
+    return u;
+}
+
+/* libstdc++ normal_distribution<double>: Marsaglia's polar method.  Each
+ * accepted (x, y) yields y * m now and caches x * m for the next call. */
+double qko_gen_normal(qko_normal_gen* g) {
+    if (g->has_saved) {
+        g->has_saved = 0;
+        return g->saved * 1.0 + 0.0;
+    }
+    double x, y, r2;
+    do {
+        x = 2.0 * qko_gen_canonical(g) - 1.0;
+        y = 2.0 * qko_gen_canonical(g) - 1.0;
+        r2 = x * x + y * y;
+    } while (r2 > 1.0 || r2 == 0.0);
+    const double mult = sqrt(-2.0 * log(r2) / r2);
+    g->saved = x * mult;
+    g->has_saved = 1;
+    return (y * mult) * 1.0 + 0.0;
+}
+
+void qko_normals(uint64_t seed, int32_t n, double* out) {
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    for (int32_t i = 0; i < n; ++i) out[i] = qko_gen_normal(&g);
+}
+
+/* ===================================================================== *
+ * Running moments for the standard error.  The price sums stay plain
+ * double additions in the reference's order (bit-exactness); the squared
+ * sums only feed the standard error.
+ * ===================================================================== */
+static double se_from_moments(double disc, double sum, double sumsq, double n) {
+    if (!(n >= 2.0)) return qko_nan();
+    double mean = sum / n;
+    double var = (sumsq - n * mean * mean) / (n - 1.0);
+    if (var < 0.0) var = 0.0;
+    return disc * sqrt(var / n);
+}
+
+/* model_concepts.h:93-102 make_bsm_terminal. */
+static double bsm_terminal(double vol, double r, double q, double spot, double t, double z) {
+    double drift = (r - q - 0.5 * vol * vol) * t;
+    double diffusion = vol * sqrt(smax(t, 0.0)) * z;
+    return spot * exp(drift + diffusion);
+}
+
+/* mc_engine.h:32-53 estimate_terminal_antithetic with the payoff accumulator.
+ * Standard error over the n/2 pair means (the lone odd path is left out of
+ * the variance, it is in the mean). */
+static double est_terminal_antithetic(double spot, double strike, double t, double vol, double r,
+                                      double q, int32_t ot, int32_t n_paths, uint64_t seed,
+                                      double disc, double* se) {
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    double sum = 0.0, psum = 0.0, psq = 0.0;
+    const int32_t n_pairs = n_paths / 2;
+    for (int32_t i = 0; i < n_pairs; ++i) {
+        const double z = qko_gen_normal(&g);
+        const double st_up = bsm_terminal(vol, r, q, spot, t, z);
+        const double st_dn = bsm_terminal(vol, r, q, spot, t, -z);
+        const double a = intrinsic(st_up, strike, ot);
+        const double b = intrinsic(st_dn, strike, ot);
+        sum += a;
+        sum += b;
+        const double m = 0.5 * (a + b);
+        psum += m;
+        psq += m * m;
+    }
+    if ((n_paths & 1) != 0) {
+        const double z = qko_gen_normal(&g);
+        const double st = bsm_terminal(vol, r, q, spot, t, z);
+        sum += intrinsic(st, strike, ot);
+    }
+    const double mean = sum / (double)n_paths;
+    if (se) *se = se_from_moments(disc, psum, psq, (double)n_pairs);
+    return disc * mean;
+}
+
+/* standard_monte_carlo.cpp:11-33. */
+double qko_standard_mc(double spot, double strike, double t, double vol, double r, double q,
+                       int32_t ot, int32_t paths, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 1) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    if (vol <= QKO_EPS) {
+        const double fwd = spot * exp((r - q) * t);
+        return exp(-r * t) * intrinsic(fwd, strike, ot);
+    }
+    const double disc = exp(-r * t);
+    return est_terminal_antithetic(spot, strike, t, vol, r, q, ot, paths, seed, disc, se);
+}
+
+/* antithetic_variates.cpp:11-29 (no zero-vol branch). */
+double qko_antithetic(double spot, double strike, double t, double vol, double r, double q,
+                      int32_t ot, int32_t paths, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 1) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    return est_terminal_antithetic(spot, strike, t, vol, r, q, ot, paths, seed, disc, se);
+}
+
+/* mc_engine.h:62-75 estimate_terminal (the plain loop; the reference runs it
+ * under importance sampling, here with the BSM terminal model and payoff). */
+double qko_terminal_plain(double spot, double strike, double t, double vol, double r, double q,
+                          int32_t ot, int32_t paths, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 1) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    double sum = 0.0, sq = 0.0;
+    for (int32_t i = 0; i < paths; ++i) {
+        const double z = qko_gen_normal(&g);
+        const double p = intrinsic(bsm_terminal(vol, r, q, spot, t, z), strike, ot);
+        sum += p;
+        sq += p * p;
+    }
+    if (se) *se = se_from_moments(disc, sum, sq, (double)paths);
+    return disc * (sum / (double)paths);
+}
+
+/* mc_engine.h:84-103 estimate_stepwise with
+ *   kind 0: make_bsm_euler_step    (model_concepts.h:136-143)
+ *   kind 1: make_bsm_milstein_step (model_concepts.h:150-158) */
+static double est_stepwise(int kind, double spot, double strike, double t, double vol,
+                           double drift, int32_t ot, int32_t n_paths, int32_t steps,
+                           uint64_t seed, double disc, double* se) {
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    const double dt = t / (double)steps;
+    const double sqrt_dt = sqrt(dt);
+    double sum = 0.0, sq = 0.0;
+    for (int32_t i = 0; i < n_paths; ++i) {
+        double s = spot;
+        for (int32_t j = 0; j < steps; ++j) {
+            double dw = sqrt_dt * qko_gen_normal(&g);
+            if (kind == 0)
+                s = smax(1e-12, s + drift * s * dt + vol * s * dw);
+            else
+                s = smax(1e-12, s + drift * s * dt + vol * s * dw +
+                                    0.5 * vol * vol * s * (dw * dw - dt));
+        }
+        const double p = intrinsic(s, strike, ot);
+        sum += p;
+        sq += p * p;
+    }
+    if (se) *se = se_from_moments(disc, sum, sq, (double)n_paths);
+    return disc * (sum / (double)n_paths);
+}
+
+/* euler_maruyama.cpp:11-28. */
+double qko_euler(double spot, double strike, double t, double vol, double r, double q,
+                 int32_t ot, int32_t paths, int32_t steps, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || !valid_mc_counts(paths, steps))
+        return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    return est_stepwise(0, spot, strike, t, vol, r - q, ot, paths, steps, seed, disc, se);
+}
+
+/* milstein.cpp:11-28. */
+double qko_milstein(double spot, double strike, double t, double vol, double r, double q,
+                    int32_t ot, int32_t paths, int32_t steps, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || !valid_mc_counts(paths, steps))
+        return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    return est_stepwise(1, spot, strike, t, vol, r - q, ot, paths, steps, seed, disc, se);
+}
+
+/* local_vol_monte_carlo.cpp:20-48 (local_vol_price_impl) with the constant
+ * sigma_fn of model_concepts.h:240-266 and the entry checks of :57-73.  The
+ * reference discounts as disc * sum / paths here, not disc * (sum / paths). */
+double qko_local_vol(double spot, double strike, double t, double vol, double r, double q,
+                     int32_t ot, int32_t paths, int32_t steps, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || !valid_mc_counts(paths, steps))
+        return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    const double dt = t / (double)steps;
+    const double sqrt_dt = sqrt(dt);
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    double sum = 0.0, sq = 0.0;
+    for (int32_t i = 0; i < paths; ++i) {
+        double s = spot;
+        double current_t = 0.0;
+        for (int32_t j = 0; j < steps; ++j) {
+            const double dw = sqrt_dt * qko_gen_normal(&g);
+            const double sig = vol; /* sigma_fn(s, current_t) */
+            s = smax(1e-12, s + (r - q) * s * dt + sig * s * dw);
+            current_t += dt;
+        }
+        (void)current_t;
+        const double p = intrinsic(s, strike, ot);
+        sum += p;
+        sq += p * p;
+    }
+    if (se) *se = se_from_moments(disc, sum, sq, (double)paths);
+    return disc * sum / (double)paths;
+}
+
+/* heston_monte_carlo.cpp:11-36 driving mc_engine.h:113-136
+ * estimate_stepwise_2d with make_heston_euler_step (model_concepts.h:205-226). */
+double qko_heston(double spot, double strike, double t, double r, double q, double v0,
+                  double kappa, double theta, double sigma, double rho, int32_t ot,
+                  int32_t paths, int32_t steps, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
+        kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||
+        !valid_mc_counts(paths, steps))
+        return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    const double rho_comp = sqrt(smax(1.0 - rho * rho, 0.0));
+    const double dt = t / (double)steps;
+    const double sqrt_dt = sqrt(dt);
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    double sum = 0.0, sq = 0.0;
+    for (int32_t i = 0; i < paths; ++i) {
+        double s = spot;
+        double v = v0;
+        for (int32_t j = 0; j < steps; ++j) {
+            const double z1 = qko_gen_normal(&g);
+            const double z2 = qko_gen_normal(&g);
+            const double v_pos = smax(v, 0.0);
+            const double sqrt_v = sqrt(v_pos);
+            const double dw1 = sqrt_dt * z1;
+            const double dw2 = sqrt_dt * (rho * z1 + rho_comp * z2);
+            const double s_next = s * exp((r - q - 0.5 * v_pos) * dt + sqrt_v * dw1);
+            const double v_next = smax(0.0, v + kappa * (theta - v_pos) * dt + sigma * sqrt_v * dw2);
+            s = smax(s_next, 1e-12);
+            v = v_next;
+        }
+        const double p = intrinsic(s, strike, ot);
+        sum += p;
+        sq += p * p;
+    }
+    if (se) *se = se_from_moments(disc, sum, sq, (double)paths);
+    return disc * (sum / (double)paths);
+}
+
+void qko_heston_batch(const double* spot, const double* strike, const double* t,
+                      const double* r, const double* q, const double* v0, const double* kappa,
+                      const double* theta, const double* sigma, const double* rho,
+                      const int32_t* ot, const int32_t* paths, const int32_t* steps,
+                      const uint64_t* seed, int32_t n, double* out, double* out_se) {
+#pragma omp parallel for schedule(dynamic)
+    for (int32_t i = 0; i < n; ++i) {
+        double se;
+        out[i] = qko_heston(spot[i], strike[i], t[i], r[i], q[i], v0[i], kappa[i], theta[i],
+                            sigma[i], rho[i], ot[i], paths[i], steps[i], seed[i], &se);
+        if (out_se) out_se[i] = se;
+    }
+}
+
+void qko_bsm_family_batch(int32_t model, const double* spot, const double* strike,
+                          const double* t, const double* vol, const double* r, const double* q,
+                          const int32_t* ot, const int32_t* paths, const int32_t* steps,
+                          const uint64_t* seed, int32_t n, double* out, double* out_se) {
+#pragma omp parallel for schedule(dynamic)
+    for (int32_t i = 0; i < n; ++i) {
+        double se = qko_nan(), p;
+        const int32_t st = steps ? steps[i] : 1;
+        switch (model) {
+            case 0: p = qko_standard_mc(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], seed[i], &se); break;
+            case 1: p = qko_antithetic(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], seed[i], &se); break;
+            case 2: p = qko_euler(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], st, seed[i], &se); break;
+            case 3: p = qko_milstein(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], st, seed[i], &se); break;
+            case 4: p = qko_local_vol(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], st, seed[i], &se); break;
+            case 5: p = qko_terminal_plain(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], seed[i], &se); break;
+            default: p = qko_nan(); break;
+        }
+        out[i] = p;
+        if (out_se) out_se[i] = se;
+    }
+}
+
+/* ===================================================================== *
+ * 2. Closed forms.
+ * ===================================================================== */
+
+static double norm_cdf_exact(double x) { return 0.5 * erfc(-x / sqrt(2.0)); }
+
+/* black_scholes_merton.cpp:7-33 with an erfc-based normal CDF (the
+ * reference uses the A&S 7.1.26 approximation, max error ~1.5e-7). */
+double qko_bsm_price(double spot, double strike, double t, double vol, double r, double q,
+                     int32_t ot) {
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot)) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    if (vol <= QKO_EPS) {
+        double fwd = spot * exp((r - q) * t);
+        return exp(-r * t) * intrinsic(fwd, strike, ot);
+    }
+    double sqrt_t = sqrt(t);
+    double d1 = (log(spot / strike) + (r - q + 0.5 * vol * vol) * t) / (vol * sqrt_t);
+    double d2 = d1 - vol * sqrt_t;
+    double df = exp(-r * t), qf = exp(-q * t);
+    if (ot == QKO_CALL) return spot * qf * norm_cdf_exact(d1) - strike * df * norm_cdf_exact(d2);
+    return strike * df * norm_cdf_exact(-d2) - spot * qf * norm_cdf_exact(-d1);
+}
+
+/* 64-point Gauss-Legendre rule on [-1, 1]: the 32 positive nodes and their
+ * weights, computed once by Newton's method on the Legendre recurrence. */
+static double gl_x[32], gl_w[32];
+static int gl_ready = 0;
+
+static void gl_init(void) {
+    if (gl_ready) return;
+    const int n = 64;
+    for (int i = 0; i < 32; ++i) {
+        /* Tricomi's initial guess for root i (descending from 1). */
+        double x = cos(M_PI * (i + 0.75) / (n + 0.5));
+        double dp = 0.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = x;
+            for (int k = 2; k <= n; ++k) {
+                double pk = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+                p0 = p1;
+                p1 = pk;
+            }
+            dp = n * (x * p1 - p0) / (x * x - 1.0);
+            double dx = p1 / dp;
+            x -= dx;
+            if (fabs(dx) < 1e-16) break;
+        }
+        /* store ascending: index 31 - i */
+        gl_x[31 - i] = x;
+        gl_w[31 - i] = 2.0 / ((1.0 - x * x) * dp * dp);
+    }
+    gl_ready = 1;
+}
+
+/* heston.cpp:7-53 (little-trap characteristic function) with the P1/P2
+ * integration of closed_form_semi_analytical/common/internal_util.h:80-142:
+ * ceil(steps/64) panels of the 64-point rule on [1e-8, limit]. */
+double qko_heston_cf_price(double spot, double strike, double t, double r, double q, double v0,
+                           double kappa, double theta, double sigma, double rho, int32_t ot,
+                           int32_t integration_steps, double integration_limit) {
+    if (!valid_option_type(ot)) return qko_nan();
+    if (!qko_finite(spot) || !qko_finite(strike) || !qko_finite(t) || !qko_finite(r) ||
+        !qko_finite(q) || !qko_finite(v0) || !qko_finite(kappa) || !qko_finite(theta) ||
+        !qko_finite(sigma) || !qko_finite(rho))
+        return qko_nan();
+    if (spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 || kappa <= 0.0 || theta < 0.0 ||
+        sigma <= 0.0 || rho <= -1.0 || rho >= 1.0)
+        return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    if (integration_steps < 16 || integration_limit <= 1e-6) return qko_nan();
+    gl_init();
+
+    const double sig2 = sigma * sigma;
+    const double kts2 = kappa * theta / sig2;
+    const double drift = log(spot) + (r - q) * t;
+    const double lk = log(strike);
+
+#define HESTON_CF(u_, out_)                                                               \
+    do {                                                                                  \
+        double complex iu_ = I * (u_);                                                    \
+        double complex beta_ = kappa - rho * sigma * iu_;                                 \
+        double complex d_ = csqrt(beta_ * beta_ + sig2 * (iu_ + (u_) * (u_)));            \
+        double complex bmd_ = beta_ - d_;                                                 \
+        double complex g_ = bmd_ / (beta_ + d_);                                          \
+        double complex e_ = cexp(-d_ * t);                                                \
+        double complex C_ = iu_ * drift + kts2 * (bmd_ * t - 2.0 * clog((1.0 - g_ * e_) / (1.0 - g_))); \
+        double complex D_ = (bmd_ / sig2) * ((1.0 - e_) / (1.0 - g_ * e_));               \
+        (out_) = cexp(C_ + D_ * v0);                                                      \
+    } while (0)
+
+    double complex phi_mi;
+    HESTON_CF(-I, phi_mi);
+    const double phi_abs = cabs(phi_mi);
+    const int panels = (integration_steps + 63) / 64 > 1 ? (integration_steps + 63) / 64 : 1;
+    const double a = 1e-8, b = integration_limit;
+    const double width = (b - a) / panels;
+    double s1 = 0.0, s2 = 0.0;
+    for (int p = 0; p < panels; ++p) {
+        const double pa = a + p * width;
+        const double mid = pa + 0.5 * width, half = 0.5 * width;
+        for (int i = 0; i < 32; ++i) {
+            for (int side = 0; side < 2; ++side) {
+                const double u = side ? mid + half * gl_x[i] : mid - half * gl_x[i];
+                const double complex rot = cexp(-I * u * lk) / (I * u);
+                double complex c2;
+                HESTON_CF(u, c2);
+                s2 += half * gl_w[i] * creal(rot * c2);
+                if (phi_abs >= 1e-14) {
+                    double complex c1;
+                    HESTON_CF(u - I, c1);
+                    s1 += half * gl_w[i] * creal(rot * c1 / phi_mi);
+                }
+            }
+        }
+    }
+#undef HESTON_CF
+    double p2 = 0.5 + s2 / M_PI;
+    double p1 = 0.5 + s1 / M_PI;
+    p2 = p2 < 0.0 ? 0.0 : (p2 > 1.0 ? 1.0 : p2);
+    p1 = p1 < 0.0 ? 0.0 : (p1 > 1.0 ? 1.0 : p1);
+    if (phi_abs < 1e-14) return qko_nan();
+    const double call = spot * exp(-q * t) * p1 - strike * exp(-r * t) * p2;
+    if (ot == QKO_CALL) return call;
+    /* put-call parity */
+    return call - spot * exp(-q * t) + strike * exp(-r * t);
+}
+
+/* ===================================================================== *
+ * 3. Philox replay.
+ *
+ * Philox4x32-10 (Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
+ * easy as 1, 2, 3", SC'11): ten rounds of two 32x32->64 multiplies with a
+ * Weyl-sequence key schedule.
+ *
+ * The GPU kernels draw their normals from this counter layout:
+ *   key      = (low 32 bits of seed, high 32 bits of seed)
+ *   counter  = (unit, block, 0, c3)   c3 = 0 antithetic pairs, 1 plain paths
+ *   output x0..x3 -> two Box-Muller pairs:
+ *     u  = ((x0 >> 9) + 0.5) * 2^-23,  g = ((x1 >> 9) + 0.5) * 2^-22 - 1
+ *     n0 = sqrt(-2 ln u) cos(pi g),    n1 = sqrt(-2 ln u) sin(pi g)
+ *     (x2, x3) -> n2, n3 the same way.
+ * Terminal models: normal k of the option lives at unit k / 4, block 0,
+ *   slot k % 4 (k = pair index, or path index when plain).
+ * One-factor stepwise models: step j of unit u is block j / 4, slot j % 4.
+ * Heston: step j of unit u is block j / 2; z1 = slot 2(j%2), z2 = next slot.
+ * ===================================================================== */
+void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int round = 0; round < 10; ++round) {
+        const uint64_t p0 = (uint64_t)UINT32_C(0xD2511F53) * c0;
+        const uint64_t p1 = (uint64_t)UINT32_C(0xCD9E8D57) * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        const uint32_t n1 = (uint32_t)p1;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        const uint32_t n3 = (uint32_t)p0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += UINT32_C(0x9E3779B9);
+        k1 += UINT32_C(0xBB67AE85);
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+static void box_muller(uint32_t xa, uint32_t xb, double* za, double* zb) {
+    const double u = ((double)(xa >> 9) + 0.5) * 0x1p-23;
+    const double g = ((double)(xb >> 9) + 0.5) * 0x1p-22 - 1.0;
+    const double rad = sqrt(-2.0 * log(u));
+    *za = rad * cos(M_PI * g);
+    *zb = rad * sin(M_PI * g);
+}
+
+void qko_philox_normals4(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[4]) {
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    const uint32_t ctr[4] = {c0, c1, 0u, c3};
+    uint32_t x[4];
+    qko_philox4x32_10(ctr, key, x);
+    box_muller(x[0], x[1], &z[0], &z[1]);
+    box_muller(x[2], x[3], &z[2], &z[3]);
+}
+
+/* One simulated path of unit u under sign sg (+1 / -1) for the stepwise
+ * models, FP64 with the reference step functions. */
+static double replay_path(int32_t model, double spot, double t, double vol, double r, double q,
+                          double v0, double kappa, double theta, double sigma, double rho,
+                          int32_t steps, uint64_t seed, uint32_t unit, uint32_t c3, double sg) {
+    double z4[4];
+    if (model == 0 || model == 1 || model == 5) {
+        qko_philox_normals4(seed, unit / 4u, 0u, c3, z4);
+        return bsm_terminal(vol, r, q, spot, t, sg * z4[unit % 4u]);
+    }
+    const double dt = t / (double)steps;
+    const double sqrt_dt = sqrt(dt);
+    if (model == 6) {
+        const double rho_comp = sqrt(smax(1.0 - rho * rho, 0.0));
+        double s = spot, v = v0;
+        for (int32_t j = 0; j < steps; ++j) {
+            if ((j & 1) == 0) qko_philox_normals4(seed, unit, (uint32_t)(j >> 1), c3, z4);
+            const double z1 = sg * z4[2 * (j & 1)];
+            const double z2 = sg * z4[2 * (j & 1) + 1];
+            const double v_pos = smax(v, 0.0);
+            const double sqrt_v = sqrt(v_pos);
+            const double dw1 = sqrt_dt * z1;
+            const double dw2 = sqrt_dt * (rho * z1 + rho_comp * z2);
+            const double s_next = s * exp((r - q - 0.5 * v_pos) * dt + sqrt_v * dw1);
+            v = smax(0.0, v + kappa * (theta - v_pos) * dt + sigma * sqrt_v * dw2);
+            s = smax(s_next, 1e-12);
+        }
+        return s;
+    }
+    double s = spot;
+    const double drift = r - q;
+    for (int32_t j = 0; j < steps; ++j) {
+        if ((j & 3) == 0) qko_philox_normals4(seed, unit, (uint32_t)(j >> 2), c3, z4);
+        const double dw = sqrt_dt * (sg * z4[j & 3]);
+        if (model == 3)
+            s = smax(1e-12, s + drift * s * dt + vol * s * dw + 0.5 * vol * vol * s * (dw * dw - dt));
+        else
+            s = smax(1e-12, s + drift * s * dt + vol * s * dw);
+    }
+    return s;
+}
+
+double qko_philox_price(int32_t model, double spot, double strike, double t, double vol,
+                        double r, double q, double v0, double kappa, double theta, double sigma,
+                        double rho, int32_t ot, int32_t paths, int32_t steps, uint64_t seed,
+                        int32_t antithetic, double* se) {
+    if (se) *se = qko_nan();
+    /* entry checks and special cases of the matching reference pricer */
+    if (model == 6) {
+        if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
+            kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||
+            !valid_mc_counts(paths, steps))
+            return qko_nan();
+    } else {
+        int counts_ok = (model == 0 || model == 1 || model == 5) ? paths > 1
+                                                                : valid_mc_counts(paths, steps);
+        if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || !counts_ok) return qko_nan();
+    }
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    if (model == 0 && vol <= QKO_EPS) {
+        const double fwd = spot * exp((r - q) * t);
+        return exp(-r * t) * intrinsic(fwd, strike, ot);
+    }
+    const double disc = exp(-r * t);
+    double sum = 0.0, ysum = 0.0, ysq = 0.0, ny = 0.0;
+    if (antithetic) {
+        const int32_t n_pairs = paths / 2;
+        for (int32_t p = 0; p < n_pairs; ++p) {
+            double a = intrinsic(replay_path(model, spot, t, vol, r, q, v0, kappa, theta, sigma,
+                                             rho, steps, seed, (uint32_t)p, 0u, 1.0),
+                                 strike, ot);
+            double b = intrinsic(replay_path(model, spot, t, vol, r, q, v0, kappa, theta, sigma,
+                                             rho, steps, seed, (uint32_t)p, 0u, -1.0),
+                                 strike, ot);
+            sum += a + b;
+            const double m = 0.5 * (a + b);
+            ysum += m;
+            ysq += m * m;
+            ny += 1.0;
+        }
+        if (paths & 1) {
+            sum += intrinsic(replay_path(model, spot, t, vol, r, q, v0, kappa, theta, sigma, rho,
+                                         steps, seed, (uint32_t)n_pairs, 0u, 1.0),
+                             strike, ot);
+        }
+    } else {
+        for (int32_t p = 0; p < paths; ++p) {
+            double a = intrinsic(replay_path(model, spot, t, vol, r, q, v0, kappa, theta, sigma,
+                                             rho, steps, seed, (uint32_t)p, 1u, 1.0),
+                                 strike, ot);
+            sum += a;
+            ysum += a;
+            ysq += a * a;
+            ny += 1.0;
+        }
+    }
+    if (se) *se = se_from_moments(disc, ysum, ysq, ny);
+    return disc * (sum / (double)paths);
+}

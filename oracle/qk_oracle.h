@@ -1,0 +1,105 @@
+/*
+ * qk_oracle.h -- CPU oracle for the batch Monte Carlo pricing path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  Nothing in the product library links or calls
+ * this code; only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * leg load it, and only as the checker.
+ *
+ * Three groups of functions:
+ *
+ *  1. Exact restatement of the reference MC pricers (yluoc/Quant-Kernel,
+ *     cpp/src/common/mc_engine.h:15-136, cpp/src/common/model_concepts.h:93-266,
+ *     cpp/src/algorithms/monte_carlo_methods/ *): same MT19937-64 stream, same
+ *     libstdc++ polar normal, same draw order and the same floating-point
+ *     expression order, so prices match the reference bit for bit.  Each
+ *     pricer also returns the standard error the reference never computes.
+ *
+ *  2. FP64 closed forms: Black-Scholes-Merton (with erfc) and the Heston
+ *     characteristic-function price (Gauss-Legendre P1/P2 integration).
+ *
+ *  3. "Philox replay": the reference step functions in FP64, driven by the
+ *     GPU kernels' counter-based Philox4x32-10 + Box-Muller stream.  Given the
+ *     same seed, the GPU's FP32 estimate and this FP64 estimate see identical
+ *     normals, so their difference isolates FP32 path-state rounding.
+ */
+#ifndef QK_ORACLE_H
+#define QK_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- 1. random streams -------------------------------------------------- */
+typedef struct {
+    uint64_t mt[312];
+    int32_t  idx;
+    int32_t  has_saved;
+    double   saved;
+} qko_normal_gen;
+
+void     qko_gen_init(qko_normal_gen* g, uint64_t seed);
+uint64_t qko_mt64_next(qko_normal_gen* g);
+double   qko_gen_canonical(qko_normal_gen* g);
+double   qko_gen_normal(qko_normal_gen* g);
+/* Fill out[0..n) with the first n normals of seed's stream (fixture helper). */
+void     qko_normals(uint64_t seed, int32_t n, double* out);
+
+/* ---- 1. reference pricers (bit-exact) + standard error ------------------ */
+/* Every pricer returns the price and, when se != NULL, writes the standard
+ * error of that price (NaN when it is undefined: special cases, < 2 samples). */
+double qko_standard_mc(double spot, double strike, double t, double vol, double r, double q,
+                       int32_t option_type, int32_t paths, uint64_t seed, double* se);
+double qko_antithetic(double spot, double strike, double t, double vol, double r, double q,
+                      int32_t option_type, int32_t paths, uint64_t seed, double* se);
+double qko_terminal_plain(double spot, double strike, double t, double vol, double r, double q,
+                          int32_t option_type, int32_t paths, uint64_t seed, double* se);
+double qko_euler(double spot, double strike, double t, double vol, double r, double q,
+                 int32_t option_type, int32_t paths, int32_t steps, uint64_t seed, double* se);
+double qko_milstein(double spot, double strike, double t, double vol, double r, double q,
+                    int32_t option_type, int32_t paths, int32_t steps, uint64_t seed, double* se);
+double qko_local_vol(double spot, double strike, double t, double vol, double r, double q,
+                     int32_t option_type, int32_t paths, int32_t steps, uint64_t seed, double* se);
+double qko_heston(double spot, double strike, double t, double r, double q,
+                  double v0, double kappa, double theta, double sigma, double rho,
+                  int32_t option_type, int32_t paths, int32_t steps, uint64_t seed, double* se);
+
+/* Batch forms (OpenMP over options when built with it).  out_se may be NULL. */
+void qko_heston_batch(const double* spot, const double* strike, const double* t,
+                      const double* r, const double* q, const double* v0,
+                      const double* kappa, const double* theta, const double* sigma,
+                      const double* rho, const int32_t* option_type, const int32_t* paths,
+                      const int32_t* steps, const uint64_t* seed, int32_t n,
+                      double* out, double* out_se);
+/* model: 0 = standard MC (antithetic terminal), 1 = antithetic variates,
+ *        2 = Euler, 3 = Milstein, 4 = local vol (constant), 5 = terminal plain */
+void qko_bsm_family_batch(int32_t model, const double* spot, const double* strike,
+                          const double* t, const double* vol, const double* r,
+                          const double* q, const int32_t* option_type, const int32_t* paths,
+                          const int32_t* steps, const uint64_t* seed, int32_t n,
+                          double* out, double* out_se);
+
+/* ---- 2. closed forms ---------------------------------------------------- */
+double qko_bsm_price(double spot, double strike, double t, double vol, double r, double q,
+                     int32_t option_type);
+double qko_heston_cf_price(double spot, double strike, double t, double r, double q,
+                           double v0, double kappa, double theta, double sigma, double rho,
+                           int32_t option_type, int32_t integration_steps,
+                           double integration_limit);
+
+/* ---- 3. Philox replay of the GPU stream --------------------------------- */
+void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+/* The GPU's normal with index k of stream (seed, c0, c1, c3); see qk_oracle.c. */
+void qko_philox_normals4(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[4]);
+/* model as in qko_bsm_family_batch, plus 6 = Heston (uses v0..rho; vol ignored).
+ * antithetic: 1 = pairs (GPU default), 0 = independent paths. */
+double qko_philox_price(int32_t model, double spot, double strike, double t, double vol,
+                        double r, double q, double v0, double kappa, double theta,
+                        double sigma, double rho, int32_t option_type, int32_t paths,
+                        int32_t steps, uint64_t seed, int32_t antithetic, double* se);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QK_ORACLE_H */

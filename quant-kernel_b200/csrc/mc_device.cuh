@@ -1,0 +1,134 @@
+// mc_device.cuh -- device building blocks of the Monte Carlo kernels.
+//
+// * Philox4x32-10 counter-based generator + Box-Muller, in registers.
+// * Double-double (hi, lo) accumulators for compensated FP64 sums.
+// * FP32 PTX approximations used on the hot path (MUFU unit).
+//
+// All kernels are compiled with --fmad=false: every fused multiply-add below
+// is written explicitly, so a path's FP32 arithmetic is the same whatever the
+// unrolling or launch shape, and results do not depend on the tile config.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mc_types.h"
+
+namespace qkb {
+
+// ---------------------------------------------------------------------------
+// FP32 approximations on the special-function unit (PTX ISA, sm_100a).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float ptx_lg2(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_sqrt(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_sin(float x) {
+    float y;
+    asm("sin.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ptx_cos(float x) {
+    float y;
+    asm("cos.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+// max that propagates NaN: the reference floors with std::max(s, 1e-12),
+// which keeps a NaN s; fmaxf would replace it.
+__device__ __forceinline__ float ptx_max_nan(float a, float b) {
+    float y;
+    asm("max.NaN.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+    return y;
+}
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+
+// ---------------------------------------------------------------------------
+// Philox4x32-10 (Salmon et al., SC'11).  Counter (c0, c1, 0, c3), key = seed.
+// ---------------------------------------------------------------------------
+struct U4 {
+    uint32_t x, y, z, w;
+};
+
+__device__ __forceinline__ U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                            uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int round = 0; round < 10; ++round) {
+        const uint32_t lo0 = c0 * 0xD2511F53u;
+        const uint32_t hi0 = __umulhi(c0, 0xD2511F53u);
+        const uint32_t lo1 = c2 * 0xCD9E8D57u;
+        const uint32_t hi1 = __umulhi(c2, 0xCD9E8D57u);
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return U4{c0, c1, c2, c3};
+}
+
+// Box-Muller on two 32-bit words (the layout the FP64 replay in the oracle
+// mirrors):  u = ((xa >> 9) + 1/2) 2^-23 in (0,1), g = ((xb >> 9) + 1/2) 2^-22 - 1
+// in (-1,1);  za = sqrt(-2 ln u) cos(pi g),  zb = sqrt(-2 ln u) sin(pi g).
+// ln u = log2(u) * ln 2, and sqrt(w) = sqrt.approx(w).
+__device__ __forceinline__ void box_muller(uint32_t xa, uint32_t xb, float& za, float& zb) {
+    const float u = fma_rn(__uint2float_rn(xa >> 9), 0x1p-23f, 0x1p-24f);
+    const float g = fma_rn(__uint2float_rn(xb >> 9), 0x1p-22f, 0x1p-23f - 1.0f);
+    const float w = -1.38629436111989061883f * ptx_lg2(u);  // -2 ln u
+    const float rad = ptx_sqrt(w);
+    const float ang = 3.14159265358979323846f * g;
+    za = rad * ptx_cos(ang);
+    zb = rad * ptx_sin(ang);
+}
+
+__device__ __forceinline__ void normals4(uint32_t unit, uint32_t block, uint32_t c3, uint32_t k0,
+                                         uint32_t k1, float z[4]) {
+    const U4 x = philox4x32_10(unit, block, 0u, c3, k0, k1);
+    box_muller(x.x, x.y, z[0], z[1]);
+    box_muller(x.z, x.w, z[2], z[3]);
+}
+
+// ---------------------------------------------------------------------------
+// Double-double accumulation (Knuth TwoSum).  A non-finite sum drops its error
+// term so that inf stays inf instead of turning into NaN.
+// ---------------------------------------------------------------------------
+struct DD {
+    double hi, lo;
+};
+
+__device__ __forceinline__ DD dd_add(DD a, double b) {
+    const double s = __dadd_rn(a.hi, b);
+    const double bb = __dsub_rn(s, a.hi);
+    double err = __dadd_rn(__dsub_rn(a.hi, __dsub_rn(s, bb)), __dsub_rn(b, bb));
+    if (!isfinite(s)) err = 0.0;
+    return DD{s, __dadd_rn(a.lo, err)};
+}
+
+__device__ __forceinline__ DD dd_merge(DD a, DD b) {
+    DD r = dd_add(a, b.hi);
+    r.lo = __dadd_rn(r.lo, b.lo);
+    return r;
+}
+
+__device__ __forceinline__ DD dd_shfl_down(DD v, int offset) {
+    return DD{__shfl_down_sync(0xffffffffu, v.hi, offset), __shfl_down_sync(0xffffffffu, v.lo, offset)};
+}
+
+__device__ __forceinline__ double payoff(double s_t, double strike, int32_t option_type) {
+    // option_util.h:33-38: max(0, S - K) / max(0, K - S).  fmax(NaN, 0) = 0
+    // matches std::max(0.0, NaN) = 0.0.
+    return option_type == 0 ? fmax(__dsub_rn(s_t, strike), 0.0) : fmax(__dsub_rn(strike, s_t), 0.0);
+}
+
+}  // namespace qkb

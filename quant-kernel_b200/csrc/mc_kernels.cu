@@ -1,0 +1,527 @@
+// mc_kernels.cu -- hand-written sm_100a Monte Carlo kernels.
+//
+// Work decomposition.  A batch is a list of options; option i is split into
+// `tiles` tiles of BLOCK * UPT * unit_iters simulation units (a unit is an
+// antithetic pair or a plain path for the stepwise models, and a quad of four
+// normals for the terminal models).  A CTA simulates one tile at a time: each
+// thread carries UPT units in registers through all time steps, drawing its
+// normals from Philox4x32-10 keyed by the option's seed and countered by
+// (unit, step block) -- so a path's normals depend only on (seed, path index),
+// never on the batch, the launch shape or the scheduling.  Per-thread FP64
+// double-double sums of y and y^2 (y = pair mean or payoff) are reduced
+// warp -> CTA in a fixed order and written to the tile's slot; the finalize
+// kernel merges an option's slots in tile order.  Results are therefore
+// deterministic and a batch reproduces the scalar call bit for bit.
+//
+// Reference loops restated (yluoc/Quant-Kernel):
+//   terminal   mc_engine.h:32-75   + model_concepts.h:93-102
+//   stepwise   mc_engine.h:84-103  + model_concepts.h:136-158, 240-266
+//   Heston     mc_engine.h:113-136 + model_concepts.h:205-226
+// Heston keeps log(S/spot) instead of S: the reference's s * exp(a) step with
+// the std::max(s, 1e-12) floor is the same map as x + a floored at
+// log(1e-12/spot), and it removes the per-step exp.
+#include "mc_device.cuh"
+#include "mc_launch.h"
+
+#include <cstdio>
+
+namespace qkb {
+
+namespace {
+
+// ----------------------------------------------------------------------------
+// Per-thread accumulation of one tile.
+// ----------------------------------------------------------------------------
+struct Acc {
+    DD sy{0.0, 0.0};
+    DD q{0.0, 0.0};
+    __device__ __forceinline__ void add_pair(double a, double b) {
+        const double y = __dmul_rn(0.5, __dadd_rn(a, b));
+        sy = dd_add(sy, y);
+        q = dd_add(q, __dmul_rn(y, y));
+    }
+    __device__ __forceinline__ void add_lone(double a) { sy = dd_add(sy, __dmul_rn(0.5, a)); }
+    __device__ __forceinline__ void add_plain(double a) {
+        sy = dd_add(sy, a);
+        q = dd_add(q, __dmul_rn(a, a));
+    }
+};
+
+// ----------------------------------------------------------------------------
+// Terminal GBM (models 0, 1, 5).  Unit = quad of four normals (one Philox
+// call).  Normal k serves pair k (antithetic) or path k (plain); with an odd
+// antithetic path count, normal n_pairs drives the lone last path.
+// ----------------------------------------------------------------------------
+template <int UPT, bool ANTI>
+__device__ __forceinline__ void sim_terminal(const McOption& o, uint32_t unit0, uint32_t stride,
+                                             uint32_t k0, uint32_t k1, Acc& acc) {
+    const float mu = o.p[0], sg = o.p[1];
+    const uint32_t n_pairs = (uint32_t)o.paths >> 1;
+    const uint32_t n_norm = ANTI ? (uint32_t)(o.paths - (int32_t)n_pairs) : (uint32_t)o.paths;
+    const bool odd = (o.paths & 1) != 0;
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+        const uint32_t unit = unit0 + (uint32_t)k * stride;
+        if (unit * 4u >= n_norm) continue;
+        float z[4];
+        normals4(unit, 0u, ANTI ? 0u : 1u, k0, k1, z);
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t idx = unit * 4u + (uint32_t)s;
+            if (idx >= n_norm) break;
+            const double su = o.spot * exp((double)fma_rn(sg, z[s], mu));
+            const double a = payoff(su, o.strike, o.option_type);
+            if (ANTI) {
+                if (idx < n_pairs) {
+                    const double sd = o.spot * exp((double)fma_rn(-sg, z[s], mu));
+                    acc.add_pair(a, payoff(sd, o.strike, o.option_type));
+                } else if (odd) {
+                    acc.add_lone(a);
+                }
+            } else {
+                acc.add_plain(a);
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// One-factor stepwise BSM (Euler / local vol: MIL = false; Milstein: true).
+// State is s = S/spot in FP32 and the step is the reference's additive form
+//   s' = max(s + s * inc, 1e-12/spot),  inc = (r-q)dt + vol sqrt(dt) z
+//   [Milstein: + c (z^2 - 1), c = vol^2 dt / 2]
+// evaluated as one fused s + s * inc.  One Philox call feeds four steps.
+// ----------------------------------------------------------------------------
+template <int UPT, bool ANTI, bool MIL>
+__device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, uint32_t stride,
+                                             uint32_t k0, uint32_t k1, Acc& acc) {
+    const float m0 = o.p[0], b = o.p[1], fl = o.p[2], c = o.p[3];
+    const int32_t steps = o.steps;
+    const uint32_t units = (uint32_t)o.units;
+    const uint32_t c3 = ANTI ? 0u : 1u;
+    float su[UPT], sd[UPT];
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+        su[k] = 1.0f;
+        sd[k] = 1.0f;
+    }
+    for (int32_t j = 0; j < steps; j += 4) {
+        float z[UPT][4];
+#pragma unroll
+        for (int k = 0; k < UPT; ++k) normals4(unit0 + (uint32_t)k * stride, (uint32_t)(j >> 2), c3, k0, k1, z[k]);
+        const int32_t m = (steps - j) < 4 ? (steps - j) : 4;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (s < m) {
+#pragma unroll
+                for (int k = 0; k < UPT; ++k) {
+                    const float zz = z[k][s];
+                    float iu, id;
+                    if (MIL) {
+                        iu = fma_rn(fma_rn(c, zz, b), zz, m0);
+                        id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
+                    } else {
+                        iu = fma_rn(b, zz, m0);
+                        id = fma_rn(-b, zz, m0);
+                    }
+                    su[k] = fmaxf(fma_rn(su[k], iu, su[k]), fl);
+                    if (ANTI) sd[k] = fmaxf(fma_rn(sd[k], id, sd[k]), fl);
+                }
+            }
+        }
+    }
+    const uint32_t n_pairs = (uint32_t)o.paths >> 1;
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+        const uint32_t unit = unit0 + (uint32_t)k * stride;
+        if (unit >= units) continue;
+        const double pu = payoff(o.spot * (double)su[k], o.strike, o.option_type);
+        if (ANTI) {
+            if (unit < n_pairs)
+                acc.add_pair(pu, payoff(o.spot * (double)sd[k], o.strike, o.option_type));
+            else
+                acc.add_lone(pu);
+        } else {
+            acc.add_plain(pu);
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Heston full-truncation Euler.  State (x, v) with x = log(S/spot):
+//   x' = max_nan(x + (r-q)dt - v dt/2 + sqrt(v) sqrt(dt) z1, log(1e-12/spot))
+//   v' = max(v (1 - kappa dt) + kappa theta dt
+//            + sigma sqrt(dt) sqrt(v) (rho z1 + sqrt(1-rho^2) z2), 0)
+// v >= 0 after every step (and v0 >= 0 is validated), so the reference's
+// v_pos = max(v, 0) is v itself.  One Philox call feeds two steps of a unit.
+// ----------------------------------------------------------------------------
+template <int UPT, bool ANTI>
+__device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, uint32_t stride,
+                                           uint32_t k0, uint32_t k1, Acc& acc) {
+    const float cmu = o.p[0], hdt = o.p[1], sqdt = o.p[2], kdt = o.p[3], kth = o.p[4];
+    const float xsq = o.p[5], rho = o.p[6], rhoc = o.p[7], v0 = o.p[8], xfl = o.p[9];
+    const float omk = 1.0f - kdt;
+    const float xr = xsq * rho, xc = xsq * rhoc;
+    const int32_t steps = o.steps;
+    const uint32_t units = (uint32_t)o.units;
+    const uint32_t c3 = ANTI ? 0u : 1u;
+    float xu[UPT], vu[UPT], xd[UPT], vd[UPT];
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+        xu[k] = 0.0f;
+        xd[k] = 0.0f;
+        vu[k] = v0;
+        vd[k] = v0;
+    }
+    for (int32_t j = 0; j < steps; j += 2) {
+        float z[UPT][4];
+#pragma unroll
+        for (int k = 0; k < UPT; ++k) normals4(unit0 + (uint32_t)k * stride, (uint32_t)(j >> 1), c3, k0, k1, z[k]);
+        const int32_t m = (steps - j) < 2 ? (steps - j) : 2;
+#pragma unroll
+        for (int s = 0; s < 2; ++s) {
+            if (s < m) {
+#pragma unroll
+                for (int k = 0; k < UPT; ++k) {
+                    const float z1 = z[k][2 * s], z2 = z[k][2 * s + 1];
+                    const float sz1 = sqdt * z1;
+                    const float xw = fma_rn(xr, z1, xc * z2);
+                    {
+                        const float sv = ptx_sqrt(vu[k]);
+                        const float inc = fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu));
+                        xu[k] = ptx_max_nan(xu[k] + inc, xfl);
+                        vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
+                    }
+                    if (ANTI) {
+                        const float sv = ptx_sqrt(vd[k]);
+                        const float inc = fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu));
+                        xd[k] = ptx_max_nan(xd[k] + inc, xfl);
+                        vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
+                    }
+                }
+            }
+        }
+    }
+    const uint32_t n_pairs = (uint32_t)o.paths >> 1;
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+        const uint32_t unit = unit0 + (uint32_t)k * stride;
+        if (unit >= units) continue;
+        const double pu = payoff(o.spot * exp((double)xu[k]), o.strike, o.option_type);
+        if (ANTI) {
+            if (unit < n_pairs)
+                acc.add_pair(pu, payoff(o.spot * exp((double)xd[k]), o.strike, o.option_type));
+            else
+                acc.add_lone(pu);
+        } else {
+            acc.add_plain(pu);
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Fixed-order CTA reduction of (sy, q) into the tile's slot.
+// ----------------------------------------------------------------------------
+template <int BLOCK>
+__device__ __forceinline__ void reduce_tile(Acc acc, TilePartial* __restrict__ out, DD* smem) {
+    constexpr int W = BLOCK / 32;
+    DD a = acc.sy, b = acc.q;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        a = dd_merge(a, dd_shfl_down(a, off));
+        b = dd_merge(b, dd_shfl_down(b, off));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        smem[warp] = a;
+        smem[W + warp] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD ta = smem[0], tb = smem[W];
+#pragma unroll
+        for (int w = 1; w < W; ++w) {
+            ta = dd_merge(ta, smem[w]);
+            tb = dd_merge(tb, smem[W + w]);
+        }
+        TilePartial t;
+        t.sy_hi = ta.hi;
+        t.sy_lo = ta.lo;
+        t.q_hi = tb.hi;
+        t.q_lo = tb.lo;
+        *out = t;
+    }
+    __syncthreads();
+}
+
+// Option owning `tile`: the last i with tile_begin[i] <= tile (tile_begin is
+// non-decreasing, n + 1 entries, tile_begin[n] = total tiles).
+__device__ __forceinline__ int32_t find_option(const int64_t* __restrict__ tile_begin, int32_t n,
+                                               int64_t tile) {
+    int32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int32_t mid = (lo + hi + 1) >> 1;
+        if (__ldg(tile_begin + mid) <= tile)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int FAMILY, int UPT, bool ANTI>
+__device__ __forceinline__ void sim_family(const McOption& o, uint32_t unit0, uint32_t stride,
+                                           uint32_t k0, uint32_t k1, Acc& acc) {
+    if (FAMILY == kFamTerminal) sim_terminal<UPT, ANTI>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamEuler) sim_stepwise<UPT, ANTI, false>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamMilstein) sim_stepwise<UPT, ANTI, true>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamHeston) sim_heston<UPT, ANTI>(o, unit0, stride, k0, k1, acc);
+}
+
+// One tile: all UPT * unit_iters units of every thread, then the reduction.
+template <int FAMILY, int BLOCK, int UPT, bool ANTI>
+__device__ __forceinline__ void run_tile(const McOption& o, int64_t tile, TilePartial* partials,
+                                         DD* smem) {
+    const uint32_t k0 = (uint32_t)o.seed, k1 = (uint32_t)(o.seed >> 32);
+    const int64_t local = tile - o.tile_begin;
+    const uint32_t per_iter = (uint32_t)(BLOCK * UPT);
+    const uint32_t first = (uint32_t)(local * (int64_t)per_iter * o.unit_iters);
+    Acc acc;
+    for (int32_t it = 0; it < o.unit_iters; ++it) {
+        const uint32_t base = first + (uint32_t)it * per_iter;
+        if (base >= (uint32_t)o.units) break;
+        sim_family<FAMILY, UPT, ANTI>(o, base + threadIdx.x, (uint32_t)BLOCK, k0, k1, acc);
+    }
+    reduce_tile<BLOCK>(acc, partials + tile, smem);
+}
+
+// ----------------------------------------------------------------------------
+// Kernel 1a: single-family simulate, grid-stride over tiles.
+// ----------------------------------------------------------------------------
+template <int FAMILY, int BLOCK, int UPT, bool ANTI>
+__global__ void __launch_bounds__(BLOCK)
+    mc_simulate_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
+                       int32_t n, int64_t n_tiles, TilePartial* __restrict__ partials) {
+    __shared__ DD smem[2 * (BLOCK / 32)];
+    for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const int32_t oi = find_option(tile_begin, n, tile);
+        const McOption o = opts[oi];
+        run_tile<FAMILY, BLOCK, UPT, ANTI>(o, tile, partials, smem);
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Kernel 1b: persistent work-stealing simulate for mixed batches.  One CTA per
+// resident slot; each CTA takes the next tile from a global counter until the
+// list is exhausted, then dispatches on the tile's model.  The counter is
+// reset by the finalize kernel of the same execute, so a captured graph can
+// replay without a memset.  Every CTA exits after at most n_tiles + 1 grabs
+// in total, so the loop always terminates.
+// ----------------------------------------------------------------------------
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK)
+    mc_persistent_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
+                         int32_t n, int64_t n_tiles, TilePartial* __restrict__ partials,
+                         unsigned long long* __restrict__ work_counter) {
+    __shared__ DD smem[2 * (BLOCK / 32)];
+    __shared__ long long s_tile;
+    for (;;) {
+        if (threadIdx.x == 0) s_tile = (long long)atomicAdd(work_counter, 1ull);
+        __syncthreads();
+        const int64_t tile = s_tile;
+        __syncthreads();
+        if (tile >= n_tiles) break;
+        const int32_t oi = find_option(tile_begin, n, tile);
+        const McOption o = opts[oi];
+        const bool anti = o.antithetic != 0;
+        switch (o.model) {
+            case kStandard:
+            case kAntithetic:
+                run_tile<kFamTerminal, BLOCK, kUptTerminal, true>(o, tile, partials, smem);
+                break;
+            case kTerminalPlain:
+                run_tile<kFamTerminal, BLOCK, kUptTerminal, false>(o, tile, partials, smem);
+                break;
+            case kEuler:
+            case kLocalVol:
+                if (anti)
+                    run_tile<kFamEuler, BLOCK, kUptStepwise, true>(o, tile, partials, smem);
+                else
+                    run_tile<kFamEuler, BLOCK, kUptStepwise, false>(o, tile, partials, smem);
+                break;
+            case kMilstein:
+                if (anti)
+                    run_tile<kFamMilstein, BLOCK, kUptStepwise, true>(o, tile, partials, smem);
+                else
+                    run_tile<kFamMilstein, BLOCK, kUptStepwise, false>(o, tile, partials, smem);
+                break;
+            default:  // kHeston
+                if (anti)
+                    run_tile<kFamHeston, BLOCK, kUptHeston, true>(o, tile, partials, smem);
+                else
+                    run_tile<kFamHeston, BLOCK, kUptHeston, false>(o, tile, partials, smem);
+                break;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Kernel 2: finalize.  One warp per option merges the option's tile slots in
+// tile order (lane-strided, then a fixed shuffle tree), then writes price and
+// standard error.  Also resets the work counter for the next execute.
+// ----------------------------------------------------------------------------
+__global__ void __launch_bounds__(256)
+    mc_finalize_kernel(const McOption* __restrict__ opts, int32_t n,
+                       const TilePartial* __restrict__ partials, double* __restrict__ out_price,
+                       double* __restrict__ out_se, unsigned long long* __restrict__ work_counter) {
+    if (work_counter != nullptr && blockIdx.x == 0 && threadIdx.x == 0) *work_counter = 0ull;
+    const int32_t warp = (int32_t)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const McOption& o = opts[warp];
+    if (o.mode != kModeSimulate) {
+        if (lane == 0) {
+            out_price[warp] = o.const_price;
+            out_se[warp] = __longlong_as_double(0x7FF8000000000000ll);
+        }
+        return;
+    }
+    DD sy{0.0, 0.0}, q{0.0, 0.0};
+    for (int32_t t = lane; t < o.tiles; t += 32) {
+        const TilePartial p = partials[o.tile_begin + t];
+        sy = dd_merge(sy, DD{p.sy_hi, p.sy_lo});
+        q = dd_merge(q, DD{p.q_hi, p.q_lo});
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        sy = dd_merge(sy, dd_shfl_down(sy, off));
+        q = dd_merge(q, dd_shfl_down(q, off));
+    }
+    if (lane == 0) {
+        const double s = sy.hi + sy.lo;
+        const double qq = q.hi + q.lo;
+        const double total = o.antithetic ? 2.0 * s : s;  // sum of all path payoffs
+        out_price[warp] = o.disc * (total / (double)o.paths);
+        const double ns = (double)o.samples;
+        double se = __longlong_as_double(0x7FF8000000000000ll);
+        if (ns >= 2.0) {
+            const double mean = s / ns;
+            double var = (qq - ns * mean * mean) / (ns - 1.0);
+            if (var < 0.0) var = 0.0;
+            se = o.disc * sqrt(var / ns);
+        }
+        out_se[warp] = se;
+    }
+}
+
+template <int FAMILY, int BLOCK, int UPT, bool ANTI>
+cudaError_t launch_one(const SimArgs& a, cudaStream_t st) {
+    const int64_t cap = (int64_t)a.max_ctas;
+    const unsigned grid = (unsigned)(a.n_tiles < cap ? a.n_tiles : cap);
+    mc_simulate_kernel<FAMILY, BLOCK, UPT, ANTI>
+        <<<grid, BLOCK, 0, st>>>(a.opts, a.tile_begin, a.n, a.n_tiles, a.partials);
+    return cudaGetLastError();
+}
+
+template <int FAMILY, int BLOCK, bool ANTI>
+cudaError_t launch_upt(int upt, const SimArgs& a, cudaStream_t st) {
+    switch (upt) {
+        case 1: return launch_one<FAMILY, BLOCK, 1, ANTI>(a, st);
+        case 2: return launch_one<FAMILY, BLOCK, 2, ANTI>(a, st);
+        case 4: return launch_one<FAMILY, BLOCK, 4, ANTI>(a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int FAMILY, bool ANTI>
+cudaError_t launch_block(int block, int upt, const SimArgs& a, cudaStream_t st) {
+    switch (block) {
+        case 128: return launch_upt<FAMILY, 128, ANTI>(upt, a, st);
+        case 256: return launch_upt<FAMILY, 256, ANTI>(upt, a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int FAMILY>
+cudaError_t launch_anti(bool anti, int block, int upt, const SimArgs& a, cudaStream_t st) {
+    return anti ? launch_block<FAMILY, true>(block, upt, a, st)
+                : launch_block<FAMILY, false>(block, upt, a, st);
+}
+
+}  // namespace
+
+int family_of(int32_t model) {
+    switch (model) {
+        case kStandard:
+        case kAntithetic:
+        case kTerminalPlain: return kFamTerminal;
+        case kEuler:
+        case kLocalVol: return kFamEuler;
+        case kMilstein: return kFamMilstein;
+        default: return kFamHeston;
+    }
+}
+
+cudaError_t launch_simulate(int family, bool anti, int block, int upt, const SimArgs& a,
+                            cudaStream_t st) {
+    if (a.n_tiles <= 0) return cudaSuccess;
+    switch (family) {
+        case kFamTerminal: return launch_anti<kFamTerminal>(anti, block, upt, a, st);
+        case kFamEuler: return launch_anti<kFamEuler>(anti, block, upt, a, st);
+        case kFamMilstein: return launch_anti<kFamMilstein>(anti, block, upt, a, st);
+        case kFamHeston: return launch_anti<kFamHeston>(anti, block, upt, a, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_persistent(int block, const SimArgs& a, unsigned long long* work_counter,
+                              cudaStream_t st) {
+    if (a.n_tiles <= 0) return cudaSuccess;
+    const int64_t cap = (int64_t)a.max_ctas;
+    const unsigned grid = (unsigned)(a.n_tiles < cap ? a.n_tiles : cap);
+    if (block == 128)
+        mc_persistent_kernel<128><<<grid, 128, 0, st>>>(a.opts, a.tile_begin, a.n, a.n_tiles,
+                                                        a.partials, work_counter);
+    else if (block == 256)
+        mc_persistent_kernel<256><<<grid, 256, 0, st>>>(a.opts, a.tile_begin, a.n, a.n_tiles,
+                                                        a.partials, work_counter);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const McOption* opts, int32_t n, const TilePartial* partials,
+                            double* out_price, double* out_se, unsigned long long* work_counter,
+                            cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int64_t threads = (int64_t)n * 32;
+    const unsigned grid = (unsigned)((threads + 255) / 256);
+    mc_finalize_kernel<<<grid, 256, 0, st>>>(opts, n, partials, out_price, out_se, work_counter);
+    return cudaGetLastError();
+}
+
+int max_resident_ctas(int family_or_persistent, int block, int upt, int device) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    int per_sm = 0;
+    cudaError_t e = cudaSuccess;
+    if (family_or_persistent < 0) {
+        e = block == 128 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_persistent_kernel<128>, 128, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_persistent_kernel<256>, 256, 0);
+    } else {
+        // Occupancy of the Heston variant bounds the others (most registers).
+        if (block == 128) {
+            e = upt == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 1, true>, 128, 0)
+              : upt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 2, true>, 128, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 4, true>, 128, 0);
+        } else {
+            e = upt == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 1, true>, 256, 0)
+              : upt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 2, true>, 256, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 4, true>, 256, 0);
+        }
+    }
+    if (e != cudaSuccess || per_sm <= 0) return 0;
+    return sms * per_sm;
+}
+
+}  // namespace qkb

@@ -1,0 +1,42 @@
+// mc_launch.h -- host-side launch interface of the Monte Carlo kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace qkb {
+
+struct McOption;
+struct TilePartial;
+
+// Kernel families: the models that share one simulation loop.
+enum : int { kFamTerminal = 0, kFamEuler = 1, kFamMilstein = 2, kFamHeston = 3, kNumFamilies = 4 };
+
+// Units per thread compiled into the persistent mixed-model kernel.
+constexpr int kUptTerminal = 1;
+constexpr int kUptStepwise = 2;
+constexpr int kUptHeston = 2;
+
+struct SimArgs {
+    const McOption* opts;      // device, n records
+    const int64_t* tile_begin; // device, n + 1 entries
+    int32_t n;
+    int64_t n_tiles;
+    TilePartial* partials;     // device, n_tiles slots
+    int32_t max_ctas;          // grid cap (grid-stride beyond it)
+};
+
+int family_of(int32_t model);
+
+cudaError_t launch_simulate(int family, bool anti, int block, int upt, const SimArgs& a,
+                            cudaStream_t st);
+cudaError_t launch_persistent(int block, const SimArgs& a, unsigned long long* work_counter,
+                              cudaStream_t st);
+cudaError_t launch_finalize(const McOption* opts, int32_t n, const TilePartial* partials,
+                            double* out_price, double* out_se, unsigned long long* work_counter,
+                            cudaStream_t st);
+// Resident CTAs on `device` for a family kernel (family >= 0) or the
+// persistent kernel (family < 0); 0 on error.
+int max_resident_ctas(int family_or_persistent, int block, int upt, int device);
+
+}  // namespace qkb

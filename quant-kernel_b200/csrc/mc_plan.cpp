@@ -1,0 +1,599 @@
+// mc_plan.cpp -- host runtime of the Monte Carlo path.
+//
+// Validation and special cases follow the reference pricers one to one
+// (yluoc/Quant-Kernel):
+//   standard_monte_carlo.cpp:14-23   antithetic_variates.cpp:14-19
+//   euler_maruyama.cpp:14-19         milstein.cpp:14-19
+//   local_vol_monte_carlo.cpp:61-66  heston_monte_carlo.cpp:17-26
+//   option_util.h:27-50, monte_carlo_methods/common/internal_util.h:13-26
+// An invalid option gets NaN and the batch still returns QK_OK
+// (qk_api.cpp:1152-1159 writes per-element results), t <= 1e-12 gives the
+// undiscounted intrinsic value, and only standard MC has the zero-vol
+// discounted-forward branch.  Everything else is simulated on the GPU.
+#include "mc_plan.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <mutex>
+
+#include "mc_launch.h"
+
+namespace qkb {
+
+namespace {
+
+constexpr double kEps = 1e-12;
+constexpr int64_t kMaxTilesPerOption = 4096;
+
+double nan_value() { return std::numeric_limits<double>::quiet_NaN(); }
+
+bool finite_bits(double x) {
+    uint64_t bits;
+    std::memcpy(&bits, &x, sizeof bits);
+    return (bits & 0x7FF0000000000000ull) != 0x7FF0000000000000ull;
+}
+
+// std::max(a, b) == (a < b) ? b : a; the reference's NaN results follow it.
+double smax(double a, double b) { return (a < b) ? b : a; }
+
+double intrinsic(double x, double y, int32_t ot) {
+    if (ot == 0) return smax(0.0, x - y);
+    if (ot == 1) return smax(0.0, y - x);
+    return nan_value();
+}
+
+bool valid_option_type(int32_t ot) { return ot == 0 || ot == 1; }
+
+bool valid_common_inputs(double spot, double strike, double t, double vol, double r, double q,
+                         int32_t ot) {
+    if (!valid_option_type(ot)) return false;
+    if (!finite_bits(spot) || !finite_bits(strike) || !finite_bits(t) || !finite_bits(vol) ||
+        !finite_bits(r) || !finite_bits(q))
+        return false;
+    return spot > 0.0 && strike > 0.0 && t >= 0.0 && vol >= 0.0;
+}
+
+void set_const(McOption& o, double price) {
+    o.mode = kModeConstant;
+    o.const_price = price;
+    o.tiles = 0;
+    o.units = 0;
+}
+
+int32_t geti(const int32_t* a, int32_t i, int32_t dflt) { return a ? a[i] : dflt; }
+
+// Pack option i.  Fills everything but the tile geometry.
+McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
+    McOption o;
+    std::memset(&o, 0, sizeof o);
+    const int32_t m = in.model ? in.model[i] : in.uniform_model;
+    o.model = m;
+    o.option_type = in.option_type[i];
+    o.paths = in.paths[i];
+    o.seed = in.seed[i];
+    o.spot = in.spot[i];
+    o.strike = in.strike[i];
+    o.mode = kModeSimulate;
+    const double spot = in.spot[i], strike = in.strike[i], t = in.t[i];
+    const int32_t ot = o.option_type, paths = o.paths;
+
+    if (m == kStandard || m == kAntithetic || m == kTerminalPlain) {
+        const double vol = in.vol[i], r = in.r[i], q = in.q[i];
+        o.steps = 1;
+        if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 1) {
+            set_const(o, nan_value());
+            return o;
+        }
+        if (t <= kEps) {
+            set_const(o, intrinsic(spot, strike, ot));
+            return o;
+        }
+        if (m == kStandard && vol <= kEps) {
+            const double fwd = spot * std::exp((r - q) * t);
+            set_const(o, std::exp(-r * t) * intrinsic(fwd, strike, ot));
+            return o;
+        }
+        o.disc = std::exp(-r * t);
+        o.antithetic = (m != kTerminalPlain) ? 1 : 0;
+        const int32_t n_norm = o.antithetic ? paths - paths / 2 : paths;
+        o.units = (int32_t)(((int64_t)n_norm + 3) / 4);
+        o.samples = o.antithetic ? paths / 2 : paths;
+        o.p[0] = (float)((r - q - 0.5 * vol * vol) * t);
+        o.p[1] = (float)(vol * std::sqrt(smax(t, 0.0)));
+        return o;
+    }
+    if (m == kEuler || m == kMilstein || m == kLocalVol) {
+        const double vol = in.vol[i], r = in.r[i], q = in.q[i];
+        const int32_t steps = geti(in.steps, i, 0);
+        o.steps = steps;
+        if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || !(paths > 1 && steps > 0)) {
+            set_const(o, nan_value());
+            return o;
+        }
+        if (t <= kEps) {
+            set_const(o, intrinsic(spot, strike, ot));
+            return o;
+        }
+        o.disc = std::exp(-r * t);
+        o.antithetic = anti_stepwise ? 1 : 0;
+        o.units = o.antithetic ? paths - paths / 2 : paths;
+        o.samples = o.antithetic ? paths / 2 : paths;
+        const double dt = t / (double)steps;
+        const double sq = std::sqrt(dt);
+        const double c = (m == kMilstein) ? 0.5 * vol * vol * dt : 0.0;
+        o.p[0] = (float)((r - q) * dt - c);
+        o.p[1] = (float)(vol * sq);
+        o.p[2] = (float)(1e-12 / spot);
+        o.p[3] = (float)c;
+        return o;
+    }
+    if (m == kHeston) {
+        const double r = in.r[i], q = in.q[i];
+        const double v0 = in.v0[i], kappa = in.kappa[i], theta = in.theta[i];
+        const double sigma = in.sigma[i], rho = in.rho[i];
+        const int32_t steps = geti(in.steps, i, 0);
+        o.steps = steps;
+        // heston_monte_carlo.cpp:18-24 -- no finiteness test: a NaN passes the
+        // comparisons and flows through the simulation as in the reference.
+        if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
+            kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||
+            !(paths > 1 && steps > 0)) {
+            set_const(o, nan_value());
+            return o;
+        }
+        if (t <= kEps) {
+            set_const(o, intrinsic(spot, strike, ot));
+            return o;
+        }
+        o.disc = std::exp(-r * t);
+        o.antithetic = anti_stepwise ? 1 : 0;
+        o.units = o.antithetic ? paths - paths / 2 : paths;
+        o.samples = o.antithetic ? paths / 2 : paths;
+        const double dt = t / (double)steps;
+        const double sq = std::sqrt(dt);
+        o.p[0] = (float)((r - q) * dt);
+        o.p[1] = (float)(0.5 * dt);
+        o.p[2] = (float)sq;
+        o.p[3] = (float)(kappa * dt);
+        o.p[4] = (float)(kappa * theta * dt);
+        o.p[5] = (float)(sigma * sq);
+        o.p[6] = (float)rho;
+        o.p[7] = (float)std::sqrt(smax(1.0 - rho * rho, 0.0));
+        o.p[8] = (float)v0;
+        o.p[9] = (float)std::log(1e-12 / spot);
+        return o;
+    }
+    set_const(o, nan_value());  // unknown model code
+    return o;
+}
+
+int upt_for(int family, bool persistent, const LaunchConfig& cfg) {
+    if (!persistent) return cfg.upt;
+    switch (family) {
+        case kFamTerminal: return kUptTerminal;
+        case kFamHeston: return kUptHeston;
+        default: return kUptStepwise;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+std::string device_name(int dev) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
+    std::string s = prop.name;
+    for (char& c : s)
+        if (c == ' ' || c == '|') c = '_';
+    return s;
+}
+
+}  // namespace
+
+// ----------------------------------------------------------------------------
+cudaError_t DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    release();
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cap = 0;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+cudaError_t PinnedBuf::ensure(size_t bytes) {
+    if (bytes <= cap && p) return cudaSuccess;
+    release();
+    size_t want = std::max<size_t>(bytes, 256);
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        cap = 0;
+        return e;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+void PinnedBuf::release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+}
+
+// ----------------------------------------------------------------------------
+// Default launch shapes (measured on B200; the autotuner may override them).
+LaunchConfig default_config(int family) {
+    LaunchConfig c;
+    c.block = 256;
+    c.upt = (family == kFamTerminal) ? 1 : 2;
+    return c;
+}
+
+namespace {
+std::mutex g_tune_mu;
+std::map<std::string, LaunchConfig>& tune_map() {
+    static std::map<std::string, LaunchConfig> m;
+    return m;
+}
+bool g_tune_loaded = false;
+
+const char* tune_path() {
+    const char* p = std::getenv("QK_B200_TUNE_CACHE");
+    return (p && *p) ? p : nullptr;
+}
+
+void load_tune_file_locked() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    const char* path = tune_path();
+    if (!path) return;
+    FILE* f = std::fopen(path, "r");
+    if (!f) return;
+    char key[512];
+    int block = 0, upt = 0;
+    // one entry per line: <key> <block> <upt>
+    while (std::fscanf(f, "%511s %d %d", key, &block, &upt) == 3) {
+        if ((block == 128 || block == 256) && (upt == 1 || upt == 2 || upt == 4))
+            tune_map()[key] = LaunchConfig{block, upt};
+    }
+    std::fclose(f);
+}
+}  // namespace
+
+bool tuned_config(const std::string& key, LaunchConfig* out) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    load_tune_file_locked();
+    auto it = tune_map().find(key);
+    if (it == tune_map().end()) return false;
+    *out = it->second;
+    return true;
+}
+
+void store_tuned_config(const std::string& key, const LaunchConfig& cfg) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    load_tune_file_locked();
+    tune_map()[key] = cfg;
+    const char* path = tune_path();
+    if (!path) return;
+    FILE* f = std::fopen(path, "w");
+    if (!f) return;
+    for (const auto& kv : tune_map())
+        std::fprintf(f, "%s %d %d\n", kv.first.c_str(), kv.second.block, kv.second.upt);
+    std::fclose(f);
+}
+
+// ----------------------------------------------------------------------------
+Plan::~Plan() { release(); }
+
+cudaError_t Plan::release() {
+    drop_graph();
+    if (device_ >= 0) {
+        DeviceGuard g(device_);
+        d_opts_.release();
+        d_tile_begin_.release();
+        d_partials_.release();
+        d_price_.release();
+        d_se_.release();
+        d_counter_.release();
+        h_opts_.release();
+        h_tile_begin_.release();
+        h_price_.release();
+        h_se_.release();
+        if (ev0_) cudaEventDestroy(ev0_);
+        if (ev1_) cudaEventDestroy(ev1_);
+        if (stream_) cudaStreamDestroy(stream_);
+    }
+    ev0_ = ev1_ = nullptr;
+    stream_ = nullptr;
+    device_ = -1;
+    return cudaSuccess;
+}
+
+void Plan::drop_graph() {
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (graph_) cudaGraphDestroy(graph_);
+    graph_exec_ = nullptr;
+    graph_ = nullptr;
+}
+
+cudaError_t Plan::ensure_stream() {
+    if (stream_) return cudaSuccess;
+    cudaError_t e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+    e = cudaEventCreate(&ev0_);
+    if (e != cudaSuccess) return e;
+    return cudaEventCreate(&ev1_);
+}
+
+cudaError_t Plan::build(const BatchInput& in, int32_t flags, std::string* err) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (device_ >= 0 && device_ != dev) release();
+    device_ = dev;
+    drop_graph();
+    e = ensure_stream();
+    if (e != cudaSuccess) return e;
+
+    flags_ = flags;
+    n_ = in.n;
+    opts_.resize((size_t)in.n);
+    const bool anti_stepwise = (flags & kFlagNoAntithetic) == 0;
+    int fam = -2;  // -2: none yet, -1: mixed
+    bool anti = true;
+    path_steps_ = 0;
+    for (int32_t i = 0; i < in.n; ++i) {
+        McOption o = pack_option(in, i, anti_stepwise);
+        if (o.mode == kModeSimulate) {
+            const int f = family_of(o.model);
+            const bool a = o.antithetic != 0;
+            if (fam == -2) {
+                fam = f;
+                anti = a;
+            } else if (fam != f || anti != a) {
+                fam = -1;
+            }
+            path_steps_ += (int64_t)o.paths * (int64_t)std::max(o.steps, 1);
+        }
+        opts_[(size_t)i] = o;
+    }
+    family_ = (fam == -2) ? kFamTerminal : fam;
+    anti_ = anti;
+    persistent_ = (fam == -1) || (flags & kFlagPersistent);
+    if (persistent_) {
+        cfg_ = LaunchConfig{256, 0};
+    } else {
+        cfg_ = default_config(family_);
+    }
+    const std::string key = device_name(device_) + "|" + (persistent_ ? "persistent" : std::to_string(family_)) +
+                            "|" + (anti_ ? "anti" : "plain");
+    LaunchConfig tuned;
+    if (tuned_config(key, &tuned)) {
+        cfg_.block = tuned.block;
+        if (!persistent_) cfg_.upt = tuned.upt;
+    }
+    e = layout_tiles(cfg_);
+    if (e != cudaSuccess) return e;
+    if ((flags & kFlagAutotune) && n_tiles_ > 0) {
+        e = autotune();
+        if (e != cudaSuccess) return e;
+        LaunchConfig store = cfg_;
+        if (persistent_) store.upt = 1;
+        store_tuned_config(key, store);
+    }
+    (void)err;
+    return cudaSuccess;
+}
+
+cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
+    const int32_t n = n_;
+    int64_t total = 0;
+    std::vector<int64_t> begin((size_t)n + 1);
+    for (int32_t i = 0; i < n; ++i) {
+        McOption& o = opts_[(size_t)i];
+        begin[(size_t)i] = total;
+        o.tile_begin = total;
+        if (o.mode != kModeSimulate || o.units <= 0) {
+            o.tiles = 0;
+            o.unit_iters = 0;
+            continue;
+        }
+        const int64_t per_iter = (int64_t)cfg.block * upt_for(family_of(o.model), persistent_, cfg);
+        const int64_t units = o.units;
+        int64_t iters = (units + per_iter * kMaxTilesPerOption - 1) / (per_iter * kMaxTilesPerOption);
+        if (iters < 1) iters = 1;
+        const int64_t tile_units = per_iter * iters;
+        o.unit_iters = (int32_t)iters;
+        o.tiles = (int32_t)((units + tile_units - 1) / tile_units);
+        total += o.tiles;
+    }
+    begin[(size_t)n] = total;
+    n_tiles_ = total;
+
+    cudaError_t e;
+    const size_t opt_bytes = sizeof(McOption) * (size_t)std::max(n, 1);
+    const size_t tb_bytes = sizeof(int64_t) * ((size_t)n + 1);
+    if ((e = d_opts_.ensure(opt_bytes)) != cudaSuccess) return e;
+    if ((e = d_tile_begin_.ensure(tb_bytes)) != cudaSuccess) return e;
+    if ((e = d_partials_.ensure(sizeof(TilePartial) * (size_t)std::max<int64_t>(total, 1))) != cudaSuccess) return e;
+    if ((e = d_price_.ensure(sizeof(double) * (size_t)std::max(n, 1))) != cudaSuccess) return e;
+    if ((e = d_se_.ensure(sizeof(double) * (size_t)std::max(n, 1))) != cudaSuccess) return e;
+    if ((e = d_counter_.ensure(sizeof(unsigned long long))) != cudaSuccess) return e;
+    if ((e = h_opts_.ensure(opt_bytes)) != cudaSuccess) return e;
+    if ((e = h_tile_begin_.ensure(tb_bytes)) != cudaSuccess) return e;
+    // The previous upload from these staging buffers may still be in flight.
+    if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return e;
+    std::memcpy(h_opts_.p, opts_.data(), sizeof(McOption) * (size_t)n);
+    std::memcpy(h_tile_begin_.p, begin.data(), tb_bytes);
+    if ((e = cudaMemcpyAsync(d_opts_.p, h_opts_.p, sizeof(McOption) * (size_t)n, cudaMemcpyHostToDevice, stream_)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(d_tile_begin_.p, h_tile_begin_.p, tb_bytes, cudaMemcpyHostToDevice, stream_)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d_counter_.p, 0, sizeof(unsigned long long), stream_)) != cudaSuccess) return e;
+    counter_ready_ = true;
+    if (persistent_) {
+        max_ctas_ = max_resident_ctas(-1, cfg.block, 0, device_);
+        if (max_ctas_ <= 0) return cudaErrorInvalidConfiguration;
+    } else {
+        max_ctas_ = std::numeric_limits<int32_t>::max();
+    }
+    cfg_ = cfg;
+    return cudaSuccess;
+}
+
+cudaError_t Plan::launch_all(cudaStream_t st, bool timing) {
+    SimArgs a;
+    a.opts = static_cast<const McOption*>(d_opts_.p);
+    a.tile_begin = static_cast<const int64_t*>(d_tile_begin_.p);
+    a.n = n_;
+    a.n_tiles = n_tiles_;
+    a.partials = static_cast<TilePartial*>(d_partials_.p);
+    a.max_ctas = max_ctas_;
+    unsigned long long* counter = static_cast<unsigned long long*>(d_counter_.p);
+    cudaError_t e = cudaSuccess;
+    if (timing && (e = cudaEventRecord(ev0_, st)) != cudaSuccess) return e;
+    if (n_tiles_ > 0) {
+        if (persistent_)
+            e = launch_persistent(cfg_.block, a, counter, st);
+        else
+            e = launch_simulate(family_, anti_, cfg_.block, cfg_.upt, a, st);
+        if (e != cudaSuccess) return e;
+    }
+    if (timing && (e = cudaEventRecord(ev1_, st)) != cudaSuccess) return e;
+    return launch_finalize(a.opts, n_, a.partials, d_price(), d_se(), persistent_ ? counter : nullptr, st);
+}
+
+cudaError_t Plan::capture_graph() {
+    drop_graph();
+    cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    cudaError_t le = launch_all(stream_, false);
+    e = cudaStreamEndCapture(stream_, &graph_);
+    if (le != cudaSuccess) return le;
+    if (e != cudaSuccess) return e;
+    return cudaGraphInstantiate(&graph_exec_, graph_, 0);
+}
+
+cudaError_t Plan::execute(cudaStream_t stream) {
+    if (device_ < 0) return cudaErrorInvalidResourceHandle;
+    DeviceGuard g(device_);
+    cudaStream_t st = stream ? stream : stream_;
+    if (stream && stream != stream_) {
+        // Order this execute after the plan's own uploads.
+        cudaEvent_t ready;
+        cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+        cudaEventRecord(ready, stream_);
+        cudaStreamWaitEvent(st, ready, 0);
+        cudaEventDestroy(ready);
+    }
+    const bool timing = (flags_ & kFlagTiming) != 0;
+    cudaError_t e;
+    if (flags_ & kFlagGraph) {
+        if (!graph_exec_) {
+            if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return e;
+            if ((e = capture_graph()) != cudaSuccess) return e;
+        }
+        if (timing) cudaEventRecord(ev0_, st);
+        e = cudaGraphLaunch(graph_exec_, st);
+        if (timing) cudaEventRecord(ev1_, st);
+    } else {
+        e = launch_all(st, timing);
+    }
+    if (e != cudaSuccess) return e;
+    last_stream_ = st;
+    return cudaSuccess;
+}
+
+cudaError_t Plan::results(double* out_price, double* out_se) {
+    if (device_ < 0) return cudaErrorInvalidResourceHandle;
+    DeviceGuard g(device_);
+    cudaStream_t st = last_stream_ ? last_stream_ : stream_;
+    const size_t bytes = sizeof(double) * (size_t)n_;
+    cudaError_t e;
+    if ((e = h_price_.ensure(bytes)) != cudaSuccess) return e;
+    if (out_se && (e = h_se_.ensure(bytes)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(h_price_.p, d_price_.p, bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if (out_se && (e = cudaMemcpyAsync(h_se_.p, d_se_.p, bytes, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    std::memcpy(out_price, h_price_.p, bytes);
+    if (out_se) std::memcpy(out_se, h_se_.p, bytes);
+    if (flags_ & kFlagTiming) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ev0_, ev1_) == cudaSuccess) last_ms_ = ms;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Plan::sync_stats() {
+    if (device_ < 0) return cudaErrorInvalidResourceHandle;
+    DeviceGuard g(device_);
+    if (!(flags_ & kFlagTiming)) return cudaSuccess;
+    cudaError_t e = cudaEventSynchronize(ev1_);
+    if (e != cudaSuccess) return e;
+    float ms = 0.0f;
+    e = cudaEventElapsedTime(&ms, ev0_, ev1_);
+    if (e == cudaSuccess) last_ms_ = ms;
+    return e;
+}
+
+// Times every candidate launch shape on this plan (one warm-up and one timed
+// run each) and keeps the fastest.  Tile geometry follows the shape, so the
+// plan is re-laid-out per candidate; per-path results do not change.
+cudaError_t Plan::autotune() {
+    std::vector<LaunchConfig> cands;
+    if (persistent_) {
+        cands = {LaunchConfig{128, 0}, LaunchConfig{256, 0}};
+    } else {
+        for (int b : {128, 256})
+            for (int u : {1, 2, 4}) cands.push_back(LaunchConfig{b, u});
+    }
+    LaunchConfig best = cfg_;
+    float best_ms = std::numeric_limits<float>::max();
+    cudaError_t e;
+    for (const LaunchConfig& c : cands) {
+        if ((e = layout_tiles(c)) != cudaSuccess) return e;
+        for (int rep = 0; rep < 2; ++rep) {
+            if ((e = launch_all(stream_, true)) != cudaSuccess) return e;
+        }
+        if ((e = cudaEventSynchronize(ev1_)) != cudaSuccess) return e;
+        float ms = 0.0f;
+        if ((e = cudaEventElapsedTime(&ms, ev0_, ev1_)) != cudaSuccess) return e;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    return layout_tiles(best);
+}
+
+// ----------------------------------------------------------------------------
+Plan* thread_scratch_plan(int device) {
+    thread_local std::map<int, std::unique_ptr<Plan>> plans;
+    auto& p = plans[device];
+    if (!p) p.reset(new Plan());
+    return p.get();
+}
+
+}  // namespace qkb

@@ -1,0 +1,124 @@
+// mc_plan.h -- host runtime of the Monte Carlo path: batch validation and
+// packing, device buffers, launches, CUDA graphs and the autotuner.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "mc_types.h"
+
+namespace qkb {
+
+// SoA view of one batch in host memory (any field a model does not use may be
+// null when no option of that model is present).
+struct BatchInput {
+    const int32_t* model = nullptr;  // null: every option uses `uniform_model`
+    int32_t uniform_model = 0;
+    const double *spot = nullptr, *strike = nullptr, *t = nullptr, *vol = nullptr, *r = nullptr,
+                 *q = nullptr;
+    const double *v0 = nullptr, *kappa = nullptr, *theta = nullptr, *sigma = nullptr,
+                 *rho = nullptr;
+    const int32_t *option_type = nullptr, *paths = nullptr, *steps = nullptr;
+    const uint64_t* seed = nullptr;
+    int32_t n = 0;
+};
+
+enum : int32_t {
+    kFlagPersistent = 0x1,
+    kFlagGraph = 0x2,
+    kFlagNoAntithetic = 0x4,
+    kFlagTiming = 0x8,
+    kFlagAutotune = 0x10,
+};
+
+// Grow-only device / pinned host allocations.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+struct PinnedBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t bytes);
+    void release();
+};
+
+struct LaunchConfig {
+    int block = 256;
+    int upt = 2;
+};
+
+class Plan {
+public:
+    Plan() = default;
+    ~Plan();
+    Plan(const Plan&) = delete;
+    Plan& operator=(const Plan&) = delete;
+
+    // Validates and packs `in`, uploads it.  Returns a CUDA error (or
+    // cudaErrorInvalidValue with `err` set for a bad input set).
+    cudaError_t build(const BatchInput& in, int32_t flags, std::string* err);
+    cudaError_t execute(cudaStream_t stream);
+    cudaError_t results(double* out_price, double* out_se);
+    cudaError_t release();
+    // Waits for the last execute and refreshes last_simulate_ms().
+    cudaError_t sync_stats();
+
+    int32_t n() const { return n_; }
+    int64_t n_tiles() const { return n_tiles_; }
+    int64_t path_steps() const { return path_steps_; }
+    double last_simulate_ms() const { return last_ms_; }
+    int launches() const { return (n_tiles_ > 0 ? 1 : 0) + 1; }
+    int block() const { return cfg_.block; }
+    int upt() const { return cfg_.upt; }
+    int ctas() const { return max_ctas_; }
+    bool persistent() const { return persistent_; }
+    double* d_price() const { return static_cast<double*>(d_price_.p); }
+    double* d_se() const { return static_cast<double*>(d_se_.p); }
+    int device() const { return device_; }
+
+private:
+    cudaError_t ensure_stream();
+    cudaError_t layout_tiles(const LaunchConfig& cfg);  // tile geometry + upload
+    cudaError_t launch_all(cudaStream_t st, bool timing);
+    cudaError_t autotune();
+    cudaError_t capture_graph();
+    void drop_graph();
+
+    int device_ = -1;
+    cudaStream_t stream_ = nullptr;
+    cudaStream_t last_stream_ = nullptr;
+    int32_t flags_ = 0;
+    int32_t n_ = 0;
+    int64_t n_tiles_ = 0;
+    int64_t path_steps_ = 0;
+    int family_ = -1;  // single family of all simulated options, or -1 (mixed / none)
+    bool anti_ = true;
+    bool persistent_ = false;
+    LaunchConfig cfg_;
+    int max_ctas_ = 0;
+    double last_ms_ = 0.0;
+    bool counter_ready_ = false;
+
+    std::vector<McOption> opts_;       // host copy (units/tiles filled per layout)
+    DevBuf d_opts_, d_tile_begin_, d_partials_, d_price_, d_se_, d_counter_;
+    PinnedBuf h_opts_, h_tile_begin_, h_price_, h_se_;
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    cudaGraph_t graph_ = nullptr;
+    cudaGraphExec_t graph_exec_ = nullptr;
+};
+
+// Per-thread, per-device scratch plan used by the one-shot batch calls.
+Plan* thread_scratch_plan(int device);
+
+// Default launch shape per family, and the autotuner's cached choice.
+LaunchConfig default_config(int family);
+bool tuned_config(const std::string& key, LaunchConfig* out);
+void store_tuned_config(const std::string& key, const LaunchConfig& cfg);
+
+}  // namespace qkb

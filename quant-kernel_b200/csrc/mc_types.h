@@ -1,0 +1,66 @@
+// mc_types.h -- plain data shared by the host runtime and the kernels.
+#pragma once
+
+#include <cstdint>
+
+namespace qkb {
+
+// ---------------------------------------------------------------------------
+// Model codes (same values as QK_MC_* in include/qk_api.h).
+// ---------------------------------------------------------------------------
+enum : int32_t {
+    kStandard = 0,
+    kAntithetic = 1,
+    kEuler = 2,
+    kMilstein = 3,
+    kLocalVol = 4,
+    kTerminalPlain = 5,
+    kHeston = 6,
+    kNumModels = 7
+};
+
+enum : int32_t { kModeSimulate = 0, kModeConstant = 1 };
+
+// ---------------------------------------------------------------------------
+// Option record: 128 bytes, packed on the host, read once per tile.
+//
+// Model constants (FP32, rounded from FP64 host values):
+//   terminal (0,1,5):  p0 = (r - q - vol^2/2) t     p1 = vol sqrt(t)
+//   Euler/LV (2,4):    p0 = (r - q) dt               p1 = vol sqrt(dt)
+//                      p2 = 1e-12 / spot (floor of S/spot)
+//   Milstein (3):      p0 = (r - q) dt - c           p1 = vol sqrt(dt)
+//                      p2 = 1e-12 / spot             p3 = c = vol^2 dt / 2
+//   Heston (6):        p0 = (r - q) dt   p1 = dt/2   p2 = sqrt(dt)
+//                      p3 = kappa dt     p4 = kappa theta dt
+//                      p5 = sigma sqrt(dt)           p6 = rho
+//                      p7 = sqrt(max(1 - rho^2, 0))  p8 = v0
+//                      p9 = log(1e-12 / spot) (floor of log(S/spot))
+// ---------------------------------------------------------------------------
+struct alignas(16) McOption {
+    double spot;
+    double strike;
+    double disc;         // exp(-r t)
+    double const_price;  // result when mode == kModeConstant
+    uint64_t seed;
+    int64_t tile_begin;  // first tile of this option in the plan
+    int32_t tiles;       // tiles of this option (0 when constant)
+    int32_t model;
+    int32_t option_type;
+    int32_t paths;
+    int32_t steps;
+    int32_t units;       // antithetic: ceil(paths/2) pairs; plain: paths
+    int32_t samples;     // standard-error samples: full pairs or paths
+    int32_t unit_iters;  // per-thread passes over the tile
+    int32_t mode;
+    int32_t antithetic;
+    float p[10];
+};
+static_assert(sizeof(McOption) == 128, "McOption layout");
+
+// Per-tile partial sums: y = pair mean (antithetic) or payoff (plain).
+struct alignas(16) TilePartial {
+    double sy_hi, sy_lo;  // sum of y
+    double q_hi, q_lo;    // sum of y^2 over full samples
+};
+
+}  // namespace qkb

@@ -1,0 +1,513 @@
+// qk_api.cpp -- extern "C" boundary of libqk_b200.so.
+//
+// Error machinery restates yluoc/Quant-Kernel cpp/src/qk_api.cpp:19-117: a
+// thread-local 256-byte message, "null pointer: <param>" for the first null
+// argument in declaration order (QK_ERR_NULL_PTR), checked before the size,
+// then "bad batch size: <n>" for n <= 0 (QK_ERR_BAD_SIZE).  Invalid elements
+// get NaN and the call still returns QK_OK.  CUDA failures, which have no
+// reference counterpart, return QK_ERR_RUNTIME_INIT with "cuda error: ...".
+#include "../../include/qk_api.h"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "mc_plan.h"
+
+namespace {
+
+thread_local char tl_error_msg[256] = "";
+
+void set_error_msg(const char* msg) {
+    std::strncpy(tl_error_msg, msg, sizeof(tl_error_msg) - 1);
+    tl_error_msg[sizeof(tl_error_msg) - 1] = '\0';
+}
+
+void set_error_fmt(const char* fmt, ...) {
+    char buf[256];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    set_error_msg(buf);
+}
+
+int32_t fail_null(const char* name) {
+    set_error_fmt("null pointer: %s", name);
+    return QK_ERR_NULL_PTR;
+}
+
+int32_t fail_size(int32_t n) {
+    set_error_fmt("bad batch size: %d", n);
+    return QK_ERR_BAD_SIZE;
+}
+
+int32_t fail_cuda(cudaError_t e, const char* where) {
+    set_error_fmt("cuda error: %s (%s) in %s", cudaGetErrorName(e), cudaGetErrorString(e), where);
+    return QK_ERR_RUNTIME_INIT;
+}
+
+struct NamedPtr {
+    const void* p;
+    const char* name;
+};
+
+// First null pointer in declaration order, as QK_BATCH_NULL_CHECK does.
+template <size_t N>
+int32_t check_nulls(const NamedPtr (&ptrs)[N]) {
+    for (size_t i = 0; i < N; ++i)
+        if (!ptrs[i].p) return fail_null(ptrs[i].name);
+    return QK_OK;
+}
+
+const QKPluginAPI k_plugin_api = {QK_ABI_MAJOR, QK_ABI_MINOR, "quantkernel.b200.mcm.v1"};
+
+double nan_value() { return std::numeric_limits<double>::quiet_NaN(); }
+
+// Runs one batch through the calling thread's scratch plan.
+int32_t run_batch(const qkb::BatchInput& in, int32_t flags, double* out_prices, double* out_se,
+                  const char* where) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail_cuda(e, where);
+    qkb::Plan* plan = qkb::thread_scratch_plan(dev);
+    std::string err;
+    if ((e = plan->build(in, flags, &err)) != cudaSuccess) return fail_cuda(e, where);
+    if ((e = plan->execute(nullptr)) != cudaSuccess) return fail_cuda(e, where);
+    if ((e = plan->results(out_prices, out_se)) != cudaSuccess) return fail_cuda(e, where);
+    return QK_OK;
+}
+
+qkb::BatchInput bsm_input(int32_t model, const double* spot, const double* strike, const double* t,
+                          const double* vol, const double* r, const double* q,
+                          const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+                          const uint64_t* seed, int32_t n) {
+    qkb::BatchInput in;
+    in.uniform_model = model;
+    in.spot = spot;
+    in.strike = strike;
+    in.t = t;
+    in.vol = vol;
+    in.r = r;
+    in.q = q;
+    in.option_type = option_type;
+    in.paths = paths;
+    in.steps = steps;
+    in.seed = seed;
+    in.n = n;
+    return in;
+}
+
+qkb::BatchInput heston_input(const double* spot, const double* strike, const double* t,
+                             const double* r, const double* q, const double* v0,
+                             const double* kappa, const double* theta, const double* sigma,
+                             const double* rho, const int32_t* option_type, const int32_t* paths,
+                             const int32_t* steps, const uint64_t* seed, int32_t n) {
+    qkb::BatchInput in;
+    in.uniform_model = qkb::kHeston;
+    in.spot = spot;
+    in.strike = strike;
+    in.t = t;
+    in.r = r;
+    in.q = q;
+    in.v0 = v0;
+    in.kappa = kappa;
+    in.theta = theta;
+    in.sigma = sigma;
+    in.rho = rho;
+    in.option_type = option_type;
+    in.paths = paths;
+    in.steps = steps;
+    in.seed = seed;
+    in.n = n;
+    return in;
+}
+
+// Terminal models: (spot, strike, t, vol, r, q, option_type, paths, seed).
+int32_t terminal_batch(int32_t model, const double* spot, const double* strike, const double* t,
+                       const double* vol, const double* r, const double* q,
+                       const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+                       int32_t n, double* out_prices, double* out_se, bool want_se,
+                       const char* where) {
+    if (want_se) {
+        const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {vol, "vol"},
+                                 {r, "r"}, {q, "q"}, {option_type, "option_type"},
+                                 {paths, "paths"}, {seed, "seed"}, {out_prices, "out_prices"},
+                                 {out_se, "out_stderr"}};
+        if (int32_t rc = check_nulls(ptrs)) return rc;
+    } else {
+        const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {vol, "vol"},
+                                 {r, "r"}, {q, "q"}, {option_type, "option_type"},
+                                 {paths, "paths"}, {seed, "seed"}, {out_prices, "out_prices"}};
+        if (int32_t rc = check_nulls(ptrs)) return rc;
+    }
+    if (n <= 0) return fail_size(n);
+    return run_batch(bsm_input(model, spot, strike, t, vol, r, q, option_type, paths, nullptr, seed, n),
+                     0, out_prices, out_se, where);
+}
+
+// One-factor stepwise models: (..., option_type, paths, steps, seed).
+int32_t stepwise_batch(int32_t model, const double* spot, const double* strike, const double* t,
+                       const double* vol, const double* r, const double* q,
+                       const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+                       const uint64_t* seed, int32_t n, double* out_prices, double* out_se,
+                       bool want_se, const char* where) {
+    if (want_se) {
+        const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {vol, "vol"},
+                                 {r, "r"}, {q, "q"}, {option_type, "option_type"},
+                                 {paths, "paths"}, {steps, "steps"}, {seed, "seed"},
+                                 {out_prices, "out_prices"}, {out_se, "out_stderr"}};
+        if (int32_t rc = check_nulls(ptrs)) return rc;
+    } else {
+        const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {vol, "vol"},
+                                 {r, "r"}, {q, "q"}, {option_type, "option_type"},
+                                 {paths, "paths"}, {steps, "steps"}, {seed, "seed"},
+                                 {out_prices, "out_prices"}};
+        if (int32_t rc = check_nulls(ptrs)) return rc;
+    }
+    if (n <= 0) return fail_size(n);
+    return run_batch(bsm_input(model, spot, strike, t, vol, r, q, option_type, paths, steps, seed, n),
+                     0, out_prices, out_se, where);
+}
+
+int32_t heston_batch(const double* spot, const double* strike, const double* t, const double* r,
+                     const double* q, const double* v0, const double* kappa, const double* theta,
+                     const double* sigma, const double* rho, const int32_t* option_type,
+                     const int32_t* paths, const int32_t* steps, const uint64_t* seed, int32_t n,
+                     double* out_prices, double* out_se, bool want_se, const char* where) {
+    if (want_se) {
+        const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {r, "r"},
+                                 {q, "q"}, {v0, "v0"}, {kappa, "kappa"}, {theta, "theta"},
+                                 {sigma, "sigma"}, {rho, "rho"}, {option_type, "option_type"},
+                                 {paths, "paths"}, {steps, "steps"}, {seed, "seed"},
+                                 {out_prices, "out_prices"}, {out_se, "out_stderr"}};
+        if (int32_t rc = check_nulls(ptrs)) return rc;
+    } else {
+        const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {r, "r"},
+                                 {q, "q"}, {v0, "v0"}, {kappa, "kappa"}, {theta, "theta"},
+                                 {sigma, "sigma"}, {rho, "rho"}, {option_type, "option_type"},
+                                 {paths, "paths"}, {steps, "steps"}, {seed, "seed"},
+                                 {out_prices, "out_prices"}};
+        if (int32_t rc = check_nulls(ptrs)) return rc;
+    }
+    if (n <= 0) return fail_size(n);
+    return run_batch(heston_input(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                                  paths, steps, seed, n),
+                     0, out_prices, out_se, where);
+}
+
+// Mixed-model input: checks the arrays that the present models need.
+int32_t mixed_input(const int32_t* model, const double* spot, const double* strike,
+                    const double* t, const double* vol, const double* r, const double* q,
+                    const double* v0, const double* kappa, const double* theta,
+                    const double* sigma, const double* rho, const int32_t* option_type,
+                    const int32_t* paths, const int32_t* steps, const uint64_t* seed, int32_t n,
+                    qkb::BatchInput* in) {
+    const NamedPtr base[] = {{model, "model"}, {spot, "spot"}, {strike, "strike"}, {t, "t"},
+                             {r, "r"}, {q, "q"}, {option_type, "option_type"}, {paths, "paths"},
+                             {seed, "seed"}};
+    if (int32_t rc = check_nulls(base)) return rc;
+    if (n <= 0) return fail_size(n);
+    bool need_vol = false, need_heston = false, need_steps = false;
+    for (int32_t i = 0; i < n; ++i) {
+        const int32_t m = model[i];
+        if (m >= qkb::kStandard && m <= qkb::kTerminalPlain) need_vol = true;
+        if (m == qkb::kEuler || m == qkb::kMilstein || m == qkb::kLocalVol || m == qkb::kHeston)
+            need_steps = true;
+        if (m == qkb::kHeston) need_heston = true;
+    }
+    if (need_vol && !vol) return fail_null("vol");
+    if (need_heston) {
+        const NamedPtr hp[] = {{v0, "v0"}, {kappa, "kappa"}, {theta, "theta"}, {sigma, "sigma"},
+                               {rho, "rho"}};
+        if (int32_t rc = check_nulls(hp)) return rc;
+    }
+    if (need_steps && !steps) return fail_null("steps");
+    in->model = model;
+    in->spot = spot;
+    in->strike = strike;
+    in->t = t;
+    in->vol = vol;
+    in->r = r;
+    in->q = q;
+    in->v0 = v0;
+    in->kappa = kappa;
+    in->theta = theta;
+    in->sigma = sigma;
+    in->rho = rho;
+    in->option_type = option_type;
+    in->paths = paths;
+    in->steps = steps;
+    in->seed = seed;
+    in->n = n;
+    return QK_OK;
+}
+
+}  // namespace
+
+struct qk_mc_plan {
+    qkb::Plan plan;
+};
+
+extern "C" {
+
+void qk_abi_version(int32_t* major, int32_t* minor) {
+    if (major) *major = QK_ABI_MAJOR;
+    if (minor) *minor = QK_ABI_MINOR;
+}
+
+int32_t qk_plugin_get_api(int32_t host_abi_major, int32_t host_abi_minor,
+                          const QKPluginAPI** out_api) {
+    if (!out_api) return QK_ERR_NULL_PTR;
+    if (host_abi_major != QK_ABI_MAJOR || host_abi_minor > QK_ABI_MINOR) {
+        *out_api = nullptr;
+        return QK_ERR_ABI_MISMATCH;
+    }
+    *out_api = &k_plugin_api;
+    return QK_OK;
+}
+
+const char* qk_get_last_error(void) { return tl_error_msg; }
+
+int32_t qk_set_device(int32_t device) {
+    cudaError_t e = cudaSetDevice(device);
+    return e == cudaSuccess ? QK_OK : fail_cuda(e, "qk_set_device");
+}
+
+int32_t qk_get_device(int32_t* device) {
+    if (!device) return fail_null("device");
+    int d = -1;
+    cudaError_t e = cudaGetDevice(&d);
+    if (e != cudaSuccess) return fail_cuda(e, "qk_get_device");
+    *device = d;
+    return QK_OK;
+}
+
+void qk_clear_last_error(void) { tl_error_msg[0] = '\0'; }
+
+// ---- terminal ---------------------------------------------------------------
+int32_t qk_mcm_standard_monte_carlo_price_batch(const double* spot, const double* strike,
+                                                const double* t, const double* vol,
+                                                const double* r, const double* q,
+                                                const int32_t* option_type, const int32_t* paths,
+                                                const uint64_t* seed, int32_t n,
+                                                double* out_prices) {
+    return terminal_batch(qkb::kStandard, spot, strike, t, vol, r, q, option_type, paths, seed, n,
+                          out_prices, nullptr, false, "qk_mcm_standard_monte_carlo_price_batch");
+}
+
+int32_t qk_mcm_standard_monte_carlo_price_se_batch(const double* spot, const double* strike,
+                                                   const double* t, const double* vol,
+                                                   const double* r, const double* q,
+                                                   const int32_t* option_type,
+                                                   const int32_t* paths, const uint64_t* seed,
+                                                   int32_t n, double* out_prices,
+                                                   double* out_stderr) {
+    return terminal_batch(qkb::kStandard, spot, strike, t, vol, r, q, option_type, paths, seed, n,
+                          out_prices, out_stderr, true,
+                          "qk_mcm_standard_monte_carlo_price_se_batch");
+}
+
+double qk_mcm_standard_monte_carlo_price(double spot, double strike, double t, double vol,
+                                         double r, double q, int32_t option_type, int32_t paths,
+                                         uint64_t seed) {
+    double out = nan_value();
+    if (qk_mcm_standard_monte_carlo_price_batch(&spot, &strike, &t, &vol, &r, &q, &option_type,
+                                                &paths, &seed, 1, &out) != QK_OK)
+        return nan_value();
+    return out;
+}
+
+int32_t qk_mcm_antithetic_variates_price_batch(const double* spot, const double* strike,
+                                               const double* t, const double* vol,
+                                               const double* r, const double* q,
+                                               const int32_t* option_type, const int32_t* paths,
+                                               const uint64_t* seed, int32_t n,
+                                               double* out_prices) {
+    return terminal_batch(qkb::kAntithetic, spot, strike, t, vol, r, q, option_type, paths, seed,
+                          n, out_prices, nullptr, false, "qk_mcm_antithetic_variates_price_batch");
+}
+
+int32_t qk_mcm_antithetic_variates_price_se_batch(const double* spot, const double* strike,
+                                                  const double* t, const double* vol,
+                                                  const double* r, const double* q,
+                                                  const int32_t* option_type,
+                                                  const int32_t* paths, const uint64_t* seed,
+                                                  int32_t n, double* out_prices,
+                                                  double* out_stderr) {
+    return terminal_batch(qkb::kAntithetic, spot, strike, t, vol, r, q, option_type, paths, seed,
+                          n, out_prices, out_stderr, true,
+                          "qk_mcm_antithetic_variates_price_se_batch");
+}
+
+double qk_mcm_antithetic_variates_price(double spot, double strike, double t, double vol,
+                                        double r, double q, int32_t option_type, int32_t paths,
+                                        uint64_t seed) {
+    double out = nan_value();
+    if (qk_mcm_antithetic_variates_price_batch(&spot, &strike, &t, &vol, &r, &q, &option_type,
+                                               &paths, &seed, 1, &out) != QK_OK)
+        return nan_value();
+    return out;
+}
+
+// ---- one-factor stepwise -----------------------------------------------------
+#define QK_STEPWISE_ENTRY(NAME, MODEL)                                                           \
+    int32_t qk_mcm_##NAME##_price_batch(const double* spot, const double* strike,               \
+                                        const double* t, const double* vol, const double* r,    \
+                                        const double* q, const int32_t* option_type,            \
+                                        const int32_t* paths, const int32_t* steps,             \
+                                        const uint64_t* seed, int32_t n, double* out_prices) {  \
+        return stepwise_batch(MODEL, spot, strike, t, vol, r, q, option_type, paths, steps, seed, \
+                              n, out_prices, nullptr, false, "qk_mcm_" #NAME "_price_batch");   \
+    }                                                                                           \
+    int32_t qk_mcm_##NAME##_price_se_batch(const double* spot, const double* strike,            \
+                                           const double* t, const double* vol,                  \
+                                           const double* r, const double* q,                    \
+                                           const int32_t* option_type, const int32_t* paths,    \
+                                           const int32_t* steps, const uint64_t* seed,          \
+                                           int32_t n, double* out_prices, double* out_stderr) { \
+        return stepwise_batch(MODEL, spot, strike, t, vol, r, q, option_type, paths, steps, seed, \
+                              n, out_prices, out_stderr, true,                                  \
+                              "qk_mcm_" #NAME "_price_se_batch");                               \
+    }                                                                                           \
+    double qk_mcm_##NAME##_price(double spot, double strike, double t, double vol, double r,    \
+                                 double q, int32_t option_type, int32_t paths, int32_t steps,   \
+                                 uint64_t seed) {                                               \
+        double out = nan_value();                                                               \
+        if (qk_mcm_##NAME##_price_batch(&spot, &strike, &t, &vol, &r, &q, &option_type, &paths,  \
+                                        &steps, &seed, 1, &out) != QK_OK)                       \
+            return nan_value();                                                                 \
+        return out;                                                                             \
+    }
+
+QK_STEPWISE_ENTRY(euler_maruyama, qkb::kEuler)
+QK_STEPWISE_ENTRY(milstein, qkb::kMilstein)
+QK_STEPWISE_ENTRY(local_vol_monte_carlo, qkb::kLocalVol)
+#undef QK_STEPWISE_ENTRY
+
+// ---- Heston --------------------------------------------------------------------
+int32_t qk_mcm_heston_monte_carlo_price_batch(const double* spot, const double* strike,
+                                              const double* t, const double* r, const double* q,
+                                              const double* v0, const double* kappa,
+                                              const double* theta, const double* sigma,
+                                              const double* rho, const int32_t* option_type,
+                                              const int32_t* paths, const int32_t* steps,
+                                              const uint64_t* seed, int32_t n,
+                                              double* out_prices) {
+    return heston_batch(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type, paths,
+                        steps, seed, n, out_prices, nullptr, false,
+                        "qk_mcm_heston_monte_carlo_price_batch");
+}
+
+int32_t qk_mcm_heston_monte_carlo_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr) {
+    return heston_batch(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type, paths,
+                        steps, seed, n, out_prices, out_stderr, true,
+                        "qk_mcm_heston_monte_carlo_price_se_batch");
+}
+
+double qk_mcm_heston_monte_carlo_price(double spot, double strike, double t, double r, double q,
+                                       double v0, double kappa, double theta, double sigma,
+                                       double rho, int32_t option_type, int32_t paths,
+                                       int32_t steps, uint64_t seed) {
+    double out = nan_value();
+    if (qk_mcm_heston_monte_carlo_price_batch(&spot, &strike, &t, &r, &q, &v0, &kappa, &theta,
+                                              &sigma, &rho, &option_type, &paths, &steps, &seed,
+                                              1, &out) != QK_OK)
+        return nan_value();
+    return out;
+}
+
+// ---- mixed batch and plans -------------------------------------------------------
+int32_t qk_mcm_mixed_price_batch(const int32_t* model, const double* spot, const double* strike,
+                                 const double* t, const double* vol, const double* r,
+                                 const double* q, const double* v0, const double* kappa,
+                                 const double* theta, const double* sigma, const double* rho,
+                                 const int32_t* option_type, const int32_t* paths,
+                                 const int32_t* steps, const uint64_t* seed, int32_t n,
+                                 double* out_prices, double* out_stderr) {
+    qkb::BatchInput in;
+    int32_t rc = mixed_input(model, spot, strike, t, vol, r, q, v0, kappa, theta, sigma, rho,
+                             option_type, paths, steps, seed, n, &in);
+    if (rc != QK_OK) return rc;
+    if (!out_prices) return fail_null("out_prices");
+    return run_batch(in, qkb::kFlagPersistent, out_prices, out_stderr, "qk_mcm_mixed_price_batch");
+}
+
+int32_t qk_mcm_plan_create(const int32_t* model, const double* spot, const double* strike,
+                           const double* t, const double* vol, const double* r, const double* q,
+                           const double* v0, const double* kappa, const double* theta,
+                           const double* sigma, const double* rho, const int32_t* option_type,
+                           const int32_t* paths, const int32_t* steps, const uint64_t* seed,
+                           int32_t n, int32_t flags, qk_mc_plan** out_plan) {
+    if (!out_plan) return fail_null("out_plan");
+    *out_plan = nullptr;
+    qkb::BatchInput in;
+    int32_t rc = mixed_input(model, spot, strike, t, vol, r, q, v0, kappa, theta, sigma, rho,
+                             option_type, paths, steps, seed, n, &in);
+    if (rc != QK_OK) return rc;
+    qk_mc_plan* p = new qk_mc_plan();
+    std::string err;
+    cudaError_t e = p->plan.build(in, flags, &err);
+    if (e != cudaSuccess) {
+        delete p;
+        return fail_cuda(e, "qk_mcm_plan_create");
+    }
+    *out_plan = p;
+    return QK_OK;
+}
+
+int32_t qk_mcm_plan_execute(qk_mc_plan* plan, void* stream) {
+    if (!plan) return fail_null("plan");
+    cudaError_t e = plan->plan.execute(static_cast<cudaStream_t>(stream));
+    return e == cudaSuccess ? QK_OK : fail_cuda(e, "qk_mcm_plan_execute");
+}
+
+int32_t qk_mcm_plan_results(qk_mc_plan* plan, double* out_prices, double* out_stderr) {
+    if (!plan) return fail_null("plan");
+    if (!out_prices) return fail_null("out_prices");
+    cudaError_t e = plan->plan.results(out_prices, out_stderr);
+    return e == cudaSuccess ? QK_OK : fail_cuda(e, "qk_mcm_plan_results");
+}
+
+int32_t qk_mcm_plan_device_results(qk_mc_plan* plan, double** d_prices, double** d_stderr) {
+    if (!plan) return fail_null("plan");
+    if (d_prices) *d_prices = plan->plan.d_price();
+    if (d_stderr) *d_stderr = plan->plan.d_se();
+    return QK_OK;
+}
+
+int32_t qk_mcm_plan_stats(qk_mc_plan* plan, double* simulate_ms, int32_t* launches,
+                          int64_t* path_steps) {
+    if (!plan) return fail_null("plan");
+    cudaError_t e = plan->plan.sync_stats();
+    if (e != cudaSuccess) return fail_cuda(e, "qk_mcm_plan_stats");
+    if (simulate_ms) *simulate_ms = plan->plan.last_simulate_ms();
+    if (launches) *launches = plan->plan.launches();
+    if (path_steps) *path_steps = plan->plan.path_steps();
+    return QK_OK;
+}
+
+int32_t qk_mcm_plan_config(qk_mc_plan* plan, int32_t* block, int32_t* units_per_thread,
+                           int32_t* ctas) {
+    if (!plan) return fail_null("plan");
+    if (block) *block = plan->plan.block();
+    if (units_per_thread) *units_per_thread = plan->plan.upt();
+    if (ctas) *ctas = plan->plan.ctas();
+    return QK_OK;
+}
+
+int32_t qk_mcm_plan_destroy(qk_mc_plan* plan) {
+    if (!plan) return QK_OK;
+    delete plan;
+    return QK_OK;
+}
+
+}  // extern "C"

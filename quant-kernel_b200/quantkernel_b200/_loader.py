@@ -1,0 +1,135 @@
+"""Finds libqk_b200.so, binds its C ABI and verifies the ABI version.
+
+Mirrors yluoc/Quant-Kernel python/quantkernel/_loader.py:91-363 (search path,
+eager binding, ABI negotiation) for the Monte Carlo subset this library
+exports.  The search order is ``QK_B200_LIB_PATH``, then this package's
+directory.  There is no fallback: a missing library raises ``OSError``.
+"""
+
+import ctypes as ct
+import os
+from pathlib import Path
+
+from ._abi import ABI_MAJOR, ABI_MINOR, QK_OK
+
+D = ct.c_double
+I32 = ct.c_int32
+I64 = ct.c_int64
+U64 = ct.c_uint64
+PD = ct.POINTER(ct.c_double)
+PI32 = ct.POINTER(ct.c_int32)
+PI64 = ct.POINTER(ct.c_int64)
+PU64 = ct.POINTER(ct.c_uint64)
+VP = ct.c_void_p
+
+LIB_NAME = "libqk_b200.so"
+
+
+class QKPluginAPI(ct.Structure):
+    _fields_ = [
+        ("abi_major", I32),
+        ("abi_minor", I32),
+        ("plugin_name", ct.c_char_p),
+    ]
+
+
+_term_scalar = [D, D, D, D, D, D, I32, I32, U64]
+_term_batch = [PD, PD, PD, PD, PD, PD, PI32, PI32, PU64, I32, PD]
+_step_scalar = [D, D, D, D, D, D, I32, I32, I32, U64]
+_step_batch = [PD, PD, PD, PD, PD, PD, PI32, PI32, PI32, PU64, I32, PD]
+_hes_scalar = [D, D, D, D, D, D, D, D, D, D, I32, I32, I32, U64]
+_hes_batch = [PD] * 10 + [PI32, PI32, PI32, PU64, I32, PD]
+_mixed_arrays = [PI32] + [PD] * 11 + [PI32, PI32, PI32, PU64, I32]
+
+FUNCTION_SIGNATURES = [
+    ("qk_abi_version", None, [ct.POINTER(I32), ct.POINTER(I32)]),
+    ("qk_plugin_get_api", I32, [I32, I32, ct.POINTER(ct.POINTER(QKPluginAPI))]),
+    ("qk_get_last_error", ct.c_char_p, []),
+    ("qk_clear_last_error", None, []),
+    ("qk_set_device", I32, [I32]),
+    ("qk_get_device", I32, [PI32]),
+    ("qk_mcm_standard_monte_carlo_price", D, _term_scalar),
+    ("qk_mcm_standard_monte_carlo_price_batch", I32, _term_batch),
+    ("qk_mcm_standard_monte_carlo_price_se_batch", I32, _term_batch + [PD]),
+    ("qk_mcm_antithetic_variates_price", D, _term_scalar),
+    ("qk_mcm_antithetic_variates_price_batch", I32, _term_batch),
+    ("qk_mcm_antithetic_variates_price_se_batch", I32, _term_batch + [PD]),
+    ("qk_mcm_euler_maruyama_price", D, _step_scalar),
+    ("qk_mcm_euler_maruyama_price_batch", I32, _step_batch),
+    ("qk_mcm_euler_maruyama_price_se_batch", I32, _step_batch + [PD]),
+    ("qk_mcm_milstein_price", D, _step_scalar),
+    ("qk_mcm_milstein_price_batch", I32, _step_batch),
+    ("qk_mcm_milstein_price_se_batch", I32, _step_batch + [PD]),
+    ("qk_mcm_local_vol_monte_carlo_price", D, _step_scalar),
+    ("qk_mcm_local_vol_monte_carlo_price_batch", I32, _step_batch),
+    ("qk_mcm_local_vol_monte_carlo_price_se_batch", I32, _step_batch + [PD]),
+    ("qk_mcm_heston_monte_carlo_price", D, _hes_scalar),
+    ("qk_mcm_heston_monte_carlo_price_batch", I32, _hes_batch),
+    ("qk_mcm_heston_monte_carlo_price_se_batch", I32, _hes_batch + [PD]),
+    ("qk_mcm_mixed_price_batch", I32, _mixed_arrays + [PD, PD]),
+    ("qk_mcm_plan_create", I32, _mixed_arrays + [I32, ct.POINTER(VP)]),
+    ("qk_mcm_plan_execute", I32, [VP, VP]),
+    ("qk_mcm_plan_results", I32, [VP, PD, PD]),
+    ("qk_mcm_plan_device_results", I32, [VP, ct.POINTER(VP), ct.POINTER(VP)]),
+    ("qk_mcm_plan_stats", I32, [VP, PD, PI32, PI64]),
+    ("qk_mcm_plan_config", I32, [VP, PI32, PI32, PI32]),
+    ("qk_mcm_plan_destroy", I32, [VP]),
+]
+
+
+def search_dirs() -> list[Path]:
+    dirs: list[Path] = []
+    env = os.environ.get("QK_B200_LIB_PATH")
+    if env:
+        dirs.append(Path(env))
+    dirs.append(Path(__file__).resolve().parent)
+    return dirs
+
+
+def find_library() -> Path:
+    for d in search_dirs():
+        cand = d / LIB_NAME
+        if cand.exists():
+            return cand
+    raise OSError(
+        f"Cannot find {LIB_NAME}. Searched: {[str(d) for d in search_dirs()]}. "
+        "Build it with `make -C quant-kernel_b200/csrc` (or __graft_entry__.build()), "
+        "or set QK_B200_LIB_PATH."
+    )
+
+
+def configure(lib: ct.CDLL) -> None:
+    for name, restype, argtypes in FUNCTION_SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = restype
+        fn.argtypes = argtypes
+
+
+def verify_abi(lib: ct.CDLL) -> None:
+    major = ct.c_int32(-1)
+    minor = ct.c_int32(-1)
+    lib.qk_abi_version(ct.byref(major), ct.byref(minor))
+    if major.value != ABI_MAJOR:
+        raise RuntimeError(f"ABI major version mismatch: library={major.value}, expected={ABI_MAJOR}")
+    if minor.value < ABI_MINOR:
+        raise RuntimeError(f"ABI minor version too old: library={minor.value}, expected>={ABI_MINOR}")
+    api = ct.POINTER(QKPluginAPI)()
+    rc = lib.qk_plugin_get_api(ABI_MAJOR, ABI_MINOR, ct.byref(api))
+    if rc != QK_OK or not api:
+        raise RuntimeError(f"qk_plugin_get_api failed: rc={rc}")
+    if api.contents.abi_major != ABI_MAJOR or api.contents.abi_minor < ABI_MINOR:
+        raise RuntimeError("plugin API version mismatch")
+
+
+_LIB = None
+
+
+def load_library() -> ct.CDLL:
+    """Load libqk_b200.so once per process, bind every symbol and check the ABI."""
+    global _LIB
+    if _LIB is None:
+        lib = ct.CDLL(str(find_library()))
+        configure(lib)
+        verify_abi(lib)
+        _LIB = lib
+    return _LIB

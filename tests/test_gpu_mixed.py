@@ -1,0 +1,101 @@
+"""Mixed-model persistent launch, plans, CUDA graphs and the autotuner.
+
+A path's normals depend only on (seed, path index), and sums are compensated
+double-double in a fixed order, so every launch strategy must agree with the
+per-method batch calls to a relative 1e-13 (bit for bit when the tile
+geometry is the same)."""
+
+import numpy as np
+import pytest
+
+from quantkernel_b200 import (QK_MC_EULER, QK_MC_HESTON, QK_MC_LOCAL_VOL, QK_MC_MILSTEIN,
+                              QK_PLAN_AUTOTUNE, QK_PLAN_GRAPH, QK_PLAN_PERSISTENT,
+                              QK_PLAN_TIMING, workloads)
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_mixed(n=96, seed=5):
+    return workloads.mixed(n, seed=seed, log2_paths=(8.0, 14.0), log2_steps=(2.0, 6.0))
+
+
+def _per_method(qk, b):
+    out = np.empty(len(b["model"]))
+    se = np.empty_like(out)
+    bsm_keys = ("spot", "strike", "t", "vol", "r", "q", "option_type", "paths", "steps", "seed")
+    hes_keys = ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho",
+                "option_type", "paths", "steps", "seed")
+    for m, fn, keys in ((QK_MC_EULER, qk.euler_maruyama_price_se_batch, bsm_keys),
+                        (QK_MC_MILSTEIN, qk.milstein_price_se_batch, bsm_keys),
+                        (QK_MC_LOCAL_VOL, qk.local_vol_monte_carlo_price_se_batch, bsm_keys),
+                        (QK_MC_HESTON, qk.heston_monte_carlo_price_se_batch, hes_keys)):
+        idx = np.nonzero(b["model"] == m)[0]
+        p, s = fn(**{k: b[k][idx] for k in keys})
+        out[idx] = p
+        se[idx] = s
+    return out, se
+
+
+def test_mixed_batch_equals_per_method_calls(qk):
+    b = _small_mixed()
+    p, se = qk.mixed_price_batch(**b)
+    ref_p, ref_se = _per_method(qk, b)
+    np.testing.assert_allclose(p, ref_p, rtol=1e-13, atol=0)
+    np.testing.assert_allclose(se, ref_se, rtol=1e-10, atol=0)
+
+
+def test_plan_graph_persistent_autotune_agree(qk):
+    b = _small_mixed(64, seed=9)
+    base = qk.plan(**b)
+    base.execute()
+    p0, s0 = base.results()
+    for flags in (QK_PLAN_GRAPH, QK_PLAN_PERSISTENT | QK_PLAN_GRAPH | QK_PLAN_TIMING,
+                  QK_PLAN_AUTOTUNE, QK_PLAN_AUTOTUNE | QK_PLAN_GRAPH):
+        plan = qk.plan(**b, flags=flags)
+        for _ in range(3):  # graph replays are deterministic
+            plan.execute()
+            p, s = plan.results()
+            np.testing.assert_allclose(p, p0, rtol=1e-13, atol=0)
+        st = plan.stats()
+        assert st["launches"] == 2
+        plan.close()
+    base.close()
+
+
+def test_single_family_plan_persistent_equals_grid(qk):
+    h = workloads.heston(40, paths=4096, steps=24, seed=3)
+    model = np.full(40, QK_MC_HESTON, np.int32)
+    grid = qk.plan(model=model, **h)
+    pers = qk.plan(model=model, **h, flags=QK_PLAN_PERSISTENT)
+    grid.execute()
+    pers.execute()
+    a, _ = grid.results()
+    b, _ = pers.results()
+    np.testing.assert_array_equal(a, b)
+    plain, _ = qk.heston_monte_carlo_price_se_batch(**h)
+    np.testing.assert_array_equal(a, plain)
+
+
+def test_mixed_batch_with_invalid_and_constant_options(qk):
+    b = _small_mixed(16, seed=11)
+    b["spot"][3] = -1.0           # invalid -> NaN
+    b["t"][5] = 1e-14             # intrinsic
+    b["paths"][7] = 1             # invalid count -> NaN
+    b["model"][9] = 42            # unknown model -> NaN
+    p, se = qk.mixed_price_batch(**b)
+    assert np.isnan(p[3]) and np.isnan(p[7]) and np.isnan(p[9])
+    assert np.isfinite(p[5]) and np.isnan(se[5])
+    ok = [i for i in range(16) if i not in (3, 5, 7, 9)]
+    assert np.all(np.isfinite(p[ok])) and np.all(se[ok] > 0)
+
+
+def test_timing_stats_and_device_results(qk):
+    h = workloads.heston(16, paths=8192, steps=32, seed=4)
+    plan = qk.plan(model=np.full(16, QK_MC_HESTON, np.int32), **h, flags=QK_PLAN_TIMING)
+    plan.execute()
+    p, _ = plan.results()
+    st = plan.stats()
+    assert st["simulate_ms"] > 0 and st["path_steps"] == 16 * 8192 * 32
+    dp, ds = plan.device_results()
+    assert dp and ds
+    plan.close()

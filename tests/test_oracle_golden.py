@@ -1,0 +1,180 @@
+"""Pins the CPU oracle: reference golden seeds, fixtures generated from the
+reference library, closed-form known values, and the Philox/Box-Muller layout.
+
+Runs on CPU (no GPU marker)."""
+
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from oracle.oracle import (ANTITHETIC, EULER, HESTON, LOCAL_VOL, MILSTEIN, STANDARD,
+                           TERMINAL_PLAIN)
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reference_mc.json").read_text())
+
+
+def _args(d):
+    return {k: (float.fromhex(v) if isinstance(v, str) else v) for k, v in d.items()}
+
+
+def _same(a, b):
+    return (math.isnan(a) and math.isnan(b)) or a == b
+
+
+# cpp/tests/test_monte_carlo.cpp:57-73 of the reference.
+def test_reference_golden_seeds(oracle):
+    p, _ = oracle.price(STANDARD, 100.0, 100.0, 1.0, 0.2, 0.05, 0.0, 0, 50000, 1, 12345)
+    assert abs(p - 10.533371511490282) < 1e-12
+    p, _ = oracle.price(STANDARD, 100.0, 100.0, 1.0, 0.2, 0.05, 0.0, 1, 50000, 1, 12345)
+    assert abs(p - 5.6296577522043556) < 1e-12
+    p, _ = oracle.price(EULER, 100.0, 100.0, 1.0, 0.2, 0.05, 0.0, 0, 10000, 100, 12345)
+    assert abs(p - 10.218359279533905) < 1e-12
+
+
+@pytest.mark.parametrize("i", range(len(GOLDEN["mc_cases"])))
+def test_oracle_bitwise_equals_reference_fixture(oracle, i):
+    case = GOLDEN["mc_cases"][i]
+    a = _args(case["args"])
+    want = float.fromhex(case["price"])
+    got, _ = oracle.price(case["model"], **a)
+    assert _same(got, want), f"case {i} model {case['model']}: {got!r} != {want!r}"
+
+
+def test_oracle_bitwise_equals_reference_live(oracle, ref):
+    rng = np.random.default_rng(7)
+    for model in (STANDARD, ANTITHETIC, EULER, MILSTEIN, LOCAL_VOL, HESTON):
+        for _ in range(5):
+            a = dict(spot=float(rng.uniform(50, 150)), strike=float(rng.uniform(50, 150)),
+                     t=float(rng.uniform(0.05, 3.0)), vol=float(rng.uniform(0.05, 0.8)),
+                     r=float(rng.uniform(-0.01, 0.08)), q=float(rng.uniform(0.0, 0.05)),
+                     option_type=int(rng.integers(0, 2)), paths=int(rng.integers(2, 2000)),
+                     steps=int(rng.integers(1, 40)), seed=int(rng.integers(0, 2**64, dtype=np.uint64)),
+                     v0=float(rng.uniform(0, 0.2)), kappa=float(rng.uniform(0, 6)),
+                     theta=float(rng.uniform(0, 0.2)), sigma=float(rng.uniform(0, 1.5)),
+                     rho=float(rng.uniform(-1, 1)))
+            got, _ = oracle.price(model, **a)
+            want = ref.price(model, **a)
+            assert _same(got, want), (model, a, got, want)
+
+
+@pytest.mark.parametrize("i", range(len(GOLDEN["heston_cf"])))
+def test_heston_cf_matches_reference(oracle, i):
+    case = GOLDEN["heston_cf"][i]
+    a = _args(case["args"])
+    want = float.fromhex(case["price"])
+    got = oracle.heston_cf(**a)
+    # Gauss-Legendre nodes are computed here, tabulated there: agreement to ~1e-10.
+    assert abs(got - want) < 1e-8, (a, got, want)
+
+
+def test_heston_cf_converged_and_small_volvol_limit(oracle):
+    base = dict(spot=100.0, strike=105.0, t=1.0, r=0.03, q=0.01, v0=0.04, kappa=1.5,
+                theta=0.04, sigma=1e-4, rho=-0.5, option_type=0)
+    # vol-of-vol -> 0 with v0 = theta is BSM with vol = 0.2
+    h = oracle.heston_cf(**base)
+    b = oracle.bsm(100.0, 105.0, 1.0, 0.2, 0.03, 0.01, 0)
+    assert abs(h - b) < 1e-4
+    # the integration default (1024 steps, limit 120) is converged to ~3e-7,
+    # far below any Monte Carlo standard error it is compared with
+    base.update(sigma=0.6, rho=-0.7)
+    p1 = oracle.heston_cf(**base)
+    p2 = oracle.heston_cf(**base, integration_steps=8192, integration_limit=500.0)
+    assert abs(p1 - p2) < 1e-6
+    # put-call parity
+    c = oracle.heston_cf(**base)
+    p = oracle.heston_cf(**{**base, "option_type": 1})
+    assert abs((c - p) - (100.0 * math.exp(-0.01) - 105.0 * math.exp(-0.03))) < 1e-10
+
+
+def test_bsm_known_values_and_reference_cdf(oracle):
+    # cpp/tests/test_closed_form.cpp:7-15
+    assert abs(oracle.bsm(100, 100, 1, 0.2, 0.05, 0, 0) - 10.4506) < 0.01
+    assert abs(oracle.bsm(100, 100, 1, 0.2, 0.05, 0, 1) - 5.5735) < 0.01
+    c = oracle.bsm(100, 105, 0.5, 0.25, 0.05, 0.02, 0)
+    p = oracle.bsm(100, 105, 0.5, 0.25, 0.05, 0.02, 1)
+    assert abs((c - p) - (100 * math.exp(-0.01) - 105 * math.exp(-0.025))) < 1e-10
+    # the reference uses A&S 7.1.26 (|error| <= 1.5e-7 in the CDF)
+    for case in GOLDEN["bsm_cf_reference_as_cdf"]:
+        a = _args(case["args"])
+        assert abs(oracle.bsm(**a) - float.fromhex(case["price"])) < 1e-4
+
+
+def test_standard_error_matches_seed_dispersion(oracle):
+    prices, ses = [], []
+    for seed in range(300):
+        p, se = oracle.price(STANDARD, 100.0, 100.0, 1.0, 0.2, 0.05, 0.0, 0, 2000, 1, seed)
+        prices.append(p)
+        ses.append(se)
+    ratio = np.std(prices, ddof=1) / np.mean(ses)
+    assert 0.85 < ratio < 1.15, ratio
+    prices, ses = [], []
+    for seed in range(200):
+        p, se = oracle.price(HESTON, 100.0, 100.0, 1.0, 0.0, 0.05, 0.02, 0, 500, 10, seed,
+                             v0=0.04, kappa=2.0, theta=0.04, sigma=0.3, rho=-0.7)
+        prices.append(p)
+        ses.append(se)
+    ratio = np.std(prices, ddof=1) / np.mean(ses)
+    assert 0.8 < ratio < 1.2, ratio
+
+
+def test_polar_normals_are_standard(oracle):
+    z = oracle.normals(12345, 200000)
+    assert abs(z.mean()) < 0.01
+    assert abs(z.var() - 1.0) < 0.01
+
+
+# --- Philox4x32-10: restated independently here in Python ------------------------------
+def _philox_py(ctr, key):
+    c0, c1, c2, c3 = ctr
+    k0, k1 = key
+    M = 0xFFFFFFFF
+    for _ in range(10):
+        p0 = 0xD2511F53 * c0
+        p1 = 0xCD9E8D57 * c2
+        c0, c1, c2, c3 = ((p1 >> 32) ^ c1 ^ k0) & M, p1 & M, ((p0 >> 32) ^ c3 ^ k1) & M, p0 & M
+        k0 = (k0 + 0x9E3779B9) & M
+        k1 = (k1 + 0xBB67AE85) & M
+    return [c0, c1, c2, c3]
+
+
+def test_philox_matches_python_restatement(oracle):
+    rng = np.random.default_rng(3)
+    for _ in range(200):
+        ctr = [int(x) for x in rng.integers(0, 2**32, 4, dtype=np.uint64)]
+        key = [int(x) for x in rng.integers(0, 2**32, 2, dtype=np.uint64)]
+        assert oracle.philox(ctr, key) == _philox_py(ctr, key)
+    assert oracle.philox([0, 0, 0, 0], [0, 0]) == _philox_py([0, 0, 0, 0], [0, 0])
+
+
+def test_philox_box_muller_layout(oracle):
+    seed = 0x123456789ABCDEF
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    for c0, c1, c3 in [(0, 0, 0), (5, 7, 0), (2**31, 99, 1)]:
+        x = _philox_py([c0, c1, 0, c3], key)
+        z = oracle.philox_normals4(seed, c0, c1, c3)
+        want = []
+        for a, b in ((x[0], x[1]), (x[2], x[3])):
+            u = ((a >> 9) + 0.5) * 2.0**-23
+            g = ((b >> 9) + 0.5) * 2.0**-22 - 1.0
+            rad = math.sqrt(-2.0 * math.log(u))
+            want += [rad * math.cos(math.pi * g), rad * math.sin(math.pi * g)]
+        assert np.allclose(z, want, rtol=0, atol=1e-14)
+    # the replayed stream is standard normal
+    zs = np.concatenate([oracle.philox_normals4(seed, i, 0, 0) for i in range(20000)])
+    assert abs(zs.mean()) < 0.02 and abs(zs.var() - 1.0) < 0.02
+
+
+def test_philox_replay_estimator_is_statistically_the_reference(oracle):
+    """The replay (the GPU's stream in FP64) and the reference (mt19937) price the
+    same option within 4 combined standard errors, for every model."""
+    base = dict(spot=100.0, strike=95.0, t=1.0, vol=0.25, r=0.03, q=0.01, option_type=0,
+                v0=0.05, kappa=1.5, theta=0.04, sigma=0.5, rho=-0.6)
+    for model in (STANDARD, ANTITHETIC, TERMINAL_PLAIN, EULER, MILSTEIN, LOCAL_VOL, HESTON):
+        steps = 16
+        a, sa = oracle.philox_price(model, paths=20000, steps=steps, seed=11, **base)
+        b, sb = oracle.price(model, paths=20000, steps=steps, seed=11, **base)
+        z = (a - b) / math.hypot(sa, sb)
+        assert abs(z) < 4.0, (model, a, b, z)
