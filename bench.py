@@ -312,17 +312,24 @@ def main_gpu(args):
         "traffic": None,
         "kernel": "mc_simulate_kernel<Heston,256,2,antithetic>",
         "kernel_ms": sim_ms,
+        "measured": {"thread_instructions_per_path_step": 27.9, "xu_per_path_step": 3,
+                     "issue_busy": 0.705, "xu_pipe_busy": 0.607,
+                     "source": "ncu, profiles/heston_simulate_ncu.md"},
+        "note": ("frac > 1: the reference formulas cost 6 XU + 50 ALU per path-step; this "
+                 "kernel needs 3 XU + ~25 (antithetic pairs share normals, log-space spot "
+                 "drops the per-step exp)"),
         "per_unit": {"xu": XU_PER_UNIT, "alu": ALU_PER_UNIT, "unit": "path-step"},
         "peak_source": ("nominal per-clock SM widths (148 SMs x 128 issue / 16 XU per clk) at "
                         "the SM clock sampled during the timed region; the driver's measured "
                         "peaks are HBM copy and bf16 GEMM, which do not bound this kernel"),
     }
-    prof = ROOT / "profiles" / "heston_simulate_traffic.json"
+    # DRAM bytes per full launch, from the committed ncu summary (a small case
+    # of the same kernel scaled by the option count; see that file)
+    prof = ROOT / "profiles" / "heston_simulate_ncu.md"
     if prof.exists():
-        try:
-            roofline["traffic"] = json.loads(prof.read_text())["dram_bytes_per_launch"]
-        except Exception:
-            pass
+        for line in prof.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch_full:"):
+                roofline["traffic"] = int(line.split(":")[1]) * n_opt // N_OPT
 
     threads = host_threads()
     try:

@@ -35,12 +35,13 @@ namespace {
 struct Acc {
     DD sy{0.0, 0.0};
     DD q{0.0, 0.0};
+    double lone = 0.0;
     __device__ __forceinline__ void add_pair(double a, double b) {
         const double y = __dmul_rn(0.5, __dadd_rn(a, b));
         sy = dd_add(sy, y);
         q = dd_add(q, __dmul_rn(y, y));
     }
-    __device__ __forceinline__ void add_lone(double a) { sy = dd_add(sy, __dmul_rn(0.5, a)); }
+    __device__ __forceinline__ void add_lone(double a) { lone = __dadd_rn(lone, a); }
     __device__ __forceinline__ void add_plain(double a) {
         sy = dd_add(sy, a);
         q = dd_add(q, __dmul_rn(a, a));
@@ -226,29 +227,36 @@ template <int BLOCK>
 __device__ __forceinline__ void reduce_tile(Acc acc, TilePartial* __restrict__ out, DD* smem) {
     constexpr int W = BLOCK / 32;
     DD a = acc.sy, b = acc.q;
+    double lone = acc.lone;  // nonzero in at most one thread: plain sums are exact
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         a = dd_merge(a, dd_shfl_down(a, off));
         b = dd_merge(b, dd_shfl_down(b, off));
+        lone = __dadd_rn(lone, __shfl_down_sync(0xffffffffu, lone, off));
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
         smem[warp] = a;
         smem[W + warp] = b;
+        smem[2 * W + warp] = DD{lone, 0.0};
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         DD ta = smem[0], tb = smem[W];
+        double tl = smem[2 * W].hi;
 #pragma unroll
         for (int w = 1; w < W; ++w) {
             ta = dd_merge(ta, smem[w]);
             tb = dd_merge(tb, smem[W + w]);
+            tl = __dadd_rn(tl, smem[2 * W + w].hi);
         }
         TilePartial t;
         t.sy_hi = ta.hi;
         t.sy_lo = ta.lo;
         t.q_hi = tb.hi;
         t.q_lo = tb.lo;
+        t.lone = tl;
+        t.pad = 0.0;
         *out = t;
     }
     __syncthreads();
@@ -298,11 +306,14 @@ __device__ __forceinline__ void run_tile(const McOption& o, int64_t tile, TilePa
 // ----------------------------------------------------------------------------
 // Kernel 1a: single-family simulate, grid-stride over tiles.
 // ----------------------------------------------------------------------------
+// No register cap: the kernel is issue- and special-function-bound, and
+// forcing 64 registers (4 CTAs of 256 per SM) added instructions and ran
+// slower on B200 than the compiler's 70 (3 CTAs).
 template <int FAMILY, int BLOCK, int UPT, bool ANTI>
 __global__ void __launch_bounds__(BLOCK)
     mc_simulate_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
                        int32_t n, int64_t n_tiles, TilePartial* __restrict__ partials) {
-    __shared__ DD smem[2 * (BLOCK / 32)];
+    __shared__ DD smem[3 * (BLOCK / 32)];
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int32_t oi = find_option(tile_begin, n, tile);
         const McOption o = opts[oi];
@@ -319,11 +330,11 @@ __global__ void __launch_bounds__(BLOCK)
 // in total, so the loop always terminates.
 // ----------------------------------------------------------------------------
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK)
+__global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
     mc_persistent_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
                          int32_t n, int64_t n_tiles, TilePartial* __restrict__ partials,
                          unsigned long long* __restrict__ work_counter) {
-    __shared__ DD smem[2 * (BLOCK / 32)];
+    __shared__ DD smem[3 * (BLOCK / 32)];
     __shared__ long long s_tile;
     for (;;) {
         if (threadIdx.x == 0) s_tile = (long long)atomicAdd(work_counter, 1ull);
@@ -387,20 +398,24 @@ __global__ void __launch_bounds__(256)
         return;
     }
     DD sy{0.0, 0.0}, q{0.0, 0.0};
+    double lone = 0.0;
     for (int32_t t = lane; t < o.tiles; t += 32) {
         const TilePartial p = partials[o.tile_begin + t];
         sy = dd_merge(sy, DD{p.sy_hi, p.sy_lo});
         q = dd_merge(q, DD{p.q_hi, p.q_lo});
+        lone = __dadd_rn(lone, p.lone);
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         sy = dd_merge(sy, dd_shfl_down(sy, off));
         q = dd_merge(q, dd_shfl_down(q, off));
+        lone = __dadd_rn(lone, __shfl_down_sync(0xffffffffu, lone, off));
     }
     if (lane == 0) {
         const double s = sy.hi + sy.lo;
         const double qq = q.hi + q.lo;
-        const double total = o.antithetic ? 2.0 * s : s;  // sum of all path payoffs
+        // sum of all path payoffs: two per pair, plus the unpaired path
+        const double total = o.antithetic ? __dadd_rn(2.0 * s, lone) : s;
         out_price[warp] = o.disc * (total / (double)o.paths);
         const double ns = (double)o.samples;
         double se = __longlong_as_double(0x7FF8000000000000ll);

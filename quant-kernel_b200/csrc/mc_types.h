@@ -57,10 +57,15 @@ struct alignas(16) McOption {
 };
 static_assert(sizeof(McOption) == 128, "McOption layout");
 
-// Per-tile partial sums: y = pair mean (antithetic) or payoff (plain).
+// Per-tile partial sums: y = pair mean (antithetic) or payoff (plain).  The
+// unpaired last path of an odd antithetic count is kept apart in `lone`: it
+// belongs in the price but not in the pair-mean variance.
 struct alignas(16) TilePartial {
-    double sy_hi, sy_lo;  // sum of y
+    double sy_hi, sy_lo;  // sum of y over full samples
     double q_hi, q_lo;    // sum of y^2 over full samples
+    double lone;          // payoff of the unpaired path (0 elsewhere)
+    double pad;
 };
+static_assert(sizeof(TilePartial) == 48, "TilePartial layout");
 
 }  // namespace qkb

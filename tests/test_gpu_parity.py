@@ -22,6 +22,15 @@ pytestmark = pytest.mark.gpu
 P_EXCEED = 2.0 * stats.norm.sf(3.0)  # 0.0027
 
 
+def _z(a, b, se):
+    """z-score; an option whose payoffs are all zero on both sides (deep out of
+    the money) has zero variance and must then agree exactly."""
+    a, b, se = map(np.asarray, (a, b, se))
+    zero = se == 0
+    assert np.all(a[zero] == b[zero])
+    return np.where(zero, 0.0, (a - b) / np.where(zero, 1.0, se))
+
+
 def _check(z, label, zmax=5.0):
     z = np.asarray(z)
     assert np.all(np.isfinite(z)), label
@@ -43,10 +52,10 @@ def test_bsm_terminal_full_size_vs_closed_form_and_reference(qk, oracle):
         p, se = fn(**b)
         cf = np.array([oracle.bsm(b["spot"][i], b["strike"][i], b["t"][i], b["vol"][i], b["r"][i],
                                   b["q"][i], int(b["option_type"][i])) for i in range(64)])
-        _check((p - cf) / se, f"{name} GPU vs BSM closed form")
+        _check(_z(p, cf, se), f"{name} GPU vs BSM closed form")
         cp, cse = oracle.bsm_family_batch(model, b["spot"], b["strike"], b["t"], b["vol"], b["r"],
                                           b["q"], b["option_type"], b["paths"], None, b["seed"])
-        _check((p - cp) / np.hypot(se, cse), f"{name} GPU vs reference CPU MC")
+        _check(_z(p, cp, np.hypot(se, cse)), f"{name} GPU vs reference CPU MC")
 
 
 @pytest.mark.parametrize("model", [2, 3, 4])
@@ -60,52 +69,72 @@ def test_stepwise_vs_reference_cpu_mc(qk, oracle, model):
     p, se = fn(**b, steps=steps)
     cp, cse = oracle.bsm_family_batch(model, b["spot"], b["strike"], b["t"], b["vol"], b["r"],
                                       b["q"], b["option_type"], b["paths"], steps, b["seed"])
-    _check((p - cp) / np.hypot(se, cse), f"model {model} GPU vs reference CPU MC")
+    _check(_z(p, cp, np.hypot(se, cse)), f"model {model} GPU vs reference CPU MC")
 
 
 def test_heston_vs_reference_cpu_mc(qk, oracle):
     h = workloads.heston(32, paths=32768, steps=50, seed=77)
     p, se = qk.heston_monte_carlo_price_se_batch(**h)
     cp, cse = oracle.heston_batch(**h)
-    _check((p - cp) / np.hypot(se, cse), "Heston GPU vs reference CPU MC (32 x 32768 x 50)")
+    _check(_z(p, cp, np.hypot(se, cse)), "Heston GPU vs reference CPU MC (32 x 32768 x 50)")
 
 
 def test_heston_full_size_vs_cf_and_reference_subset(qk, oracle):
     """The benchmark workload at full size: 1024 calls x 262144 paths x 200 steps.
 
-    Against the FP64 characteristic-function price the comparison includes the
-    200-step Euler discretisation bias (largest at low Feller ratio), which no
-    kernel can remove; it is reported, and bounded by the same multiplicity
-    rule with |z| < 6.  The discretisation-free check is against the
-    reference's CPU Monte Carlo at identical steps, on a subset."""
+    The FP64 characteristic-function price is the continuous-time Heston
+    price; the reference's full-truncation Euler at 200 steps is biased away
+    from it, strongly at low Feller ratio 2 kappa theta / sigma^2 (the box
+    reaches 0.01).  So:
+      (1) options with Feller >= 1 (small scheme bias) match the CF price
+          within the multiplicity rule;
+      (2) the most biased options match the reference's own CPU Monte Carlo
+          at the same 200 steps -- the discretisation-free check;
+      (3) their gap to the CF price shrinks when the GPU runs more steps (slowly:
+          full truncation converges at a low rate when v sits at 0), so the gap
+          belongs to the scheme, not to the kernel.
+    Observed errors are printed."""
     h = workloads.heston()
     p, se = qk.heston_monte_carlo_price_se_batch(**h)
     assert np.all(np.isfinite(p)) and np.all(se > 0)
-    cf = np.array([oracle.heston_cf(h["spot"][i], h["strike"][i], h["t"][i], h["r"][i], h["q"][i],
-                                    h["v0"][i], h["kappa"][i], h["theta"][i], h["sigma"][i],
-                                    h["rho"][i], 0) for i in range(len(p))])
+    n = len(p)
+
+    def cf_of(b, i):
+        return oracle.heston_cf(b["spot"][i], b["strike"][i], b["t"][i], b["r"][i], b["q"][i],
+                                b["v0"][i], b["kappa"][i], b["theta"][i], b["sigma"][i],
+                                b["rho"][i], 0)
+
+    cf = np.array([cf_of(h, i) for i in range(n)])
     z = (p - cf) / se
     feller = 2 * h["kappa"] * h["theta"] / h["sigma"] ** 2
     err = np.abs(p - cf) / h["spot"]
-    print(f"max |price - CF| / S = {err.max():.2e}, mean = {err.mean():.2e}, "
-          f"mean SE/S = {(se / h['spot']).mean():.2e}")
-    print(f"mean z, Feller < 0.5: {z[feller < 0.5].mean():+.3f} (n={int((feller < 0.5).sum())}); "
-          f"Feller >= 1: {z[feller >= 1].mean():+.3f} (n={int((feller >= 1).sum())})")
-    n = z.size
-    allowed = int(stats.binom.ppf(0.999, n, P_EXCEED))
-    exceed = int((np.abs(z) > 3).sum())
-    print(f"GPU vs Heston CF: |z|>3 {exceed} (expected {n * P_EXCEED:.1f}, allowed {allowed}), "
-          f"max|z| {np.abs(z).max():.2f}")
-    assert np.abs(z).max() < 6.0
-    assert exceed <= allowed + int((feller < 0.5).sum() * 0.1)
-    # discretisation-free: reference CPU MC at identical 200 steps, 4 options
-    idx = np.array([0, 1, 2, 3])
-    sub = {k: v[idx] for k, v in workloads.heston(1024, paths=32768, steps=200).items()}
+    hi = feller >= 1.0
+    print(f"|price - CF|/S: max {err.max():.2e} mean {err.mean():.2e}; Feller>=1: max "
+          f"{err[hi].max():.2e}; mean SE/S {(se / h['spot']).mean():.2e}")
+    for lo_f, hi_f in ((0, 0.25), (0.25, 0.5), (0.5, 1.0), (1.0, 1e9)):
+        m = (feller >= lo_f) & (feller < hi_f)
+        if m.any():
+            print(f"  Feller [{lo_f}, {hi_f}): n={int(m.sum())} mean z vs CF {z[m].mean():+.2f}")
+    _check(z[hi], "Heston GPU vs CF, Feller >= 1 (1024 x 262144 x 200)")
+
+    order = np.argsort(feller)
+    idx = np.concatenate([order[:8], order[-4:]])
+    sub = {k: v[idx] for k, v in workloads.heston(paths=32768).items()}
     gp, gse = qk.heston_monte_carlo_price_se_batch(**sub)
     cp, cse = oracle.heston_batch(**sub)
-    zz = (gp - cp) / np.hypot(gse, cse)
-    print("subset z vs reference CPU MC:", np.round(zz, 2))
-    assert np.abs(zz).max() < 4.0
+    print("lowest Feller:", np.round(feller[order[:8]], 3))
+    _check(_z(gp, cp, np.hypot(gse, cse)),
+           "Heston GPU vs reference CPU MC, 200 steps, 8 lowest + 4 highest Feller", zmax=4.5)
+
+    low = {k: v[order[:8]] for k, v in workloads.heston(paths=65536).items()}
+    cfl = np.array([cf_of(low, i) for i in range(8)])
+    g200, _ = qk.heston_monte_carlo_price_se_batch(**low)
+    low800 = dict(low, steps=np.full(8, 1600, np.int32))
+    g1600, s1600 = qk.heston_monte_carlo_price_se_batch(**low800)
+    e200, e1600 = np.abs(g200 - cfl), np.abs(g1600 - cfl)
+    print("low-Feller |GPU - CF| at 200 steps:", np.round(e200, 4), " at 1600 steps:", np.round(e1600, 4))
+    # full truncation converges slowly at Feller ~0.02 (observed: -23% for 8x the steps)
+    assert e1600.mean() < 0.85 * e200.mean()
 
 
 def test_fixture_edge_cases_on_gpu(qk, oracle):
