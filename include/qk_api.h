@@ -162,6 +162,27 @@ QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_se_batch(
     const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
     const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
 
+/* Heston batch that allocates no memory.  No counterpart in the reference.
+ * For callers that cannot call cudaMalloc: services whose host framework owns
+ * every device allocation (a caching allocator or a capped pool), processes
+ * that must not grow their GPU footprint after start-up, and latency-bound
+ * paths that cannot afford an allocation or the synchronisation of a free.
+ * Same inputs and outputs as qk_mcm_heston_monte_carlo_price_se_batch (host
+ * arrays; out_stderr may be NULL) and the same kernels and results; every
+ * device buffer lives in one fixed 12.6 MiB array per GPU, held until the
+ * process exits.  Limits: n <= 4096 options and at most 262,144 tiles in
+ * total (a tile is 512 antithetic path pairs of one option, e.g. 1024 options
+ * of 262,144 paths); larger batches return QK_ERR_BAD_SIZE before any GPU
+ * work.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current, so make it before any
+ * stream capture.  Calls share the array; this entry point serialises them
+ * and is synchronous, so its calls never overlap on the GPU. */
+QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_batch_noalloc(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+
 /* Mixed-model batch: option i is priced with model[i] (QK_MC_*).  Fields a
  * model does not use are ignored and may hold anything (vol for Heston;
  * v0..rho for the BSM models; steps for the terminal models).  Runs as one

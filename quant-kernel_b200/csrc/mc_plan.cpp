@@ -68,7 +68,40 @@ void set_const(McOption& o, double price) {
 
 int32_t geti(const int32_t* a, int32_t i, int32_t dflt) { return a ? a[i] : dflt; }
 
-// Pack option i.  Fills everything but the tile geometry.
+int upt_for(int family, bool persistent, const LaunchConfig& cfg) {
+    if (!persistent) return cfg.upt;
+    switch (family) {
+        case kFamTerminal: return kUptTerminal;
+        case kFamHeston: return kUptHeston;
+        default: return kUptStepwise;
+    }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+std::string device_name(int dev) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
+    std::string s = prop.name;
+    for (char& c : s)
+        if (c == ' ' || c == '|') c = '_';
+    return s;
+}
+
+}  // namespace
+
+// Packs option i: validation, special cases and model constants; the tile
+// geometry is filled by tile_option().
 McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
     McOption o;
     std::memset(&o, 0, sizeof o);
@@ -173,37 +206,21 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
     return o;
 }
 
-int upt_for(int family, bool persistent, const LaunchConfig& cfg) {
-    if (!persistent) return cfg.upt;
-    switch (family) {
-        case kFamTerminal: return kUptTerminal;
-        case kFamHeston: return kUptHeston;
-        default: return kUptStepwise;
+int32_t tile_option(McOption& o, int block, int upt) {
+    if (o.mode != kModeSimulate || o.units <= 0) {
+        o.tiles = 0;
+        o.unit_iters = 0;
+        return 0;
     }
+    const int64_t per_iter = (int64_t)block * upt;
+    const int64_t units = o.units;
+    int64_t iters = (units + per_iter * kMaxTilesPerOption - 1) / (per_iter * kMaxTilesPerOption);
+    if (iters < 1) iters = 1;
+    const int64_t tile_units = per_iter * iters;
+    o.unit_iters = (int32_t)iters;
+    o.tiles = (int32_t)((units + tile_units - 1) / tile_units);
+    return o.tiles;
 }
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-    }
-};
-
-std::string device_name(int dev) {
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
-    std::string s = prop.name;
-    for (char& c : s)
-        if (c == ' ' || c == '|') c = '_';
-    return s;
-}
-
-}  // namespace
 
 // ----------------------------------------------------------------------------
 cudaError_t DevBuf::ensure(size_t bytes) {
@@ -416,19 +433,7 @@ cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
         McOption& o = opts_[(size_t)i];
         begin[(size_t)i] = total;
         o.tile_begin = total;
-        if (o.mode != kModeSimulate || o.units <= 0) {
-            o.tiles = 0;
-            o.unit_iters = 0;
-            continue;
-        }
-        const int64_t per_iter = (int64_t)cfg.block * upt_for(family_of(o.model), persistent_, cfg);
-        const int64_t units = o.units;
-        int64_t iters = (units + per_iter * kMaxTilesPerOption - 1) / (per_iter * kMaxTilesPerOption);
-        if (iters < 1) iters = 1;
-        const int64_t tile_units = per_iter * iters;
-        o.unit_iters = (int32_t)iters;
-        o.tiles = (int32_t)((units + tile_units - 1) / tile_units);
-        total += o.tiles;
+        total += tile_option(o, cfg.block, upt_for(family_of(o.model), persistent_, cfg));
     }
     begin[(size_t)n] = total;
     n_tiles_ = total;

@@ -113,6 +113,12 @@ private:
     cudaGraphExec_t graph_exec_ = nullptr;
 };
 
+// Packs option i of `in` (entry checks, special cases, model constants).
+McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise);
+// Fills o.tiles / o.unit_iters for a launch of `block` threads with `upt`
+// units each; returns o.tiles.
+int32_t tile_option(McOption& o, int block, int upt);
+
 // Per-thread, per-device scratch plan used by the one-shot batch calls.
 Plan* thread_scratch_plan(int device);
 

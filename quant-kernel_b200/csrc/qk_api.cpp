@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 
+#include "mc_noalloc.h"
 #include "mc_plan.h"
 
 namespace {
@@ -423,6 +424,39 @@ double qk_mcm_heston_monte_carlo_price(double spot, double strike, double t, dou
                                               1, &out) != QK_OK)
         return nan_value();
     return out;
+}
+
+int32_t qk_mcm_heston_monte_carlo_price_batch_noalloc(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr) {
+    const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {r, "r"},
+                             {q, "q"}, {v0, "v0"}, {kappa, "kappa"}, {theta, "theta"},
+                             {sigma, "sigma"}, {rho, "rho"}, {option_type, "option_type"},
+                             {paths, "paths"}, {steps, "steps"}, {seed, "seed"},
+                             {out_prices, "out_prices"}};
+    if (int32_t rc = check_nulls(ptrs)) return rc;
+    if (n <= 0) return fail_size(n);
+    const qkb::BatchInput in = heston_input(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                            option_type, paths, steps, seed, n);
+    cudaError_t e = cudaSuccess;
+    int64_t tiles = 0;
+    switch (qkb::noalloc_heston_batch(in, out_prices, out_stderr, &e, &tiles)) {
+        case qkb::NoAllocStatus::kOk:
+            return QK_OK;
+        case qkb::NoAllocStatus::kTooManyOptions:
+            set_error_fmt("bad batch size: %d options exceed the no-allocation limit of %d", n,
+                          qkb::kNoAllocMaxOptions);
+            return QK_ERR_BAD_SIZE;
+        case qkb::NoAllocStatus::kTooManyTiles:
+            set_error_fmt("bad batch size: %lld tiles exceed the no-allocation limit of %lld "
+                          "(one tile = 512 path pairs of one option)",
+                          (long long)tiles, (long long)qkb::kNoAllocMaxTiles);
+            return QK_ERR_BAD_SIZE;
+        default:
+            return fail_cuda(e, "qk_mcm_heston_monte_carlo_price_batch_noalloc");
+    }
 }
 
 // ---- mixed batch and plans -------------------------------------------------------

@@ -66,6 +66,7 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_heston_monte_carlo_price", D, _hes_scalar),
     ("qk_mcm_heston_monte_carlo_price_batch", I32, _hes_batch),
     ("qk_mcm_heston_monte_carlo_price_se_batch", I32, _hes_batch + [PD]),
+    ("qk_mcm_heston_monte_carlo_price_batch_noalloc", I32, _hes_batch + [PD]),
     ("qk_mcm_mixed_price_batch", I32, _mixed_arrays + [PD, PD]),
     ("qk_mcm_plan_create", I32, _mixed_arrays + [I32, ct.POINTER(VP)]),
     ("qk_mcm_plan_execute", I32, [VP, VP]),
