@@ -222,6 +222,18 @@ QK_EXPORT int32_t qk_mcm_plan_config(qk_mc_plan* plan, int32_t* block, int32_t* 
                                      int32_t* ctas);
 QK_EXPORT int32_t qk_mcm_plan_destroy(qk_mc_plan* plan);
 
+/* ======================================================================= *
+ * Part 3 -- Heston surrogate (ABI 2.13, no counterpart in the reference)
+ * ======================================================================= */
+
+/* Tensor-core building block of the surrogate: C = A . B^T with A [m x k] and
+ * B [n x k] bf16 row-major DEVICE pointers (16-byte aligned, k % 64 == 0,
+ * n % 64 == 0), fp32 output.  With splits > 1 the k range is cut into `splits`
+ * equal parts (k % (64 * splits) == 0) and c holds `splits` partial slabs
+ * [splits][m][n].  Asynchronous on `stream` (NULL = default stream). */
+QK_EXPORT int32_t qk_sur_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_t n,
+                                   int32_t k, int32_t splits, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -8,7 +8,6 @@
 // reference counterpart, return QK_ERR_RUNTIME_INIT with "cuda error: ...".
 #include "../../include/qk_api.h"
 
-#include <cstdarg>
 #include <cstdio>
 #include <cstring>
 #include <limits>
@@ -17,40 +16,15 @@
 #include <cuda_runtime.h>
 
 #include "mc_noalloc.h"
+#include "qk_error.h"
 #include "mc_plan.h"
 
 namespace {
 
-thread_local char tl_error_msg[256] = "";
-
-void set_error_msg(const char* msg) {
-    std::strncpy(tl_error_msg, msg, sizeof(tl_error_msg) - 1);
-    tl_error_msg[sizeof(tl_error_msg) - 1] = '\0';
-}
-
-void set_error_fmt(const char* fmt, ...) {
-    char buf[256];
-    va_list ap;
-    va_start(ap, fmt);
-    std::vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    set_error_msg(buf);
-}
-
-int32_t fail_null(const char* name) {
-    set_error_fmt("null pointer: %s", name);
-    return QK_ERR_NULL_PTR;
-}
-
-int32_t fail_size(int32_t n) {
-    set_error_fmt("bad batch size: %d", n);
-    return QK_ERR_BAD_SIZE;
-}
-
-int32_t fail_cuda(cudaError_t e, const char* where) {
-    set_error_fmt("cuda error: %s (%s) in %s", cudaGetErrorName(e), cudaGetErrorString(e), where);
-    return QK_ERR_RUNTIME_INIT;
-}
+using qkb::fail_cuda;
+using qkb::fail_null;
+using qkb::fail_size;
+using qkb::set_error_fmt;
 
 struct NamedPtr {
     const void* p;
@@ -272,7 +246,7 @@ int32_t qk_plugin_get_api(int32_t host_abi_major, int32_t host_abi_minor,
     return QK_OK;
 }
 
-const char* qk_get_last_error(void) { return tl_error_msg; }
+const char* qk_get_last_error(void) { return qkb::last_error(); }
 
 int32_t qk_set_device(int32_t device) {
     cudaError_t e = cudaSetDevice(device);
@@ -288,7 +262,7 @@ int32_t qk_get_device(int32_t* device) {
     return QK_OK;
 }
 
-void qk_clear_last_error(void) { tl_error_msg[0] = '\0'; }
+void qk_clear_last_error(void) { qkb::clear_error(); }
 
 // ---- terminal ---------------------------------------------------------------
 int32_t qk_mcm_standard_monte_carlo_price_batch(const double* spot, const double* strike,

@@ -1,0 +1,426 @@
+// sur_gemm.cu -- tcgen05 / TMEM / TMA BF16 GEMM with fused MLP epilogues.
+// See sur_gemm.cuh for the structure.
+#include "sur_gemm.cuh"
+
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+namespace qkb {
+
+namespace {
+
+constexpr int kStages = 4;
+constexpr int kBM = 128;
+constexpr int kBK = 64;                       // 64 bf16 = 128 B = one swizzle row
+constexpr uint32_t kSpinLimit = 1u << 25;     // bounded mbarrier polls (seconds)
+constexpr uint32_t kABytes = kBM * kBK * 2;   // 16 KiB
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after kSpinLimit polls (each poll may suspend briefly).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kSpinLimit; ++i)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 B apart (SBO), leading offset unused for swizzled K-major (1),
+// descriptor version 1 (sm_100), layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1) << 16) |
+           (static_cast<uint64_t>(1024 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
+           (static_cast<uint64_t>(2) << 61);
+}
+
+// Instruction descriptor, kind::f16: D fp32, A and B bf16, both K-major,
+// N >> 3 at bit 17, M >> 4 at bit 24.
+template <int BN>
+__device__ __forceinline__ constexpr uint32_t idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(BN >> 3) << 17) |
+           (static_cast<uint32_t>(kBM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// 32 consecutive fp32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+          "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+          "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr)
+        : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+
+// 32 bf16 values to 64 contiguous bytes.
+__device__ __forceinline__ void store_bf16x32(__nv_bfloat16* dst, const float (&v)[32]) {
+    uint4* d = reinterpret_cast<uint4*>(dst);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        __nv_bfloat162 p[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) p[j] = __floats2bfloat162_rn(v[q * 8 + 2 * j], v[q * 8 + 2 * j + 1]);
+        d[q] = *reinterpret_cast<uint4*>(p);
+    }
+}
+
+__device__ __forceinline__ void load_bf16x32(const __nv_bfloat16* src, float (&v)[32]) {
+    const uint4* s = reinterpret_cast<const uint4*>(src);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uint4 u = s[q];
+        const __nv_bfloat162* p = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            float2 f = __bfloat1622float2(p[j]);
+            v[q * 8 + 2 * j] = f.x;
+            v[q * 8 + 2 * j + 1] = f.y;
+        }
+    }
+}
+
+template <int BN, int EPI>
+__device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m0, int n0) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int row = m0 + warp * 32 + lane;
+    const bool live = row < a.M;
+    const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    float v[32];
+    if (EPI == kEpiF32) {
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+            tmem_ld32(tbase + c * 32, v);
+            if (live) {
+                float4* dst = reinterpret_cast<float4*>(
+                    a.c_f32 + (static_cast<size_t>(blockIdx.z) * a.M + row) * a.N + n0 + c * 32);
+#pragma unroll
+                for (int q = 0; q < 8; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            }
+        }
+    } else if (EPI == kEpiFwd) {
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+            tmem_ld32(tbase + c * 32, v);
+            const int col0 = n0 + c * 32;
+            float z[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                z[j] = v[j] + __ldg(a.bias + col0 + j);
+                v[j] = z[j] * sigmoidf_(z[j]);
+            }
+            if (live) {
+                if (a.z_out) store_bf16x32(a.z_out + static_cast<size_t>(row) * a.N + col0, z);
+                if (a.h_out) store_bf16x32(a.h_out + static_cast<size_t>(row) * a.N + col0, v);
+                if (a.t_out) {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        a.t_out[static_cast<size_t>(col0 + j) * a.ldt + row] = __float2bfloat16_rn(v[j]);
+                }
+            }
+        }
+    } else if (EPI == kEpiBwd) {
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+            tmem_ld32(tbase + c * 32, v);
+            const int col0 = n0 + c * 32;
+            if (live) {
+                float z[32];
+                load_bf16x32(a.z_in + static_cast<size_t>(row) * a.N + col0, z);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float s = sigmoidf_(z[j]);
+                    v[j] = v[j] * s * (1.0f + z[j] * (1.0f - s));
+                }
+                store_bf16x32(a.d_out + static_cast<size_t>(row) * a.N + col0, v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    a.dt_out[static_cast<size_t>(col0 + j) * a.ldt + row] = __float2bfloat16_rn(v[j]);
+            }
+        }
+    } else {  // kEpiLast: BN == N (the whole hidden row is in this CTA)
+        float y = 0.0f;
+#pragma unroll 1
+        for (int c = 0; c < BN / 32; ++c) {
+            tmem_ld32(tbase + c * 32, v);
+            const int col0 = c * 32;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const float z = v[j] + __ldg(a.bias + col0 + j);
+                y = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), y);
+            }
+        }
+        y += __ldg(a.b4);
+        if (live) a.y_out[row] = y;
+        if (a.target != nullptr) {
+            const float dy = live ? a.loss_scale * (y - a.target[row]) : 0.0f;
+            if (live) a.dy_out[row] = dy;
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c) {
+                tmem_ld32(tbase + c * 32, v);
+                const int col0 = c * 32;
+                float h[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float z = v[j] + __ldg(a.bias + col0 + j);
+                    const float s = sigmoidf_(z);
+                    h[j] = z * s;
+                    v[j] = dy * __ldg(a.w4 + col0 + j) * s * (1.0f + z * (1.0f - s));
+                }
+                if (live) {
+                    store_bf16x32(a.d_out + static_cast<size_t>(row) * a.N + col0, v);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        a.dt_out[static_cast<size_t>(col0 + j) * a.ldt + row] = __float2bfloat16_rn(v[j]);
+                        a.t_out[static_cast<size_t>(col0 + j) * a.ldt + row] = __float2bfloat16_rn(h[j]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int BN, int EPI>
+__global__ void __launch_bounds__(128, 1)
+    umma_gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+                     const GemmArgs a) {
+    constexpr uint32_t kBBytes = BN * kBK * 2;
+    constexpr uint32_t kStage = kABytes + kBBytes;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                               ~static_cast<uintptr_t>(1023));
+    __shared__ __align__(8) uint64_t full_bar[kStages];
+    __shared__ __align__(8) uint64_t empty_bar[kStages];
+    __shared__ __align__(8) uint64_t acc_bar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
+    const int kb0 = blockIdx.z * (a.k_per_split / kBK);
+    int krem = a.K - blockIdx.z * a.k_per_split;
+    if (krem > a.k_per_split) krem = a.k_per_split;
+    const int nkb = krem > 0 ? krem / kBK : 0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_u32(&full_bar[s]), 1);
+            mbar_init(smem_u32(&empty_bar[s]), 1);
+        }
+        mbar_init(smem_u32(&acc_bar), 1);
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(static_cast<uint32_t>(BN))
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+
+    int last_round[kStages];
+#pragma unroll
+    for (int s = 0; s < kStages; ++s) last_round[s] = -1;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % kStages;
+            const int round = kb / kStages;
+            if (round > 0 && !mbar_wait(smem_u32(&empty_bar[s]), (round - 1) & 1)) {
+                abort_flag = 1;
+                atomicExch(a.err, 1);
+                break;
+            }
+            if (abort_flag) break;
+            const uint32_t sa = smem_u32(smem + s * kStage);
+            mbar_expect_tx(smem_u32(&full_bar[s]), kStage);
+            const int kx = (kb0 + kb) * kBK;
+            tma_load_2d(sa, &ta, kx, m0, smem_u32(&full_bar[s]));
+            tma_load_2d(sa + kABytes, &tb, kx, n0, smem_u32(&full_bar[s]));
+            last_round[s] = round;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        constexpr uint32_t idesc = idesc_bf16<BN>();
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % kStages;
+            if (!mbar_wait(smem_u32(&full_bar[s]), (kb / kStages) & 1)) {
+                abort_flag = 1;
+                atomicExch(a.err, 2);
+                break;
+            }
+            if (abort_flag) break;
+            fence_after();
+            const uint32_t sa = smem_u32(smem + s * kStage);
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk)
+                umma_bf16(tmem, desc_sw128(sa + kk * 32), desc_sw128(sa + kABytes + kk * 32), idesc,
+                          (kb | kk) != 0 ? 1u : 0u);
+            umma_commit(smem_u32(&empty_bar[s]));
+        }
+        umma_commit(smem_u32(&acc_bar));  // arrives once every issued MMA has completed
+    }
+    __syncwarp();
+
+    // Epilogue: accumulator ready (bounded wait), then TMEM -> registers -> global.
+    const bool acc_ok = mbar_wait(smem_u32(&acc_bar), 0);
+    __syncwarp();
+    fence_after();
+    if (!acc_ok) {
+        if (threadIdx.x == 0) atomicExch(a.err, 3);
+        abort_flag = 1;
+    }
+    __syncthreads();
+    if (!abort_flag && nkb > 0) epilogue<BN, EPI>(a, tmem, m0, n0);
+
+    // Teardown: the producer drains its own loads (bounded), then TMEM is freed.
+    if (warp == 0 && lane == 0 && abort_flag) {
+        for (int s = 0; s < kStages; ++s)
+            if (last_round[s] >= 0) mbar_wait(smem_u32(&full_bar[s]), last_round[s] & 1);
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(static_cast<uint32_t>(BN))
+                     : "memory");
+    }
+}
+
+template <int BN, int EPI>
+cudaError_t launch_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& a, int splits,
+                     cudaStream_t st) {
+    constexpr size_t smem = kStages * (kABytes + BN * kBK * 2) + 1024;
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(umma_gemm_kernel<BN, EPI>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    dim3 grid((a.M + kBM - 1) / kBM, a.N / BN, splits);
+    umma_gemm_kernel<BN, EPI><<<grid, 128, smem, st>>>(ta, tb, a);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+bool make_tmap_bf16(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
+                    uint32_t box_rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!encode) return false;
+    // Host-side checks of the TMA rules: 16-byte aligned base, row stride a
+    // multiple of 16 bytes, a 64-element (128-byte) inner box.
+    if ((reinterpret_cast<uintptr_t>(base) & 15) != 0 || (cols * 2) % 16 != 0 || cols < 64) return false;
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {cols * 2};
+    const cuuint32_t box[2] = {64, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+cudaError_t launch_umma_gemm(int epi, int bn, const CUtensorMap& ta, const CUtensorMap& tb,
+                             const GemmArgs& a, int splits, cudaStream_t st) {
+    if (a.K % kBK != 0 || a.k_per_split % kBK != 0 || a.N % bn != 0 || splits < 1)
+        return cudaErrorInvalidValue;
+    switch (bn) {
+        case 64:
+            if (epi == kEpiF32) return launch_t<64, kEpiF32>(ta, tb, a, splits, st);
+            break;
+        case 128:
+            if (epi == kEpiF32) return launch_t<128, kEpiF32>(ta, tb, a, splits, st);
+            if (epi == kEpiFwd) return launch_t<128, kEpiFwd>(ta, tb, a, splits, st);
+            if (epi == kEpiBwd) return launch_t<128, kEpiBwd>(ta, tb, a, splits, st);
+            break;
+        case 256:
+            if (epi == kEpiF32) return launch_t<256, kEpiF32>(ta, tb, a, splits, st);
+            if (epi == kEpiFwd) return launch_t<256, kEpiFwd>(ta, tb, a, splits, st);
+            if (epi == kEpiLast) return launch_t<256, kEpiLast>(ta, tb, a, splits, st);
+            if (epi == kEpiBwd) return launch_t<256, kEpiBwd>(ta, tb, a, splits, st);
+            break;
+        default:
+            break;
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace qkb

@@ -75,6 +75,7 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_plan_stats", I32, [VP, PD, PI32, PI64]),
     ("qk_mcm_plan_config", I32, [VP, PI32, PI32, PI32]),
     ("qk_mcm_plan_destroy", I32, [VP]),
+    ("qk_sur_gemm_bf16", I32, [VP, VP, VP, I32, I32, I32, I32, VP]),
 ]
 
 
