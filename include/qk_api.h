@@ -234,6 +234,59 @@ QK_EXPORT int32_t qk_mcm_plan_destroy(qk_mc_plan* plan);
 QK_EXPORT int32_t qk_sur_gemm_bf16(const void* a, const void* b, float* c, int32_t m, int32_t n,
                                    int32_t k, int32_t splits, void* stream);
 
+/* The surrogate: an MLP 9 -> 256 -> 256 -> 256 -> 1 (SiLU, BF16 weights and
+ * activations, FP32 accumulation, FP32 master weights) from the features
+ *   f = (S/K, T, r, q, v0, kappa, theta, sigma, rho)
+ * to the Heston call price / S.  Inputs are normalised to [-1, 1] over the
+ * training box [box_lo, box_hi] (a dimension with lo == hi maps to 0).  It is
+ * trained on the GPU by the library's own tcgen05 forward/backward GEMMs and
+ * Adam kernels on labels the caller produces (normally this library's Heston
+ * Monte Carlo).  All arrays are host arrays; features are row-major n x 9. */
+typedef struct qk_sur_model qk_sur_model;
+
+QK_EXPORT int32_t qk_sur_heston_create(const double* box_lo, const double* box_hi, uint64_t seed,
+                                       qk_sur_model** out_model);
+QK_EXPORT int32_t qk_sur_heston_destroy(qk_sur_model* model);
+QK_EXPORT int32_t qk_sur_heston_set_dataset(qk_sur_model* model, const double* features,
+                                            const double* target, int64_t n);
+/* Adam (beta 0.9/0.999, eps 1e-8), lr cosine-decayed from `lr` over all steps of
+ * this call, minibatch `batch` (a multiple of 128), a fresh permutation per
+ * epoch.  out_epoch_loss (may be NULL) receives each epoch's mean MSE. */
+QK_EXPORT int32_t qk_sur_heston_train(qk_sur_model* model, int32_t epochs, int32_t batch,
+                                      double lr, uint64_t shuffle_seed, double* out_epoch_loss);
+/* price / S for each row of features (no box check). */
+QK_EXPORT int32_t qk_sur_heston_predict(qk_sur_model* model, const double* features, int64_t n,
+                                        double* out);
+/* Device-resident inference: x_rows = normalised bf16 rows [n][64] (DEVICE),
+ * y = price / S (DEVICE, fp32); asynchronous on `stream` (NULL = model's). */
+QK_EXPORT int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows, int64_t n,
+                                               float* y, void* stream);
+/* Normalised bf16 rows [n][64] (HOST output buffer of n*64 uint16). */
+QK_EXPORT int32_t qk_sur_heston_features(qk_sur_model* model, const double* features, int64_t n,
+                                         void* out_rows);
+/* Loss (mean squared error) and its 134,401 gradients for one batch (n a
+ * multiple of 128), without an update; replaces the model's dataset. */
+QK_EXPORT int32_t qk_sur_heston_gradients(qk_sur_model* model, const double* features,
+                                          const double* target, int32_t n, double* grads,
+                                          double* loss);
+/* Parameters in the order W1[256][9], b1, W2[256][256], b2, W3[256][256], b3,
+ * w4[256], b4 (134,401 values). */
+QK_EXPORT int32_t qk_sur_heston_parameters(qk_sur_model* model, double* out);
+QK_EXPORT int32_t qk_sur_heston_set_parameters(qk_sur_model* model, const double* in);
+QK_EXPORT int32_t qk_sur_heston_save(qk_sur_model* model, const char* path);
+QK_EXPORT int32_t qk_sur_heston_load(qk_sur_model* model, const char* path);
+/* Prices a Heston batch: options whose features lie in the training box are
+ * priced by the surrogate (puts by put-call parity), the others by the Heston
+ * Monte Carlo with fallback_paths x fallback_steps and seed fallback_seed + i.
+ * out_source[i]: 0 surrogate, 1 Monte Carlo fallback, 2 no simulation (invalid
+ * input -> NaN, or t <= 1e-12 -> intrinsic value).  May be NULL. */
+QK_EXPORT int32_t qk_sur_heston_price_batch(
+    qk_sur_model* model, const double* spot, const double* strike, const double* t,
+    const double* r, const double* q, const double* v0, const double* kappa, const double* theta,
+    const double* sigma, const double* rho, const int32_t* option_type, int32_t n,
+    int32_t fallback_paths, int32_t fallback_steps, uint64_t fallback_seed, double* out_prices,
+    int32_t* out_source);
+
 #ifdef __cplusplus
 }
 #endif

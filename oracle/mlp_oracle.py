@@ -1,0 +1,71 @@
+"""FP64 reference of the surrogate MLP (9 -> 256 -> 256 -> 256 -> 1, SiLU) and
+of its mean-squared-error gradients, in numpy.
+
+TEST INFRASTRUCTURE ONLY: the checker for the GPU's tcgen05 forward/backward
+kernels.  The reference library has no such network; this is the plain
+mathematics of the architecture the surrogate specifies.  Parameter order:
+W1[256][9], b1, W2[256][256], b2, W3[256][256], b3, w4[256], b4.
+"""
+
+import numpy as np
+
+HID, IN = 256, 9
+SHAPES = [("W1", (HID, IN)), ("b1", (HID,)), ("W2", (HID, HID)), ("b2", (HID,)),
+          ("W3", (HID, HID)), ("b3", (HID,)), ("w4", (HID,)), ("b4", (1,))]
+N_PARAMS = sum(int(np.prod(s)) for _, s in SHAPES)
+
+
+def unpack(p):
+    out, k = {}, 0
+    for name, shape in SHAPES:
+        n = int(np.prod(shape))
+        out[name] = np.asarray(p[k:k + n], np.float64).reshape(shape)
+        k += n
+    return out
+
+
+def pack(d):
+    return np.concatenate([d[name].reshape(-1) for name, _ in SHAPES])
+
+
+def _sig(z):
+    return 1.0 / (1.0 + np.exp(-z))
+
+
+def forward(p, x):
+    w = unpack(p)
+    z1 = x @ w["W1"].T + w["b1"]
+    h1 = z1 * _sig(z1)
+    z2 = h1 @ w["W2"].T + w["b2"]
+    h2 = z2 * _sig(z2)
+    z3 = h2 @ w["W3"].T + w["b3"]
+    h3 = z3 * _sig(z3)
+    y = h3 @ w["w4"] + w["b4"][0]
+    return y, (z1, h1, z2, h2, z3, h3)
+
+
+def loss_and_grads(p, x, t):
+    """Mean squared error over the batch and its gradient (parameter order)."""
+    w = unpack(p)
+    y, (z1, h1, z2, h2, z3, h3) = forward(p, x)
+    n = x.shape[0]
+    loss = float(np.mean((y - t) ** 2))
+    dy = 2.0 * (y - t) / n
+
+    def dsilu(z):
+        s = _sig(z)
+        return s * (1.0 + z * (1.0 - s))
+
+    g = {"w4": h3.T @ dy, "b4": np.array([dy.sum()])}
+    dz3 = np.outer(dy, w["w4"]) * dsilu(z3)
+    g["W3"], g["b3"] = dz3.T @ h2, dz3.sum(0)
+    dz2 = (dz3 @ w["W3"]) * dsilu(z2)
+    g["W2"], g["b2"] = dz2.T @ h1, dz2.sum(0)
+    dz1 = (dz2 @ w["W2"]) * dsilu(z1)
+    g["W1"], g["b1"] = dz1.T @ x, dz1.sum(0)
+    return loss, pack(g)
+
+
+def bf16_bits_to_float(bits):
+    """bf16 bit patterns (uint16) to float64."""
+    return (np.asarray(bits, np.uint16).astype(np.uint32) << 16).view(np.float32).astype(np.float64)

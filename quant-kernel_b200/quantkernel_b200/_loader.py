@@ -76,6 +76,19 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_plan_config", I32, [VP, PI32, PI32, PI32]),
     ("qk_mcm_plan_destroy", I32, [VP]),
     ("qk_sur_gemm_bf16", I32, [VP, VP, VP, I32, I32, I32, I32, VP]),
+    ("qk_sur_heston_create", I32, [PD, PD, U64, ct.POINTER(VP)]),
+    ("qk_sur_heston_destroy", I32, [VP]),
+    ("qk_sur_heston_set_dataset", I32, [VP, PD, PD, I64]),
+    ("qk_sur_heston_train", I32, [VP, I32, I32, D, U64, PD]),
+    ("qk_sur_heston_predict", I32, [VP, PD, I64, PD]),
+    ("qk_sur_heston_predict_device", I32, [VP, VP, I64, VP, VP]),
+    ("qk_sur_heston_features", I32, [VP, PD, I64, VP]),
+    ("qk_sur_heston_gradients", I32, [VP, PD, PD, I32, PD, PD]),
+    ("qk_sur_heston_parameters", I32, [VP, PD]),
+    ("qk_sur_heston_set_parameters", I32, [VP, PD]),
+    ("qk_sur_heston_save", I32, [VP, ct.c_char_p]),
+    ("qk_sur_heston_load", I32, [VP, ct.c_char_p]),
+    ("qk_sur_heston_price_batch", I32, [VP] + [PD] * 10 + [PI32, I32, I32, I32, U64, PD, PI32]),
 ]
 
 

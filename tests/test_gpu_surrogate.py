@@ -1,0 +1,155 @@
+"""The Heston surrogate on the GPU: tcgen05 forward/backward gradients against
+the FP64 oracle, learning from the library's own Monte Carlo labels,
+determinism, checkpoints, box routing with Monte Carlo fallback, and what the
+trained network gains over Monte Carlo alone."""
+
+import time
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+from quantkernel_b200.surrogate import (HESTON_BOX_HI, HESTON_BOX_LO, N_PARAMS, HestonSurrogate,
+                                        features_of, sample_box)
+
+pytestmark = pytest.mark.gpu
+
+
+def _label(qk, n, paths, steps, seed):
+    b = sample_box(n, seed)
+    ones = np.ones(n)
+    price, se = qk.heston_monte_carlo_price_se_batch(
+        b["spot"], b["strike"], b["t"], b["r"], b["q"], b["v0"], b["kappa"], b["theta"], b["sigma"],
+        b["rho"], np.zeros(n, np.int32), (paths * ones).astype(np.int32),
+        (steps * ones).astype(np.int32), np.arange(n, dtype=np.uint64) + np.uint64(seed * 1000003))
+    f = features_of(b["spot"], b["strike"], b["t"], b["r"], b["q"], b["v0"], b["kappa"], b["theta"],
+                    b["sigma"], b["rho"])
+    return f, price / b["spot"], se / b["spot"], b
+
+
+@pytest.fixture(scope="module")
+def data(qk):
+    train = _label(qk, 32768, 8192, 32, seed=1)
+    hold = _label(qk, 2048, 65536, 32, seed=2)
+    return train, hold
+
+
+def test_gradients_match_fp64_oracle(qk):
+    """Loss and all 134,401 gradients of one batch (256 rows) against the FP64
+    oracle evaluated on the same bf16 inputs and FP32 master weights.  The GPU
+    rounds weights and activations to bf16 (8-bit mantissa), so each layer's
+    gradient must agree in direction (cosine > 0.995) and to 5% in norm."""
+    sur = HestonSurrogate(qk, seed=3)
+    b = sample_box(256, 7)
+    f = features_of(b["spot"], b["strike"], b["t"], b["r"], b["q"], b["v0"], b["kappa"], b["theta"],
+                    b["sigma"], b["rho"])
+    t = np.random.default_rng(9).uniform(0.0, 0.3, 256)
+    loss, g = sur.gradients(f, t)
+    p = sur.parameters()
+    x = mo.bf16_bits_to_float(sur.feature_rows(f))[:, :9]
+    loss_ref, g_ref = mo.loss_and_grads(p, x, t)
+    assert abs(loss - loss_ref) <= 0.02 * loss_ref, (loss, loss_ref)
+    k = 0
+    for name, shape in mo.SHAPES:
+        n = int(np.prod(shape))
+        a, r = g[k:k + n], g_ref[k:k + n]
+        k += n
+        cos = float(a @ r / (np.linalg.norm(a) * np.linalg.norm(r)))
+        rel = float(np.linalg.norm(a - r) / np.linalg.norm(r))
+        print(f"{name}: cos {cos:.5f} rel {rel:.4f}")
+        assert cos > 0.995 and rel < 0.05, (name, cos, rel)
+
+
+def test_training_learns_heston_prices(qk, data):
+    (f, t, se, _), (hf, ht, hse, _) = data
+    sur = HestonSurrogate(qk, seed=11)
+    err0 = np.abs(sur.predict(hf) - ht).mean()
+    sur.set_dataset(f, t)
+    losses = sur.train(epochs=40, batch=1024, lr=2e-3, shuffle_seed=5)
+    err = np.abs(sur.predict(hf) - ht)
+    print(f"epoch loss {losses[0]:.3e} -> {losses[-1]:.3e}; hold-out |err|/S mean {err.mean():.2e} "
+          f"p99 {np.quantile(err, 0.99):.2e} (untrained {err0:.2e}); label SE/S {hse.mean():.1e}")
+    assert np.all(np.isfinite(losses)) and losses[-1] < 0.05 * losses[0]
+    assert err.mean() < 0.05 * err0 and err.mean() < 5e-3
+
+
+def test_training_is_deterministic(qk, data):
+    (f, t, _, _), _ = data
+    params = []
+    for _ in range(2):
+        sur = HestonSurrogate(qk, seed=4)
+        sur.set_dataset(f[:4096], t[:4096])
+        sur.train(epochs=3, batch=512, lr=1e-3, shuffle_seed=8)
+        params.append(sur.parameters())
+        sur.close()
+    np.testing.assert_array_equal(params[0], params[1])
+
+
+def test_checkpoint_roundtrip(qk, data, tmp_path):
+    (f, t, _, _), (hf, _, _, _) = data
+    a = HestonSurrogate(qk, seed=12)
+    a.set_dataset(f[:2048], t[:2048])
+    a.train(epochs=2, batch=256)
+    a.save(tmp_path / "sur.bin")
+    b = HestonSurrogate(qk, seed=99)
+    b.load(tmp_path / "sur.bin")
+    np.testing.assert_array_equal(a.parameters(), b.parameters())
+    np.testing.assert_array_equal(a.predict(hf), b.predict(hf))
+    # training resumes from the saved Adam state: both continue identically
+    for m in (a, b):
+        m.set_dataset(f[:2048], t[:2048])
+        m.train(epochs=1, batch=256, shuffle_seed=3)
+    np.testing.assert_array_equal(a.parameters(), b.parameters())
+
+
+def test_price_batch_routes_box_and_fallback(qk):
+    sur = HestonSurrogate(qk, seed=5)
+    n = 8
+    args = dict(spot=np.full(n, 100.0), strike=np.array([90, 100, 110, 120, 100, 100, 100, 90.0]),
+                t=np.array([1, 0.5, 1.5, 1, 1, 1, 1, 1e-14]), r=np.full(n, 0.03), q=np.zeros(n),
+                v0=np.full(n, 0.04), kappa=np.full(n, 2.0), theta=np.full(n, 0.04),
+                sigma=np.array([0.3, 0.3, 0.3, 0.3, 1.5, 0.3, 0.3, 0.3]), rho=np.full(n, -0.5),
+                option_type=np.array([0, 1, 0, 1, 0, 0, 0, 1], np.int32))
+    args["q"][5] = 0.01     # q outside the box (the box has q = 0)
+    args["spot"][6] = -1.0  # invalid
+    price, src = sur.price_batch(**args, fallback_paths=4096, fallback_steps=16, fallback_seed=77)
+    assert list(src) == [0, 0, 0, 0, 1, 1, 2, 2]
+    assert np.isnan(price[6]) and price[7] == 0.0  # put, S > K, t -> 0: intrinsic 0
+    mc_idx = [4, 5]
+    direct = qk.heston_monte_carlo_price_batch(
+        *(args[k][mc_idx] for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho")),
+        args["option_type"][mc_idx], np.full(2, 4096, np.int32), np.full(2, 16, np.int32),
+        np.array(mc_idx, np.uint64) + np.uint64(77))
+    np.testing.assert_array_equal(price[mc_idx], direct)
+    # puts come from the network's call by put-call parity
+    f = features_of(*(args[k][[1]] for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta",
+                                             "sigma", "rho")))
+    call = 100.0 * sur.predict(f)[0]
+    assert abs(price[1] - (call - 100.0 + 100.0 * np.exp(-0.03 * 0.5))) < 1e-10
+
+
+def test_trained_network_gain_over_monte_carlo(qk, data):
+    """Prices per second of the trained network against the plain GPU Monte
+    Carlo at the benchmark's 200 steps x 262144 paths, and the network's error
+    against Monte Carlo judges (65536-path labels)."""
+    (f, t, _, _), (hf, ht, hse, hb) = data
+    sur = HestonSurrogate(qk, seed=11)
+    sur.set_dataset(f, t)
+    sur.train(epochs=40, batch=1024, lr=2e-3, shuffle_seed=5)
+    q = np.tile(hf, (128, 1))  # 262,144 queries
+    sur.predict(q[:1024])
+    t0 = time.perf_counter()
+    sur.predict(q)
+    sur_rate = q.shape[0] / (time.perf_counter() - t0)
+    m = 16
+    args = [hb[k][:m] for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho")]
+    extra = (np.zeros(m, np.int32), np.full(m, 262144, np.int32), np.full(m, 200, np.int32),
+             np.arange(m, dtype=np.uint64))
+    qk.heston_monte_carlo_price_batch(*args, *extra)
+    t0 = time.perf_counter()
+    qk.heston_monte_carlo_price_batch(*args, *extra)
+    mc_rate = m / (time.perf_counter() - t0)
+    err = np.abs(sur.predict(hf) - ht)
+    print(f"surrogate {sur_rate:.3e} prices/s vs MC {mc_rate:.3e} prices/s "
+          f"(x{sur_rate / mc_rate:.0f}); |err|/S mean {err.mean():.2e}")
+    assert sur_rate > 100 * mc_rate
