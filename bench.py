@@ -241,7 +241,10 @@ def main_gpu(args):
     h = workloads.heston(n_opt, paths=PATHS, steps=STEPS, seed=2 + 1000 * rank,
                          seed_base=5000 + 10_000_000 * rank)
     units_per_step = int(n_opt) * PATHS * STEPS
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated (non-default) stream: the plan's kernels, the L2 flush and the
+    # timing events are all ordered on it
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     plan = qk.plan(model=np.full(n_opt, QK_MC_HESTON, np.int32), flags=QK_PLAN_TIMING, **h)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -566,6 +569,7 @@ def mixed_leg(qk, reps=5):
     b = workloads.mixed()
     units = workloads.path_steps(b)
     stream = torch.cuda.current_stream()
+    assert stream.cuda_stream != 0, "time on a non-default stream"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     plan = qk.plan(**b, flags=QK_PLAN_PERSISTENT | QK_PLAN_GRAPH | QK_PLAN_AUTOTUNE | QK_PLAN_TIMING)
     ms = _time_plan(plan, stream, flush, reps)
@@ -596,6 +600,7 @@ def bsm_terminal_leg(qk, reps=20):
 
     b = workloads.bsm_terminal()
     stream = torch.cuda.current_stream()
+    assert stream.cuda_stream != 0, "time on a non-default stream"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     plan = qk.plan(model=np.full(64, QK_MC_STANDARD, np.int32), flags=QK_PLAN_GRAPH, **b)
     ms = _time_plan(plan, stream, flush, reps)

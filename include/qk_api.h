@@ -95,6 +95,19 @@ QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_batch(
     const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
     const uint64_t* seed, int32_t n, double* out_prices);
 
+/* qk_api.h:375-380 (heston_lr_delta.cpp:37-132: likelihood-ratio delta,
+ * antithetic pairs, score clipped to +-weight_clip) */
+QK_EXPORT double qk_mcm_heston_lr_delta(double spot, double strike, double t, double r, double q,
+                                        double v0, double kappa, double theta, double sigma,
+                                        double rho, int32_t option_type, int32_t paths,
+                                        int32_t steps, uint64_t seed, double weight_clip);
+/* qk_api.h:381-392 */
+QK_EXPORT int32_t qk_mcm_heston_lr_delta_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, const double* weight_clip, int32_t n, double* out_prices);
+
 /* qk_api.h:393-396 (local_vol_price_impl, constant sigma) */
 QK_EXPORT double qk_mcm_local_vol_monte_carlo_price(double spot, double strike, double t,
                                                     double vol, double r, double q,
@@ -125,6 +138,7 @@ QK_EXPORT int32_t qk_get_device(int32_t* device);
 #define QK_MC_LOCAL_VOL      4 /* constant local-vol Euler */
 #define QK_MC_TERMINAL_PLAIN 5 /* terminal GBM, independent paths */
 #define QK_MC_HESTON         6 /* Heston full-truncation Euler */
+#define QK_MC_HESTON_LR_DELTA 7 /* Heston likelihood-ratio delta; `vol` holds weight_clip */
 
 /* Plan flags. */
 #define QK_PLAN_PERSISTENT    0x1 /* one persistent work-stealing launch over all tiles */
@@ -182,6 +196,13 @@ QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_batch_noalloc(
     const double* v0, const double* kappa, const double* theta, const double* sigma,
     const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
     const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+
+QK_EXPORT int32_t qk_mcm_heston_lr_delta_se_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, const double* weight_clip, int32_t n, double* out_prices,
+    double* out_stderr);
 
 /* Mixed-model batch: option i is priced with model[i] (QK_MC_*).  Fields a
  * model does not use are ignored and may hold anything (vol for Heston;

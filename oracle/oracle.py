@@ -26,7 +26,7 @@ PU64 = ct.POINTER(U64)
 PU32 = ct.POINTER(U32)
 
 # Model codes shared with the GPU library (QK_MC_* in include/qk_api.h).
-STANDARD, ANTITHETIC, EULER, MILSTEIN, LOCAL_VOL, TERMINAL_PLAIN, HESTON = range(7)
+STANDARD, ANTITHETIC, EULER, MILSTEIN, LOCAL_VOL, TERMINAL_PLAIN, HESTON, HESTON_LR_DELTA = range(8)
 
 
 def _pd(a):
@@ -48,6 +48,7 @@ class Oracle:
             "qko_milstein": (D, step), "qko_local_vol": (D, step),
             "qko_heston": (D, [D] * 10 + [I32, I32, I32, U64, PD]),
             "qko_heston_batch": (None, [PD] * 10 + [PI32, PI32, PI32, PU64, I32, PD, PD]),
+            "qko_heston_lr_delta": (D, [D] * 10 + [I32, I32, I32, U64, D, PD]),
             "qko_bsm_family_batch": (None, [I32] + [PD] * 6 + [PI32, PI32, PI32, PU64, I32, PD, PD]),
             "qko_bsm_price": (D, [D] * 6 + [I32]),
             "qko_heston_cf_price": (D, [D] * 10 + [I32, I32, D]),
@@ -82,6 +83,9 @@ class Oracle:
         elif model == HESTON:
             p = L.qko_heston(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
                              paths, steps, seed, ct.byref(se))
+        elif model == HESTON_LR_DELTA:  # vol holds weight_clip
+            p = L.qko_heston_lr_delta(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                      option_type, paths, steps, seed, vol, ct.byref(se))
         else:
             raise ValueError(model)
         return p, se.value
@@ -166,6 +170,7 @@ class Reference:
             "qk_mcm_milstein_price": (D, step),
             "qk_mcm_local_vol_monte_carlo_price": (D, step),
             "qk_mcm_heston_monte_carlo_price": (D, [D] * 10 + [I32, I32, I32, U64]),
+            "qk_mcm_heston_lr_delta": (D, [D] * 10 + [I32, I32, I32, U64, D]),
             "qk_mcm_heston_monte_carlo_price_batch": (I32, [PD] * 10 + [PI32, PI32, PI32, PU64, I32, PD]),
             "qk_mcm_standard_monte_carlo_price_batch": (I32, [PD] * 6 + [PI32, PI32, PU64, I32, PD]),
             "qk_mcm_euler_maruyama_price_batch": (I32, [PD] * 6 + [PI32, PI32, PI32, PU64, I32, PD]),
@@ -194,6 +199,9 @@ class Reference:
         if model == HESTON:
             return L.qk_mcm_heston_monte_carlo_price(spot, strike, t, r, q, v0, kappa, theta, sigma,
                                                      rho, option_type, paths, steps, seed)
+        if model == HESTON_LR_DELTA:  # vol holds weight_clip
+            return L.qk_mcm_heston_lr_delta(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                            option_type, paths, steps, seed, vol)
         raise ValueError(model)
 
     def heston_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,

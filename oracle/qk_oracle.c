@@ -360,6 +360,86 @@ double qko_heston(double spot, double strike, double t, double r, double q, doub
     return disc * (sum / (double)paths);
 }
 
+/* std::min(a, b) is (b < a) ? b : a. */
+static double smin(double a, double b) { return (b < a) ? b : a; }
+
+/* heston_lr_delta.cpp:37-132.  Standard error over the pair samples
+ * (pf w - pa w) / 2; the unpaired path of an odd count is in the mean only. */
+double qko_heston_lr_delta(double spot, double strike, double t, double r, double q, double v0,
+                           double kappa, double theta, double sigma, double rho, int32_t ot,
+                           int32_t paths, int32_t steps, uint64_t seed, double weight_clip,
+                           double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
+        kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||
+        !valid_mc_counts(paths, steps) || weight_clip <= 0.0)
+        return qko_nan();
+    if (t <= QKO_EPS) {
+        if (ot == QKO_CALL) return (spot > strike) ? 1.0 : 0.0;
+        return (spot < strike) ? -1.0 : 0.0;
+    }
+    const double disc = exp(-r * t);
+    const double dt = t / (double)steps;
+    const double sqrt_dt = sqrt(dt);
+    const double sqrt_v0 = sqrt(smax(v0, 0.0));
+    const double rho_comp = sqrt(smax(1.0 - rho * rho, 0.0));
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    double sum = 0.0, ysum = 0.0, ysq = 0.0;
+    const int32_t n_pairs = paths / 2;
+#define LR_STEP(z1_, z2_)                                                                      \
+    do {                                                                                       \
+        const double v_pos = smax(v, 0.0);                                                     \
+        const double sqrt_v = sqrt(v_pos);                                                     \
+        const double dw1 = sqrt_dt * (z1_);                                                    \
+        const double dw2 = sqrt_dt * (rho * (z1_) + rho_comp * (z2_));                         \
+        const double s_next = s * exp((r - q - 0.5 * v_pos) * dt + sqrt_v * dw1);              \
+        v = smax(0.0, v + kappa * (theta - v_pos) * dt + sigma * sqrt_v * dw2);                \
+        s = smax(s_next, 1e-12);                                                               \
+    } while (0)
+    for (int32_t i = 0; i < n_pairs; ++i) {
+        qko_normal_gen saved = g;
+        double s = spot, v = v0, z1_first = 0.0;
+        for (int32_t j = 0; j < steps; ++j) {
+            const double z1 = qko_gen_normal(&g);
+            const double z2 = qko_gen_normal(&g);
+            if (j == 0) z1_first = z1;
+            LR_STEP(z1, z2);
+        }
+        const double pf = intrinsic(s, strike, ot);
+        double score = (sqrt_v0 > 1e-15) ? z1_first / (sqrt_v0 * sqrt_dt * spot) : 0.0;
+        score = smax(-weight_clip, smin(weight_clip, score));
+        s = spot;
+        v = v0;
+        for (int32_t j = 0; j < steps; ++j) {
+            const double z1 = -qko_gen_normal(&saved);
+            const double z2 = -qko_gen_normal(&saved);
+            LR_STEP(z1, z2);
+        }
+        const double pa = intrinsic(s, strike, ot);
+        const double y = pf * score + pa * (-score);
+        sum += y;
+        ysum += 0.5 * y;
+        ysq += 0.25 * y * y;
+    }
+    if ((paths & 1) != 0) {
+        double s = spot, v = v0, z1_first = 0.0;
+        for (int32_t j = 0; j < steps; ++j) {
+            const double z1 = qko_gen_normal(&g);
+            const double z2 = qko_gen_normal(&g);
+            if (j == 0) z1_first = z1;
+            LR_STEP(z1, z2);
+        }
+        const double p = intrinsic(s, strike, ot);
+        double score = (sqrt_v0 > 1e-15) ? z1_first / (sqrt_v0 * sqrt_dt * spot) : 0.0;
+        score = smax(-weight_clip, smin(weight_clip, score));
+        sum += p * score;
+    }
+#undef LR_STEP
+    if (se) *se = se_from_moments(disc, ysum, ysq, (double)n_pairs);
+    return disc * sum / (double)paths;
+}
+
 void qko_heston_batch(const double* spot, const double* strike, const double* t,
                       const double* r, const double* q, const double* v0, const double* kappa,
                       const double* theta, const double* sigma, const double* rho,
@@ -589,7 +669,7 @@ static double replay_path(int32_t model, double spot, double t, double vol, doub
     }
     const double dt = t / (double)steps;
     const double sqrt_dt = sqrt(dt);
-    if (model == 6) {
+    if (model == 6 || model == 7) {
         const double rho_comp = sqrt(smax(1.0 - rho * rho, 0.0));
         double s = spot, v = v0;
         for (int32_t j = 0; j < steps; ++j) {
@@ -625,6 +705,51 @@ double qko_philox_price(int32_t model, double spot, double strike, double t, dou
                         int32_t antithetic, double* se) {
     if (se) *se = qko_nan();
     /* entry checks and special cases of the matching reference pricer */
+    if (model == 7) {
+        const double clip = vol;
+        if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
+            kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||
+            !valid_mc_counts(paths, steps) || !(clip > 0.0))
+            return qko_nan();
+        if (t <= QKO_EPS) {
+            if (ot == QKO_CALL) return (spot > strike) ? 1.0 : 0.0;
+            return (spot < strike) ? -1.0 : 0.0;
+        }
+        const double disc = exp(-r * t);
+        const double sqrt_dt = sqrt(t / (double)steps);
+        const double sqrt_v0 = sqrt(smax(v0, 0.0));
+        double sum = 0.0, ysum = 0.0, ysq = 0.0, ny = 0.0;
+        const int32_t units = antithetic ? paths - paths / 2 : paths;
+        const int32_t n_pairs = paths / 2;
+        for (int32_t u = 0; u < units; ++u) {
+            double z4[4];
+            qko_philox_normals4(seed, (uint32_t)u, 0u, antithetic ? 0u : 1u, z4);
+            double w = (sqrt_v0 > 1e-15) ? z4[0] / (sqrt_v0 * sqrt_dt * spot) : 0.0;
+            w = smax(-clip, smin(clip, w));
+            const double a = intrinsic(replay_path(6, spot, t, vol, r, q, v0, kappa, theta, sigma,
+                                                   rho, steps, seed, (uint32_t)u,
+                                                   antithetic ? 0u : 1u, 1.0), strike, ot) * w;
+            if (antithetic && u < n_pairs) {
+                const double b = intrinsic(replay_path(6, spot, t, vol, r, q, v0, kappa, theta,
+                                                       sigma, rho, steps, seed, (uint32_t)u, 0u,
+                                                       -1.0), strike, ot) * (-w);
+                sum += a + b;
+                const double m = 0.5 * (a + b);
+                ysum += m;
+                ysq += m * m;
+                ny += 1.0;
+            } else if (antithetic) {
+                sum += a;
+            } else {
+                sum += a;
+                ysum += a;
+                ysq += a * a;
+                ny += 1.0;
+            }
+        }
+        if (se) *se = se_from_moments(disc, ysum, ysq, ny);
+        return disc * (sum / (double)paths);
+    }
     if (model == 6) {
         if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
             kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||

@@ -65,6 +65,13 @@ double qko_heston(double spot, double strike, double t, double r, double q,
                   double v0, double kappa, double theta, double sigma, double rho,
                   int32_t option_type, int32_t paths, int32_t steps, uint64_t seed, double* se);
 
+/* heston_lr_delta.cpp:37-132: likelihood-ratio delta with antithetic pairs
+ * (the RNG state is copied before each pair and replayed negated). */
+double qko_heston_lr_delta(double spot, double strike, double t, double r, double q,
+                           double v0, double kappa, double theta, double sigma, double rho,
+                           int32_t option_type, int32_t paths, int32_t steps, uint64_t seed,
+                           double weight_clip, double* se);
+
 /* Batch forms (OpenMP over options when built with it).  out_se may be NULL. */
 void qko_heston_batch(const double* spot, const double* strike, const double* t,
                       const double* r, const double* q, const double* v0,
@@ -92,7 +99,8 @@ double qko_heston_cf_price(double spot, double strike, double t, double r, doubl
 void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* The GPU's normal with index k of stream (seed, c0, c1, c3); see qk_oracle.c. */
 void qko_philox_normals4(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[4]);
-/* model as in qko_bsm_family_batch, plus 6 = Heston (uses v0..rho; vol ignored).
+/* model as in qko_bsm_family_batch, plus 6 = Heston (uses v0..rho; vol ignored)
+ * and 7 = Heston likelihood-ratio delta (vol holds weight_clip).
  * antithetic: 1 = pairs (GPU default), 0 = independent paths. */
 double qko_philox_price(int32_t model, double spot, double strike, double t, double vol,
                         double r, double q, double v0, double kappa, double theta,

@@ -156,7 +156,12 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 // v >= 0 after every step (and v0 >= 0 is validated), so the reference's
 // v_pos = max(v, 0) is v itself.  One Philox call feeds two steps of a unit.
 // ----------------------------------------------------------------------------
-template <int UPT, bool ANTI>
+//
+// LR = true: the likelihood-ratio delta of heston_lr_delta.cpp:37-132.  Each
+// path's payoff is weighted by the score of its first spot step,
+// w = clamp(z1_0 / (sqrt(v0) sqrt(dt) S0), -clip, clip); the antithetic path's
+// score is -w.
+template <int UPT, bool ANTI, bool LR>
 __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, uint32_t stride,
                                            uint32_t k0, uint32_t k1, Acc& acc) {
     const float cmu = o.p[0], hdt = o.p[1], sqdt = o.p[2], kdt = o.p[3], kth = o.p[4];
@@ -167,17 +172,23 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
     const uint32_t units = (uint32_t)o.units;
     const uint32_t c3 = ANTI ? 0u : 1u;
     float xu[UPT], vu[UPT], xd[UPT], vd[UPT];
+    float zfirst[UPT];
 #pragma unroll
     for (int k = 0; k < UPT; ++k) {
         xu[k] = 0.0f;
         xd[k] = 0.0f;
         vu[k] = v0;
         vd[k] = v0;
+        zfirst[k] = 0.0f;
     }
     for (int32_t j = 0; j < steps; j += 2) {
         float z[UPT][4];
 #pragma unroll
         for (int k = 0; k < UPT; ++k) normals4(unit0 + (uint32_t)k * stride, (uint32_t)(j >> 1), c3, k0, k1, z[k]);
+        if (LR && j == 0) {
+#pragma unroll
+            for (int k = 0; k < UPT; ++k) zfirst[k] = z[k][0];
+        }
         const int32_t m = (steps - j) < 2 ? (steps - j) : 2;
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
@@ -204,14 +215,18 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         }
     }
     const uint32_t n_pairs = (uint32_t)o.paths >> 1;
+    // score scale 1 / (sqrt(v0) sqrt(dt) S0); v0 = 0 is a constant-zero option
+    const double wscale = LR ? 1.0 / ((double)ptx_sqrt(v0) * (double)sqdt * o.spot) : 0.0;
 #pragma unroll
     for (int k = 0; k < UPT; ++k) {
         const uint32_t unit = unit0 + (uint32_t)k * stride;
         if (unit >= units) continue;
-        const double pu = payoff(o.spot * exp((double)xu[k]), o.strike, o.option_type);
+        double w = 1.0;
+        if (LR) w = fmin(o.weight_clip, fmax(-o.weight_clip, (double)zfirst[k] * wscale));
+        const double pu = payoff(o.spot * exp((double)xu[k]), o.strike, o.option_type) * w;
         if (ANTI) {
             if (unit < n_pairs)
-                acc.add_pair(pu, payoff(o.spot * exp((double)xd[k]), o.strike, o.option_type));
+                acc.add_pair(pu, payoff(o.spot * exp((double)xd[k]), o.strike, o.option_type) * (LR ? -w : 1.0));
             else
                 acc.add_lone(pu);
         } else {
@@ -283,7 +298,8 @@ __device__ __forceinline__ void sim_family(const McOption& o, uint32_t unit0, ui
     if (FAMILY == kFamTerminal) sim_terminal<UPT, ANTI>(o, unit0, stride, k0, k1, acc);
     if (FAMILY == kFamEuler) sim_stepwise<UPT, ANTI, false>(o, unit0, stride, k0, k1, acc);
     if (FAMILY == kFamMilstein) sim_stepwise<UPT, ANTI, true>(o, unit0, stride, k0, k1, acc);
-    if (FAMILY == kFamHeston) sim_heston<UPT, ANTI>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamHeston) sim_heston<UPT, ANTI, false>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamHestonLr) sim_heston<UPT, ANTI, true>(o, unit0, stride, k0, k1, acc);
 }
 
 // One tile: all UPT * unit_iters units of every thread, then the reduction.
@@ -365,6 +381,12 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
                     run_tile<kFamMilstein, BLOCK, kUptStepwise, true>(o, tile, partials, smem);
                 else
                     run_tile<kFamMilstein, BLOCK, kUptStepwise, false>(o, tile, partials, smem);
+                break;
+            case kHestonLrDelta:
+                if (anti)
+                    run_tile<kFamHestonLr, BLOCK, kUptHeston, true>(o, tile, partials, smem);
+                else
+                    run_tile<kFamHestonLr, BLOCK, kUptHeston, false>(o, tile, partials, smem);
                 break;
             default:  // kHeston
                 if (anti)
@@ -473,6 +495,7 @@ int family_of(int32_t model) {
         case kEuler:
         case kLocalVol: return kFamEuler;
         case kMilstein: return kFamMilstein;
+        case kHestonLrDelta: return kFamHestonLr;
         default: return kFamHeston;
     }
 }
@@ -485,6 +508,7 @@ cudaError_t launch_simulate(int family, bool anti, int block, int upt, const Sim
         case kFamEuler: return launch_anti<kFamEuler>(anti, block, upt, a, st);
         case kFamMilstein: return launch_anti<kFamMilstein>(anti, block, upt, a, st);
         case kFamHeston: return launch_anti<kFamHeston>(anti, block, upt, a, st);
+        case kFamHestonLr: return launch_anti<kFamHestonLr>(anti, block, upt, a, st);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -10,7 +10,14 @@ struct McOption;
 struct TilePartial;
 
 // Kernel families: the models that share one simulation loop.
-enum : int { kFamTerminal = 0, kFamEuler = 1, kFamMilstein = 2, kFamHeston = 3, kNumFamilies = 4 };
+enum : int {
+    kFamTerminal = 0,
+    kFamEuler = 1,
+    kFamMilstein = 2,
+    kFamHeston = 3,
+    kFamHestonLr = 4,
+    kNumFamilies = 5
+};
 
 // Units per thread compiled into the persistent mixed-model kernel.
 constexpr int kUptTerminal = 1;

@@ -89,12 +89,19 @@ struct DeviceGuard {
     }
 };
 
+// Device name (the autotuner's cache key), looked up once per device:
+// cudaGetDeviceProperties costs milliseconds.
 std::string device_name(int dev) {
+    static std::mutex mu;
+    static std::map<int, std::string> names;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = names.find(dev);
+    if (it != names.end()) return it->second;
     cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return "unknown";
-    std::string s = prop.name;
+    std::string s = cudaGetDeviceProperties(&prop, dev) == cudaSuccess ? prop.name : "unknown";
     for (char& c : s)
         if (c == ' ' || c == '|') c = '_';
+    names[dev] = s;
     return s;
 }
 
@@ -166,7 +173,7 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
         o.p[3] = (float)c;
         return o;
     }
-    if (m == kHeston) {
+    if (m == kHeston || m == kHestonLrDelta) {
         const double r = in.r[i], q = in.q[i];
         const double v0 = in.v0[i], kappa = in.kappa[i], theta = in.theta[i];
         const double sigma = in.sigma[i], rho = in.rho[i];
@@ -174,16 +181,27 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
         o.steps = steps;
         // heston_monte_carlo.cpp:18-24 -- no finiteness test: a NaN passes the
         // comparisons and flows through the simulation as in the reference.
+        // heston_lr_delta.cpp:46-53 adds weight_clip <= 0 -> NaN; a NaN clip
+        // propagates to a NaN delta there, so it is rejected here.
+        const double clip = (m == kHestonLrDelta) ? (in.weight_clip ? in.weight_clip[i] : in.vol[i]) : 1.0;
         if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
             kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||
-            !(paths > 1 && steps > 0)) {
+            !(paths > 1 && steps > 0) || !(clip > 0.0)) {
             set_const(o, nan_value());
             return o;
         }
         if (t <= kEps) {
-            set_const(o, intrinsic(spot, strike, ot));
+            if (m == kHestonLrDelta)  // heston_lr_delta.cpp:56-60: intrinsic delta
+                set_const(o, ot == 0 ? (spot > strike ? 1.0 : 0.0) : (spot < strike ? -1.0 : 0.0));
+            else
+                set_const(o, intrinsic(spot, strike, ot));
             return o;
         }
+        if (m == kHestonLrDelta && !(std::sqrt(smax(v0, 0.0)) > 1e-15)) {
+            set_const(o, 0.0);  // every score is 0 (heston_lr_delta.cpp:91-93)
+            return o;
+        }
+        if (m == kHestonLrDelta) o.weight_clip = clip;
         o.disc = std::exp(-r * t);
         o.antithetic = anti_stepwise ? 1 : 0;
         o.units = o.antithetic ? paths - paths / 2 : paths;

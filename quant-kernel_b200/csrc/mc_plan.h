@@ -21,6 +21,7 @@ struct BatchInput {
                  *q = nullptr;
     const double *v0 = nullptr, *kappa = nullptr, *theta = nullptr, *sigma = nullptr,
                  *rho = nullptr;
+    const double* weight_clip = nullptr;  // Heston LR delta; null: taken from `vol`
     const int32_t *option_type = nullptr, *paths = nullptr, *steps = nullptr;
     const uint64_t* seed = nullptr;
     int32_t n = 0;

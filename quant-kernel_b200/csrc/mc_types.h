@@ -16,7 +16,8 @@ enum : int32_t {
     kLocalVol = 4,
     kTerminalPlain = 5,
     kHeston = 6,
-    kNumModels = 7
+    kHestonLrDelta = 7,  // likelihood-ratio delta under the Heston model
+    kNumModels = 8
 };
 
 enum : int32_t { kModeSimulate = 0, kModeConstant = 1 };
@@ -35,12 +36,17 @@ enum : int32_t { kModeSimulate = 0, kModeConstant = 1 };
 //                      p5 = sigma sqrt(dt)           p6 = rho
 //                      p7 = sqrt(max(1 - rho^2, 0))  p8 = v0
 //                      p9 = log(1e-12 / spot) (floor of log(S/spot))
+//   Heston LR delta (7): the Heston constants; the record's weight_clip
+//                      bounds the first-step score z1 / (sqrt(v0) sqrt(dt) S0)
 // ---------------------------------------------------------------------------
 struct alignas(16) McOption {
     double spot;
     double strike;
     double disc;         // exp(-r t)
-    double const_price;  // result when mode == kModeConstant
+    union {
+        double const_price;  // result when mode == kModeConstant
+        double weight_clip;  // Heston LR delta (simulated): |score| bound
+    };
     uint64_t seed;
     int64_t tile_begin;  // first tile of this option in the plan
     int32_t tiles;       // tiles of this option (0 when constant)

@@ -190,10 +190,13 @@ int32_t mixed_input(const int32_t* model, const double* spot, const double* stri
     bool need_vol = false, need_heston = false, need_steps = false;
     for (int32_t i = 0; i < n; ++i) {
         const int32_t m = model[i];
-        if (m >= qkb::kStandard && m <= qkb::kTerminalPlain) need_vol = true;
-        if (m == qkb::kEuler || m == qkb::kMilstein || m == qkb::kLocalVol || m == qkb::kHeston)
+        // the LR delta reads its weight clip from `vol`
+        if ((m >= qkb::kStandard && m <= qkb::kTerminalPlain) || m == qkb::kHestonLrDelta)
+            need_vol = true;
+        if (m == qkb::kEuler || m == qkb::kMilstein || m == qkb::kLocalVol || m == qkb::kHeston ||
+            m == qkb::kHestonLrDelta)
             need_steps = true;
-        if (m == qkb::kHeston) need_heston = true;
+        if (m == qkb::kHeston || m == qkb::kHestonLrDelta) need_heston = true;
     }
     if (need_vol && !vol) return fail_null("vol");
     if (need_heston) {
@@ -431,6 +434,65 @@ int32_t qk_mcm_heston_monte_carlo_price_batch_noalloc(
         default:
             return fail_cuda(e, "qk_mcm_heston_monte_carlo_price_batch_noalloc");
     }
+}
+
+// ---- Heston likelihood-ratio delta ------------------------------------------------
+static int32_t lr_delta_batch(const double* spot, const double* strike, const double* t, const double* r,
+                       const double* q, const double* v0, const double* kappa, const double* theta,
+                       const double* sigma, const double* rho, const int32_t* option_type,
+                       const int32_t* paths, const int32_t* steps, const uint64_t* seed,
+                       const double* weight_clip, int32_t n, double* out_prices, double* out_se,
+                       bool want_se, const char* where) {
+    const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {r, "r"}, {q, "q"},
+                             {v0, "v0"}, {kappa, "kappa"}, {theta, "theta"}, {sigma, "sigma"},
+                             {rho, "rho"}, {option_type, "option_type"}, {paths, "paths"},
+                             {steps, "steps"}, {seed, "seed"}, {weight_clip, "weight_clip"},
+                             {out_prices, "out_prices"}};
+    if (int32_t rc = check_nulls(ptrs)) return rc;
+    if (want_se && !out_se) return fail_null("out_stderr");
+    if (n <= 0) return fail_size(n);
+    qkb::BatchInput in = heston_input(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                      option_type, paths, steps, seed, n);
+    in.uniform_model = qkb::kHestonLrDelta;
+    in.weight_clip = weight_clip;
+    return run_batch(in, 0, out_prices, out_se, where);
+}
+
+int32_t qk_mcm_heston_lr_delta_batch(const double* spot, const double* strike, const double* t,
+                                     const double* r, const double* q, const double* v0,
+                                     const double* kappa, const double* theta, const double* sigma,
+                                     const double* rho, const int32_t* option_type,
+                                     const int32_t* paths, const int32_t* steps,
+                                     const uint64_t* seed, const double* weight_clip, int32_t n,
+                                     double* out_prices) {
+    return lr_delta_batch(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type, paths,
+                          steps, seed, weight_clip, n, out_prices, nullptr, false,
+                          "qk_mcm_heston_lr_delta_batch");
+}
+
+int32_t qk_mcm_heston_lr_delta_se_batch(const double* spot, const double* strike, const double* t,
+                                        const double* r, const double* q, const double* v0,
+                                        const double* kappa, const double* theta,
+                                        const double* sigma, const double* rho,
+                                        const int32_t* option_type, const int32_t* paths,
+                                        const int32_t* steps, const uint64_t* seed,
+                                        const double* weight_clip, int32_t n, double* out_prices,
+                                        double* out_stderr) {
+    return lr_delta_batch(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type, paths,
+                          steps, seed, weight_clip, n, out_prices, out_stderr, true,
+                          "qk_mcm_heston_lr_delta_se_batch");
+}
+
+double qk_mcm_heston_lr_delta(double spot, double strike, double t, double r, double q, double v0,
+                              double kappa, double theta, double sigma, double rho,
+                              int32_t option_type, int32_t paths, int32_t steps, uint64_t seed,
+                              double weight_clip) {
+    double out = nan_value();
+    if (qk_mcm_heston_lr_delta_batch(&spot, &strike, &t, &r, &q, &v0, &kappa, &theta, &sigma, &rho,
+                                     &option_type, &paths, &steps, &seed, &weight_clip, 1,
+                                     &out) != QK_OK)
+        return nan_value();
+    return out;
 }
 
 // ---- mixed batch and plans -------------------------------------------------------

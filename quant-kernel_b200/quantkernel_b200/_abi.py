@@ -22,6 +22,7 @@ QK_MC_MILSTEIN = 3
 QK_MC_LOCAL_VOL = 4
 QK_MC_TERMINAL_PLAIN = 5
 QK_MC_HESTON = 6
+QK_MC_HESTON_LR_DELTA = 7
 
 QK_PLAN_PERSISTENT = 0x1
 QK_PLAN_GRAPH = 0x2

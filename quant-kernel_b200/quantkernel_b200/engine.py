@@ -366,6 +366,36 @@ class QuantKernel:
                                                             paths, steps, seed),
                                        with_se=True)
 
+    def heston_lr_delta(self, spot: float, strike: float, t: float, r: float, q: float,
+                        v0: float, kappa: float, theta: float, sigma: float, rho: float,
+                        option_type: int, paths: int, steps: int, seed: int = 42,
+                        weight_clip: float = 6.0) -> float:
+        """Likelihood-ratio delta under Heston (heston_lr_delta.cpp:37-132)."""
+        return self._call_checked("qk_mcm_heston_lr_delta", spot, strike, t, r, q, v0, kappa,
+                                  theta, sigma, rho, option_type, paths, steps, seed, weight_clip)
+
+    def _lr_arrays(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type, paths,
+                   steps, seed, weight_clip):
+        arrs = self._heston_arrays(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                   option_type, paths, steps, seed)
+        wc = self._as_f64_array(weight_clip, "weight_clip")
+        self._check_same_length(arrs[0].shape[0], weight_clip=wc)
+        return (*arrs, wc)
+
+    def heston_lr_delta_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                              option_type, paths, steps, seed, weight_clip) -> np.ndarray:
+        return self._call_batch_ctypes("qk_mcm_heston_lr_delta_batch",
+                                       *self._lr_arrays(spot, strike, t, r, q, v0, kappa, theta,
+                                                        sigma, rho, option_type, paths, steps,
+                                                        seed, weight_clip))
+
+    def heston_lr_delta_se_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                 option_type, paths, steps, seed, weight_clip):
+        return self._call_batch_ctypes("qk_mcm_heston_lr_delta_se_batch",
+                                       *self._lr_arrays(spot, strike, t, r, q, v0, kappa, theta,
+                                                        sigma, rho, option_type, paths, steps,
+                                                        seed, weight_clip), with_se=True)
+
     # ------------------------------------------------------------------ mixed / plans
     def _mixed_arrays(self, model, spot, strike, t, vol, r, q, v0, kappa, theta, sigma, rho,
                       option_type, paths, steps, seed):

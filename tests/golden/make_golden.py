@@ -25,7 +25,7 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from oracle.oracle import (  # noqa: E402
-    ANTITHETIC, EULER, HESTON, LOCAL_VOL, MILSTEIN, STANDARD, Reference)
+    ANTITHETIC, EULER, HESTON, HESTON_LR_DELTA, LOCAL_VOL, MILSTEIN, STANDARD, Reference)
 
 OUT = Path(__file__).resolve().parent / "reference_mc.json"
 
@@ -92,6 +92,23 @@ def main() -> None:
     for field in ("spot", "strike", "q", "v0", "kappa", "theta", "sigma", "rho", "t", "r"):
         for ot in (0, 1):
             add(HESTON, **{field: float("nan")}, option_type=ot, paths=64, steps=4)
+
+    # Heston likelihood-ratio delta (heston_lr_delta.cpp); `vol` carries weight_clip
+    for _ in range(10):
+        add(HESTON_LR_DELTA, spot=float(rng.uniform(80, 120)), strike=float(rng.uniform(80, 120)),
+            t=float(rng.uniform(0.1, 2.0)), r=float(rng.uniform(0.0, 0.05)),
+            q=float(rng.uniform(0.0, 0.03)), option_type=int(rng.integers(0, 2)),
+            paths=int(rng.integers(2, 3000)), steps=int(rng.integers(1, 40)),
+            seed=int(rng.integers(0, 2**63)), v0=float(rng.uniform(0.01, 0.09)),
+            kappa=float(rng.uniform(0.5, 5)), theta=float(rng.uniform(0.01, 0.09)),
+            sigma=float(rng.uniform(0.1, 1.0)), rho=float(rng.uniform(-0.9, 0.0)),
+            vol=float(rng.choice([0.5, 2.0, 6.0])))
+    add(HESTON_LR_DELTA, vol=6.0, t=1e-14, spot=110.0)              # intrinsic delta 1
+    add(HESTON_LR_DELTA, vol=6.0, t=1e-14, spot=90.0, option_type=1)  # -1
+    add(HESTON_LR_DELTA, vol=0.0)                                     # clip <= 0 -> NaN
+    add(HESTON_LR_DELTA, vol=6.0, v0=0.0, paths=100, steps=4)         # zero score -> 0
+    add(HESTON_LR_DELTA, vol=6.0, paths=3, seed=5)                    # odd count
+    add(HESTON_LR_DELTA, vol=6.0, paths=1)                            # NaN
 
     cf = []
     for _ in range(24):

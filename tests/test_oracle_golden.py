@@ -10,8 +10,8 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from oracle.oracle import (ANTITHETIC, EULER, HESTON, LOCAL_VOL, MILSTEIN, STANDARD,
-                           TERMINAL_PLAIN)
+from oracle.oracle import (ANTITHETIC, EULER, HESTON, HESTON_LR_DELTA, LOCAL_VOL, MILSTEIN,
+                           STANDARD, TERMINAL_PLAIN)
 
 GOLDEN = json.loads((Path(__file__).parent / "golden" / "reference_mc.json").read_text())
 
@@ -45,7 +45,7 @@ def test_oracle_bitwise_equals_reference_fixture(oracle, i):
 
 def test_oracle_bitwise_equals_reference_live(oracle, ref):
     rng = np.random.default_rng(7)
-    for model in (STANDARD, ANTITHETIC, EULER, MILSTEIN, LOCAL_VOL, HESTON):
+    for model in (STANDARD, ANTITHETIC, EULER, MILSTEIN, LOCAL_VOL, HESTON, HESTON_LR_DELTA):
         for _ in range(5):
             a = dict(spot=float(rng.uniform(50, 150)), strike=float(rng.uniform(50, 150)),
                      t=float(rng.uniform(0.05, 3.0)), vol=float(rng.uniform(0.05, 0.8)),
