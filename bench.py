@@ -69,6 +69,9 @@ def parse():
                     help="label 4e6 Heston tuples with the GPU MC, train the surrogate, save it")
     ap.add_argument("--surrogate", action="store_true",
                     help="surrogate inference leg only (1e6 queries, MC fallback, MC judge)")
+    ap.add_argument("--heston-cf", action="store_true",
+                    help="Heston characteristic-function leg only")
+    ap.add_argument("--cf-options", type=int, default=65536)
     ap.add_argument("--sur-train-n", type=int, default=4_000_000)
     ap.add_argument("--sur-hold-n", type=int, default=100_000)
     ap.add_argument("--sur-epochs", type=int, default=60)
@@ -99,9 +102,34 @@ def _time_cpu(impl, n_opt, paths, threads):
     return dt, int(n_opt) * int(paths) * STEPS
 
 
+def _cf_cpu_leg(s):
+    """Reference (or oracle) Heston CF batch on a bounded sample of the CF workload."""
+    from oracle import oracle as orc
+    from quantkernel_b200 import workloads
+
+    b = workloads.heston_cf()
+    cap = len(b["spot"])
+    fn = (orc.Reference() if s["impl"] == "reference" else orc.Oracle()).heston_cf
+    n = 16
+    while True:
+        t0 = time.perf_counter()
+        if s["impl"] == "reference":
+            orc.Reference().heston_cf_batch(**{k: v[:n] for k, v in b.items()})
+        else:
+            for i in range(n):
+                fn(*(b[k][i].item() for k in b))
+        dt = time.perf_counter() - t0
+        if dt >= 0.5 * s["seconds"] or n >= cap:
+            break
+        n = min(cap, max(2 * n, int(n * s["seconds"] / max(dt, 1e-3))))
+    print(json.dumps({"options": n, "seconds": dt}))
+
+
 def cpu_leg(spec):
     """Runs in a subprocess with OMP_NUM_THREADS set; prints one JSON line."""
     s = json.loads(spec)
+    if s.get("kind") == "heston_cf":
+        return _cf_cpu_leg(s)
     target = s["seconds"]
     reps = s.get("reps", 1)
     n_opt, paths = 8, 4096
@@ -115,9 +143,10 @@ def cpu_leg(spec):
     print(json.dumps({"samples": out, "n_opt": 64, "paths": paths}))
 
 
-def run_cpu(impl, threads, seconds, reps=1):
+def run_cpu(impl, threads, seconds, reps=1, kind="heston_mc"):
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    spec = json.dumps({"impl": impl, "threads": threads, "seconds": seconds, "reps": reps})
+    spec = json.dumps({"impl": impl, "threads": threads, "seconds": seconds, "reps": reps,
+                       "kind": kind})
     r = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--cpu-leg", spec],
                        env=env, capture_output=True, text=True, timeout=1800)
     if r.returncode != 0:
@@ -359,6 +388,7 @@ def main_gpu(args):
     try:
         extras["mixed"] = mixed_leg(qk)
         extras["bsm_terminal"] = bsm_terminal_leg(qk)
+        extras["heston_cf"] = heston_cf_leg(qk)
         if Path(args.sur_checkpoint).exists():
             extras["surrogate"] = surrogate_infer_leg(qk, args.sur_checkpoint,
                                                       mc_prices_per_s=value / (PATHS * STEPS))
@@ -615,6 +645,37 @@ def bsm_terminal_leg(qk, reps=20):
             "e2e_paths_per_s": paths / e2e}
 
 
+def heston_cf_leg(qk, reps=5, n=65536, cpu=True):
+    """65536 Heston calls/puts by the characteristic-function pricer (1024
+    Gauss-Legendre nodes on [1e-8, 120], 2048 FP64 characteristic-function
+    evaluations per option) through qk_cf_heston_price_cf_batch with host
+    buffers; beside it the reference's OpenMP CPU batch on a bounded sample."""
+    from quantkernel_b200 import workloads
+
+    b = workloads.heston_cf(n)
+    for _ in range(2):
+        qk.heston_price_cf_batch(**b)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        out = qk.heston_price_cf_batch(**b)
+    e2e = (time.perf_counter() - t0) / reps
+    assert np.all(np.isfinite(out))
+    res = {"workload": f"{n} Heston calls/puts, CF with 1024 steps, limit 120",
+           "e2e_ms": 1e3 * e2e, "e2e_options_per_s": n / e2e,
+           "h2d_bytes": n * 112, "d2h_bytes": n * 8}
+    if not cpu:
+        return res
+    try:
+        threads = host_threads()
+        c = run_cpu(cpu_kind(), threads, seconds=5.0, kind="heston_cf")
+        res["cpu_baseline"] = {"value": c["options"] / c["seconds"], "unit": "options/s",
+                               "cores": threads, "kind": cpu_kind(),
+                               "sample": f"first {c['options']} options of the workload"}
+    except Exception as exc:
+        res["cpu_baseline"] = {"value": None, "sample": f"failed: {exc}"[:200]}
+    return res
+
+
 def main():
     args = parse()
     if args.surrogate_train:
@@ -628,6 +689,12 @@ def main():
         return 0
     if args.cpu_leg:
         cpu_leg(args.cpu_leg)
+        return 0
+    if args.heston_cf:
+        from quantkernel_b200 import QuantKernel
+
+        leg = heston_cf_leg(QuantKernel(), n=args.cf_options, cpu=not args.profile)
+        print(json.dumps({"leg": "heston_cf", **leg}), flush=True)
         return 0
     if args.impl == "reference":
         return reference_arm(args)

@@ -119,6 +119,20 @@ QK_EXPORT int32_t qk_mcm_local_vol_monte_carlo_price_batch(
     const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
     const uint64_t* seed, int32_t n, double* out_prices);
 
+/* qk_api.h:53-55 (heston.cpp:7-53: little-trap characteristic function,
+ * P1/P2 by ceil(integration_steps/64) panels of 64-point Gauss-Legendre on
+ * [1e-8, integration_limit]; FP64 on the GPU, one CTA per option) */
+QK_EXPORT double qk_cf_heston_price_cf(double spot, double strike, double t, double r, double q,
+                                       double v0, double kappa, double theta, double sigma,
+                                       double rho, int32_t option_type, int32_t integration_steps,
+                                       double integration_limit);
+/* qk_api.h:71-76 */
+QK_EXPORT int32_t qk_cf_heston_price_cf_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* integration_steps,
+    const double* integration_limit, int32_t n, double* out_prices);
+
 /* ======================================================================= *
  * Part 2 -- additions in ABI 2.13 (no counterpart in the reference)
  * ======================================================================= */

@@ -176,6 +176,7 @@ class Reference:
             "qk_mcm_euler_maruyama_price_batch": (I32, [PD] * 6 + [PI32, PI32, PI32, PU64, I32, PD]),
             "qk_cf_black_scholes_merton_price": (D, [D] * 6 + [I32]),
             "qk_cf_heston_price_cf": (D, [D] * 10 + [I32, I32, D]),
+            "qk_cf_heston_price_cf_batch": (I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -227,6 +228,22 @@ class Reference:
                   integration_steps=1024, integration_limit=120.0):
         return self.lib.qk_cf_heston_price_cf(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
                                               option_type, integration_steps, integration_limit)
+
+    def heston_cf_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                        integration_steps, integration_limit):
+        """qk_cf_heston_price_cf_batch (OpenMP over options for n >= 512)."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (spot, strike, t, r, q, v0, kappa, theta, sigma, rho)]
+        ot = np.ascontiguousarray(option_type, np.int32)
+        st = np.ascontiguousarray(integration_steps, np.int32)
+        lim = np.ascontiguousarray(integration_limit, np.float64)
+        n = a[0].shape[0]
+        out = np.empty(n)
+        rc = self.lib.qk_cf_heston_price_cf_batch(
+            *[_pd(x) for x in a], ot.ctypes.data_as(PI32), st.ctypes.data_as(PI32), _pd(lim), n,
+            _pd(out))
+        if rc != 0:
+            raise RuntimeError(f"reference batch rc={rc}")
+        return out
 
 
 def reference_available() -> bool:

@@ -502,6 +502,11 @@ double qko_bsm_price(double spot, double strike, double t, double vol, double r,
 
 /* 64-point Gauss-Legendre rule on [-1, 1]: the 32 positive nodes and their
  * weights, computed once by Newton's method on the Legendre recurrence. */
+static double clamp01(double x) {
+    const double lo = (0.0 < x) ? x : 0.0; /* std::max(0.0, x) */
+    return (1.0 < lo) ? 1.0 : lo;           /* std::min(1.0, lo) */
+}
+
 static double gl_x[32], gl_w[32];
 static int gl_ready = 0;
 
@@ -593,11 +598,14 @@ double qko_heston_cf_price(double spot, double strike, double t, double r, doubl
         }
     }
 #undef HESTON_CF
+    /* clamp01 (internal_util.h:25-27) is std::min(1, std::max(0, x)), which
+     * maps NaN to 0; p1 is NaN unless |phi(-i)| >= 1e-14 holds, which fails
+     * for a NaN phi(-i) too (kappa = rho sigma: beta + d = 0 at u = -i). */
     double p2 = 0.5 + s2 / M_PI;
     double p1 = 0.5 + s1 / M_PI;
-    p2 = p2 < 0.0 ? 0.0 : (p2 > 1.0 ? 1.0 : p2);
-    p1 = p1 < 0.0 ? 0.0 : (p1 > 1.0 ? 1.0 : p1);
-    if (phi_abs < 1e-14) return qko_nan();
+    p2 = clamp01(p2);
+    p1 = clamp01(p1);
+    if (!(phi_abs >= 1e-14)) return qko_nan();
     const double call = spot * exp(-q * t) * p1 - strike * exp(-r * t) * p2;
     if (ot == QKO_CALL) return call;
     /* put-call parity */

@@ -12,9 +12,11 @@
 #include <cstring>
 #include <limits>
 #include <string>
+#include <vector>
 
 #include <cuda_runtime.h>
 
+#include "cf_kernels.h"
 #include "mc_noalloc.h"
 #include "qk_error.h"
 #include "mc_plan.h"
@@ -491,6 +493,42 @@ double qk_mcm_heston_lr_delta(double spot, double strike, double t, double r, do
     if (qk_mcm_heston_lr_delta_batch(&spot, &strike, &t, &r, &q, &v0, &kappa, &theta, &sigma, &rho,
                                      &option_type, &paths, &steps, &seed, &weight_clip, 1,
                                      &out) != QK_OK)
+        return nan_value();
+    return out;
+}
+
+// ---- Heston characteristic-function pricer -----------------------------------------
+int32_t qk_cf_heston_price_cf_batch(const double* spot, const double* strike, const double* t,
+                                    const double* r, const double* q, const double* v0,
+                                    const double* kappa, const double* theta, const double* sigma,
+                                    const double* rho, const int32_t* option_type,
+                                    const int32_t* integration_steps,
+                                    const double* integration_limit, int32_t n,
+                                    double* out_prices) {
+    const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {r, "r"}, {q, "q"},
+                             {v0, "v0"}, {kappa, "kappa"}, {theta, "theta"}, {sigma, "sigma"},
+                             {rho, "rho"}, {option_type, "option_type"},
+                             {integration_steps, "integration_steps"},
+                             {integration_limit, "integration_limit"}, {out_prices, "out_prices"}};
+    if (int32_t rc = check_nulls(ptrs)) return rc;
+    if (n <= 0) return fail_size(n);
+    std::vector<qkb::CfOption> recs(static_cast<size_t>(n));
+    for (int32_t i = 0; i < n; ++i)
+        recs[i] = qkb::pack_cf_option(spot[i], strike[i], t[i], r[i], q[i], v0[i], kappa[i],
+                                      theta[i], sigma[i], rho[i], option_type[i],
+                                      integration_steps[i], integration_limit[i]);
+    cudaError_t e = qkb::heston_cf_price_host(recs.data(), n, out_prices);
+    return e == cudaSuccess ? QK_OK : fail_cuda(e, "qk_cf_heston_price_cf_batch");
+}
+
+double qk_cf_heston_price_cf(double spot, double strike, double t, double r, double q, double v0,
+                             double kappa, double theta, double sigma, double rho,
+                             int32_t option_type, int32_t integration_steps,
+                             double integration_limit) {
+    double out = nan_value();
+    if (qk_cf_heston_price_cf_batch(&spot, &strike, &t, &r, &q, &v0, &kappa, &theta, &sigma, &rho,
+                                    &option_type, &integration_steps, &integration_limit, 1,
+                                    &out) != QK_OK)
         return nan_value();
     return out;
 }

@@ -70,6 +70,8 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_heston_lr_delta", D, _hes_scalar + [D]),
     ("qk_mcm_heston_lr_delta_batch", I32, [PD] * 10 + [PI32, PI32, PI32, PU64, PD, I32, PD]),
     ("qk_mcm_heston_lr_delta_se_batch", I32, [PD] * 10 + [PI32, PI32, PI32, PU64, PD, I32, PD, PD]),
+    ("qk_cf_heston_price_cf", D, [D] * 10 + [I32, I32, D]),
+    ("qk_cf_heston_price_cf_batch", I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
     ("qk_mcm_mixed_price_batch", I32, _mixed_arrays + [PD, PD]),
     ("qk_mcm_plan_create", I32, _mixed_arrays + [I32, ct.POINTER(VP)]),
     ("qk_mcm_plan_execute", I32, [VP, VP]),

@@ -396,6 +396,33 @@ class QuantKernel:
                                                         sigma, rho, option_type, paths, steps,
                                                         seed, weight_clip), with_se=True)
 
+    # ------------------------------------------------------------------ Heston CF
+    def heston_price_cf(self, spot: float, strike: float, t: float, r: float, q: float,
+                        v0: float, kappa: float, theta: float, sigma: float, rho: float,
+                        option_type: int, integration_steps: int = 1024,
+                        integration_limit: float = 120.0) -> float:
+        """Heston characteristic-function price (heston.cpp:7-53; engine.py:362-372)."""
+        return self._call_checked("qk_cf_heston_price_cf", spot, strike, t, r, q, v0, kappa,
+                                  theta, sigma, rho, option_type, integration_steps,
+                                  integration_limit)
+
+    def heston_price_cf_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                              option_type, integration_steps, integration_limit) -> np.ndarray:
+        """Batch of heston_price_cf on the GPU, one CTA per option (engine.py:422-449)."""
+        s = self._as_f64_array(spot, "spot")
+        arrs = dict(
+            strike=self._as_f64_array(strike, "strike"), t=self._as_f64_array(t, "t"),
+            r=self._as_f64_array(r, "r"), q=self._as_f64_array(q, "q"),
+            v0=self._as_f64_array(v0, "v0"), kappa=self._as_f64_array(kappa, "kappa"),
+            theta=self._as_f64_array(theta, "theta"), sigma=self._as_f64_array(sigma, "sigma"),
+            rho=self._as_f64_array(rho, "rho"),
+            option_type=self._as_i32_array(option_type, "option_type"),
+            integration_steps=self._as_i32_array(integration_steps, "integration_steps"),
+            integration_limit=self._as_f64_array(integration_limit, "integration_limit"),
+        )
+        self._check_same_length(s.shape[0], **arrs)
+        return self._call_batch_ctypes("qk_cf_heston_price_cf_batch", s, *arrs.values())
+
     # ------------------------------------------------------------------ mixed / plans
     def _mixed_arrays(self, model, spot, strike, t, vol, r, q, v0, kappa, theta, sigma, rho,
                       option_type, paths, steps, seed):

@@ -6,6 +6,9 @@ Monte Carlo seed ``seed_base + i``.
 
 * ``bsm_terminal``  -- 64 European calls/puts, terminal GBM, 131072 paths.
 * ``heston``        -- 1024 Heston calls, 200 steps, 262144 paths.
+* ``heston_cf``     -- Heston calls/puts for the characteristic-function
+  pricer: the Heston batch's parameter ranges, 1024 integration steps,
+  integration limit 120 (the reference engine's defaults).
 * ``mixed``         -- 4096 options, BSM-Euler / BSM-Milstein / constant
   local-vol / Heston in 1:1:1:1, paths log-uniform in [2^12, 2^20], steps
   log-uniform in [16, 512].
@@ -49,6 +52,16 @@ def heston(n=1024, paths=262144, steps=200, seed=2, seed_base=5000):
         steps=np.full(n, steps, np.int32),
         seed=(np.arange(n, dtype=np.uint64) + np.uint64(seed_base)),
     )
+
+
+def heston_cf(n=65536, seed=4, integration_steps=1024, integration_limit=120.0):
+    h = heston(n, paths=2, steps=1, seed=seed)
+    out = {k: h[k] for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma",
+                             "rho")}
+    out["option_type"] = (np.arange(n) & 1).astype(np.int32)
+    out["integration_steps"] = np.full(n, integration_steps, np.int32)
+    out["integration_limit"] = np.full(n, integration_limit)
+    return out
 
 
 def mixed(n=4096, seed=3, seed_base=9000, log2_paths=(12.0, 20.0), log2_steps=(4.0, 9.0)):

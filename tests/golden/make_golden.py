@@ -130,11 +130,89 @@ def main() -> None:
         bsm.append({"args": {k: (hx(v) if isinstance(v, float) else v) for k, v in a.items()},
                     "price": hx(ref.bsm(**a))})
 
+    # Heston CF with explicit integration settings and the entry checks of
+    # heston.cpp:10-24 (kept after the lists above so their draws do not move)
+    cf_edges = []
+
+    def add_cf(**kw):
+        a = dict(spot=100.0, strike=100.0, t=1.0, r=0.03, q=0.01, v0=0.04, kappa=2.0,
+                 theta=0.04, sigma=0.3, rho=-0.7, option_type=0, integration_steps=1024,
+                 integration_limit=120.0)
+        a.update(kw)
+        cf_edges.append({"args": {k: (hx(v) if isinstance(v, float) else int(v))
+                                  for k, v in a.items()},
+                         "price": hx(ref.heston_cf(**a))})
+
+    rng_cf = np.random.default_rng(20261204)
+    for steps in (16, 17, 64, 65, 100, 512, 1024, 4096, 8192):
+        for lim in (1e-5, 50.0, 120.0, 500.0):
+            add_cf(integration_steps=steps, integration_limit=lim,
+                   strike=float(rng_cf.uniform(60, 150)), t=float(rng_cf.uniform(0.05, 3)),
+                   v0=float(rng_cf.uniform(0.005, 0.2)), kappa=float(rng_cf.uniform(0.2, 6)),
+                   theta=float(rng_cf.uniform(0.005, 0.2)), sigma=float(rng_cf.uniform(0.05, 1.5)),
+                   rho=float(rng_cf.uniform(-0.95, 0.5)), q=float(rng_cf.uniform(0, 0.04)),
+                   option_type=int(rng_cf.integers(0, 2)))
+    # the reference's own Python cases (test_closed_form_api.py:18-46,
+    # test_heston_fourier.py:18-33)
+    add_cf(r=0.02, sigma=0.5, rho=-0.5)
+    for steps in (64, 512):
+        add_cf(strike=130.0, t=2.0, r=0.05, q=0.01, v0=0.09, kappa=0.8, theta=0.09, sigma=1.0,
+               rho=-0.9, integration_limit=300.0, integration_steps=steps)
+    for ot in (0, 1):
+        add_cf(option_type=ot, integration_steps=8192, integration_limit=500.0)
+    add_cf(integration_steps=15)                 # < 16 -> NaN
+    add_cf(integration_steps=0)
+    add_cf(integration_steps=-5)
+    add_cf(integration_limit=1e-6)               # <= 1e-6 -> NaN
+    add_cf(option_type=2)                        # invalid type -> NaN
+    add_cf(option_type=-1)
+    add_cf(t=1e-14, spot=110.0)                  # intrinsic, undiscounted
+    add_cf(t=1e-14, spot=90.0, option_type=1)
+    add_cf(t=0.0, spot=90.0)
+    add_cf(t=-0.1)                               # NaN
+    add_cf(spot=0.0)
+    add_cf(strike=-1.0)
+    add_cf(v0=-0.01)
+    add_cf(v0=0.0)                               # allowed
+    add_cf(theta=0.0)                            # allowed
+    add_cf(theta=-0.01)
+    add_cf(kappa=0.0)
+    add_cf(sigma=0.0)
+    add_cf(sigma=1e-4)                           # near-BSM limit
+    add_cf(rho=-1.0)
+    add_cf(rho=1.0)
+    add_cf(rho=0.999)
+    add_cf(rho=-0.999)
+    add_cf(r=float("nan"))
+    add_cf(q=float("inf"))
+    add_cf(sigma=float("nan"))
+    add_cf(t=30.0, kappa=0.1, sigma=2.0)         # long maturity, strong vol of vol
+    add_cf(strike=1000.0)                        # deep OTM call -> ~0
+    add_cf(strike=1.0, option_type=1)            # deep OTM put -> ~0
+    add_cf(strike=1.0)                           # deep ITM call
+    add_cf(t=1e-6)                               # just above the intrinsic cut
+    # beta(-i) = kappa - rho sigma <= 0: phi(-i) is NaN (0/0 or x/0 in g), so
+    # P1 is NaN and the price is NaN; = 0 exactly, and < 0
+    add_cf(kappa=0.5, rho=0.5, sigma=1.0)
+    add_cf(kappa=0.1922, rho=0.3328, sigma=1.83, v0=0.2991, theta=0.2253, t=0.0552)
+    # wide ranges: positive rho, large vol of vol, short and long maturities
+    rng_w = np.random.default_rng(20261205)
+    for _ in range(40):
+        add_cf(spot=float(rng_w.uniform(50, 150)), strike=float(rng_w.uniform(40, 200)),
+               t=float(rng_w.uniform(0.02, 5)), r=float(rng_w.uniform(-0.01, 0.08)),
+               q=float(rng_w.uniform(0, 0.05)), v0=float(rng_w.uniform(0, 0.3)),
+               kappa=float(rng_w.uniform(0.05, 8)), theta=float(rng_w.uniform(0, 0.3)),
+               sigma=float(rng_w.uniform(0.02, 2)), rho=float(rng_w.uniform(-0.99, 0.99)),
+               option_type=int(rng_w.integers(0, 2)),
+               integration_steps=int(rng_w.choice([16, 64, 200, 512, 1024, 2048])),
+               integration_limit=float(rng_w.choice([30.0, 120.0, 300.0])))
+
     doc = {
         "source": "yluoc/Quant-Kernel C ABI, compiled from cpp/src by oracle/Makefile (ref)",
         "generator": "tests/golden/make_golden.py",
         "mc_cases": cases,
         "heston_cf": cf,
+        "heston_cf_edges": cf_edges,
         "bsm_cf_reference_as_cdf": bsm,
     }
     OUT.write_text(json.dumps(doc, indent=1))

@@ -91,8 +91,12 @@ BATCHES = {
     "qk_mcm_local_vol_monte_carlo_price_batch": "spot strike t vol r q option_type paths steps seed",
     "qk_mcm_heston_monte_carlo_price_batch":
         "spot strike t r q v0 kappa theta sigma rho option_type paths steps seed",
+    "qk_cf_heston_price_cf_batch":
+        "spot strike t r q v0 kappa theta sigma rho option_type integration_steps "
+        "integration_limit",
 }
-INT_ARGS = {"option_type", "paths", "steps"}
+MC_BATCHES = sorted(k for k in BATCHES if k.startswith("qk_mcm_"))
+INT_ARGS = {"option_type", "paths", "steps", "integration_steps"}
 
 
 def _call(qk, fn, names, null=None, n=1, out=True, se=None):
@@ -137,7 +141,7 @@ def test_bad_size(qk, fn, n):
     assert qk.get_last_error() == f"bad batch size: {n}"
 
 
-@pytest.mark.parametrize("fn", sorted(BATCHES))
+@pytest.mark.parametrize("fn", MC_BATCHES)
 def test_se_batch_checks_out_stderr(qk, fn):
     se_fn = fn.replace("_price_batch", "_price_se_batch")
     qk.clear_last_error()
@@ -198,3 +202,8 @@ def test_no_gpu_means_runtime_error_not_cpu_fallback(qk):
     p = qk._lib.qk_mcm_heston_monte_carlo_price(100, 100, 1, 0.05, 0, 0.04, 2, 0.04, 0.3, -0.7,
                                                 0, 100, 10, 1)
     assert np.isnan(p)
+    qk.clear_last_error()
+    rc = _call(qk, "qk_cf_heston_price_cf_batch", BATCHES["qk_cf_heston_price_cf_batch"])
+    assert rc == -4 and qk.get_last_error().startswith("cuda error")
+    assert np.isnan(qk._lib.qk_cf_heston_price_cf(100, 100, 1, 0.03, 0, 0.04, 2, 0.04, 0.3, -0.7,
+                                                   0, 1024, 120.0))

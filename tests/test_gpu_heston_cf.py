@@ -1,0 +1,131 @@
+"""GPU Heston characteristic-function pricer against the oracle and the
+reference's own outputs.
+
+The reference prices with heston.cpp:7-53 and the Gauss-Legendre panels of
+internal_util.h:80-142; qk_cf_heston_price_cf(_batch) restates both in FP64 on
+the GPU.  Differences come only from the order of the node sums (a fixed CTA
+tree here, a serial loop there) and from the last bits of the FP64 elementary
+functions, so the bar is 1e-9 x max(1, |price|); NaN and intrinsic results of
+the entry checks (heston.cpp:10-24) must agree exactly.
+"""
+
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reference_mc.json").read_text())
+TOL = 1e-9
+KEYS = ["spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho", "option_type",
+        "integration_steps", "integration_limit"]
+
+
+def _args(d):
+    a = {k: (float.fromhex(v) if isinstance(v, str) else v) for k, v in d.items()}
+    a.setdefault("integration_steps", 1024)
+    a.setdefault("integration_limit", 120.0)
+    return a
+
+
+def _close(got, want, tol=TOL):
+    if math.isnan(want):
+        return math.isnan(got)
+    return abs(got - want) <= tol * max(1.0, abs(want))
+
+
+def _batch(qk, cases):
+    cols = {k: np.array([c[k] for c in cases]) for k in KEYS}
+    return qk.heston_price_cf_batch(*(cols[k] for k in KEYS))
+
+
+def test_reference_fixtures(qk):
+    cases = [_args(c["args"]) for c in GOLDEN["heston_cf"] + GOLDEN["heston_cf_edges"]]
+    want = [float.fromhex(c["price"]) for c in GOLDEN["heston_cf"] + GOLDEN["heston_cf_edges"]]
+    got = _batch(qk, cases)
+    bad = [(cases[i], got[i], want[i]) for i in range(len(cases)) if not _close(got[i], want[i])]
+    assert not bad, bad[:5]
+
+
+def test_scalar_equals_batch_bitwise(qk):
+    cases = [_args(c["args"]) for c in GOLDEN["heston_cf_edges"]]
+    batch = _batch(qk, cases)
+    qk_lib = qk._lib
+    for a, b in zip(cases, batch):
+        s = qk_lib.qk_cf_heston_price_cf(*(a[k] for k in KEYS))
+        assert (math.isnan(s) and math.isnan(b)) or s == b, (a, s, b)
+
+
+def test_engine_scalar_defaults_match_reference_engine(qk, oracle):
+    # engine.py:362-372: integration_steps=1024, integration_limit=120.0
+    a = dict(spot=100.0, strike=100.0, t=1.0, r=0.02, q=0.01, v0=0.04, kappa=2.0, theta=0.04,
+             sigma=0.5, rho=-0.5, option_type=0)
+    got = qk.heston_price_cf(**a)
+    assert got > 0.0 and _close(got, oracle.heston_cf(**a))
+    with pytest.raises(ValueError):
+        qk.heston_price_cf(**{**a, "option_type": 3})
+
+
+def test_random_batch_against_oracle(qk, oracle):
+    rng = np.random.default_rng(77)
+    n = 2048
+    cols = dict(
+        spot=rng.uniform(50, 150, n), strike=rng.uniform(40, 200, n), t=rng.uniform(0.02, 5, n),
+        r=rng.uniform(-0.01, 0.08, n), q=rng.uniform(0, 0.05, n), v0=rng.uniform(0.0, 0.3, n),
+        kappa=rng.uniform(0.05, 8, n), theta=rng.uniform(0.0, 0.3, n),
+        sigma=rng.uniform(0.02, 2.0, n), rho=rng.uniform(-0.99, 0.99, n),
+        option_type=rng.integers(0, 2, n).astype(np.int32),
+        integration_steps=rng.choice([16, 64, 200, 512, 1024, 2048], n).astype(np.int32),
+        integration_limit=rng.choice([30.0, 120.0, 300.0], n))
+    got = qk.heston_price_cf_batch(*(cols[k] for k in KEYS))
+    bad = []
+    for i in range(n):
+        want = oracle.heston_cf(*(cols[k][i].item() for k in KEYS))
+        if not _close(got[i], want):
+            bad.append((i, got[i], want))
+    assert not bad, bad[:5]
+
+
+def test_put_call_parity_and_bounds(qk):
+    rng = np.random.default_rng(5)
+    n = 512
+    base = dict(spot=rng.uniform(80, 120, n), strike=rng.uniform(80, 120, n),
+                t=rng.uniform(0.1, 2, n), r=rng.uniform(0, 0.05, n), q=rng.uniform(0, 0.03, n),
+                v0=rng.uniform(0.01, 0.09, n), kappa=rng.uniform(0.5, 5, n),
+                theta=rng.uniform(0.01, 0.09, n), sigma=rng.uniform(0.1, 0.8, n),
+                rho=rng.uniform(-0.9, 0.0, n), integration_steps=np.full(n, 1024, np.int32),
+                integration_limit=np.full(n, 120.0))
+    args = lambda ot: [base[k] if k != "option_type" else np.full(n, ot, np.int32) for k in KEYS]
+    c = qk.heston_price_cf_batch(*args(0))
+    p = qk.heston_price_cf_batch(*args(1))
+    fwd = base["spot"] * np.exp(-base["q"] * base["t"]) - base["strike"] * np.exp(-base["r"] * base["t"])
+    np.testing.assert_allclose(c - p, fwd, atol=1e-9)
+    assert np.all(c >= np.maximum(fwd, 0) - 1e-6) and np.all(c <= base["spot"] + 1e-9)
+
+
+def test_agrees_with_gpu_monte_carlo(qk):
+    """The Heston MC path (antithetic, full truncation) converges to the CF price."""
+    a = dict(spot=100.0, strike=105.0, t=1.0, r=0.03, q=0.01, v0=0.04, kappa=2.0, theta=0.04,
+             sigma=0.3, rho=-0.7)
+    cf = qk.heston_price_cf(**a, option_type=0)
+    price, se = qk.heston_monte_carlo_price_se_batch(
+        [a["spot"]], [a["strike"]], [a["t"]], [a["r"]], [a["q"]], [a["v0"]], [a["kappa"]],
+        [a["theta"]], [a["sigma"]], [a["rho"]], [0], [4_000_000], [400], [11])
+    assert abs(price[0] - cf) < 3.0 * se[0] + 2e-3, (price[0], se[0], cf)
+
+
+def test_large_batch_deterministic(qk):
+    rng = np.random.default_rng(9)
+    n = 100_000
+    cols = dict(spot=np.full(n, 100.0), strike=rng.uniform(70, 130, n), t=rng.uniform(0.1, 2, n),
+                r=np.full(n, 0.03), q=np.zeros(n), v0=rng.uniform(0.01, 0.09, n),
+                kappa=rng.uniform(0.5, 5, n), theta=rng.uniform(0.01, 0.09, n),
+                sigma=rng.uniform(0.1, 1.0, n), rho=rng.uniform(-0.9, 0.0, n),
+                option_type=rng.integers(0, 2, n).astype(np.int32),
+                integration_steps=np.full(n, 1024, np.int32), integration_limit=np.full(n, 120.0))
+    a = qk.heston_price_cf_batch(*(cols[k] for k in KEYS))
+    b = qk.heston_price_cf_batch(*(cols[k] for k in KEYS))
+    assert np.array_equal(a, b) and np.all(np.isfinite(a))

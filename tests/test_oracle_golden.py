@@ -70,6 +70,20 @@ def test_heston_cf_matches_reference(oracle, i):
     assert abs(got - want) < 1e-8, (a, got, want)
 
 
+@pytest.mark.parametrize("i", range(len(GOLDEN["heston_cf_edges"])))
+def test_heston_cf_edges_match_reference(oracle, i):
+    """Integration settings 16..8192 steps, limits 1e-5..500, the entry checks
+    of heston.cpp:10-24 (NaN, intrinsic) and extreme parameters."""
+    case = GOLDEN["heston_cf_edges"][i]
+    a = _args(case["args"])
+    want = float.fromhex(case["price"])
+    got = oracle.heston_cf(**a)
+    if math.isnan(want):
+        assert math.isnan(got), (a, got)
+    else:
+        assert abs(got - want) < 1e-8 * max(1.0, abs(want)), (a, got, want)
+
+
 def test_heston_cf_converged_and_small_volvol_limit(oracle):
     base = dict(spot=100.0, strike=105.0, t=1.0, r=0.03, q=0.01, v0=0.04, kappa=1.5,
                 theta=0.04, sigma=1e-4, rho=-0.5, option_type=0)
