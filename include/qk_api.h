@@ -119,6 +119,57 @@ QK_EXPORT int32_t qk_mcm_local_vol_monte_carlo_price_batch(
     const double* q, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
     const uint64_t* seed, int32_t n, double* out_prices);
 
+/* Terminal GBM with the reference's variance-reduction estimators. */
+/* qk_api.h:291-293 (control_variates.cpp:10-52: control x = disc * S_T with
+ * known mean spot e^{-qt}, beta from the same sample; paths >= 3) */
+QK_EXPORT double qk_mcm_control_variates_price(double spot, double strike, double t, double vol,
+                                               double r, double q, int32_t option_type,
+                                               int32_t paths, uint64_t seed);
+/* qk_api.h:341-346 */
+QK_EXPORT int32_t qk_mcm_control_variates_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices);
+/* qk_api.h:288-290 (importance_sampling.cpp:11-36: normal shifted by `shift`,
+ * likelihood-ratio weight exp(-shift y + shift^2/2)) */
+QK_EXPORT double qk_mcm_importance_sampling_price(double spot, double strike, double t, double vol,
+                                                  double r, double q, int32_t option_type,
+                                                  int32_t paths, double shift, uint64_t seed);
+/* qk_api.h:335-340 */
+QK_EXPORT int32_t qk_mcm_importance_sampling_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const double* shift,
+    const uint64_t* seed, int32_t n, double* out_prices);
+/* qk_api.h:297-299 (stratified_sampling.cpp:11-35: one draw per stratum
+ * [i/n, (i+1)/n), Acklam inverse normal) */
+QK_EXPORT double qk_mcm_stratified_sampling_price(double spot, double strike, double t, double vol,
+                                                  double r, double q, int32_t option_type,
+                                                  int32_t paths, uint64_t seed);
+/* qk_api.h:353-358 */
+QK_EXPORT int32_t qk_mcm_stratified_sampling_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices);
+/* qk_api.h:278-280 (quasi_monte_carlo.cpp:10-32: one-dimensional Sobol points
+ * 1..paths, Acklam inverse normal; deterministic, no seed) */
+QK_EXPORT double qk_mcm_quasi_monte_carlo_sobol_price(double spot, double strike, double t,
+                                                      double vol, double r, double q,
+                                                      int32_t option_type, int32_t paths);
+/* qk_api.h:318-322 */
+QK_EXPORT int32_t qk_mcm_quasi_monte_carlo_sobol_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, int32_t n,
+    double* out_prices);
+/* qk_api.h:281-283 (quasi_monte_carlo.cpp:34-56: Halton base 2) */
+QK_EXPORT double qk_mcm_quasi_monte_carlo_halton_price(double spot, double strike, double t,
+                                                       double vol, double r, double q,
+                                                       int32_t option_type, int32_t paths);
+/* qk_api.h:323-327 */
+QK_EXPORT int32_t qk_mcm_quasi_monte_carlo_halton_price_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, int32_t n,
+    double* out_prices);
+
 /* qk_api.h:53-55 (heston.cpp:7-53: little-trap characteristic function,
  * P1/P2 by ceil(integration_steps/64) panels of 64-point Gauss-Legendre on
  * [1e-8, integration_limit]; FP64 on the GPU, one CTA per option) */
@@ -153,6 +204,11 @@ QK_EXPORT int32_t qk_get_device(int32_t* device);
 #define QK_MC_TERMINAL_PLAIN 5 /* terminal GBM, independent paths */
 #define QK_MC_HESTON         6 /* Heston full-truncation Euler */
 #define QK_MC_HESTON_LR_DELTA 7 /* Heston likelihood-ratio delta; `vol` holds weight_clip */
+#define QK_MC_CONTROL_VARIATES 8 /* terminal GBM, control variate S_T */
+#define QK_MC_IMPORTANCE_SAMPLING 9 /* terminal GBM, shifted normal; `v0` holds the shift */
+#define QK_MC_STRATIFIED     10 /* terminal GBM, one draw per stratum */
+#define QK_MC_QMC_SOBOL      11 /* terminal GBM, Sobol points (seed ignored) */
+#define QK_MC_QMC_HALTON     12 /* terminal GBM, Halton base-2 points (seed ignored) */
 
 /* Plan flags. */
 #define QK_PLAN_PERSISTENT    0x1 /* one persistent work-stealing launch over all tiles */
@@ -189,6 +245,32 @@ QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_se_batch(
     const double* v0, const double* kappa, const double* theta, const double* sigma,
     const double* rho, const int32_t* option_type, const int32_t* paths, const int32_t* steps,
     const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+/* Variance-reduction estimators.  Standard errors: control variates -- the
+ * residual variance of payoff - beta * control over n - 2; stratified -- the
+ * squared differences of neighbouring strata pairs (conservative); importance
+ * sampling -- the weighted payoffs' sample variance; quasi-Monte Carlo -- the
+ * i.i.d. formula applied to the points (an indicator, not a confidence bound:
+ * the points are not random). */
+QK_EXPORT int32_t qk_mcm_control_variates_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_importance_sampling_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const double* shift,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_stratified_sampling_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, const uint64_t* seed,
+    int32_t n, double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_quasi_monte_carlo_sobol_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, int32_t n,
+    double* out_prices, double* out_stderr);
+QK_EXPORT int32_t qk_mcm_quasi_monte_carlo_halton_price_se_batch(
+    const double* spot, const double* strike, const double* t, const double* vol, const double* r,
+    const double* q, const int32_t* option_type, const int32_t* paths, int32_t n,
+    double* out_prices, double* out_stderr);
 
 /* Heston batch that allocates no memory.  No counterpart in the reference.
  * For callers that cannot call cudaMalloc: services whose host framework owns
@@ -197,7 +279,7 @@ QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_se_batch(
  * paths that cannot afford an allocation or the synchronisation of a free.
  * Same inputs and outputs as qk_mcm_heston_monte_carlo_price_se_batch (host
  * arrays; out_stderr may be NULL) and the same kernels and results; every
- * device buffer lives in one fixed 12.6 MiB array per GPU, held until the
+ * device buffer lives in one fixed 16.6 MiB array per GPU, held until the
  * process exits.  Limits: n <= 4096 options and at most 262,144 tiles in
  * total (a tile is 512 antithetic path pairs of one option, e.g. 1024 options
  * of 262,144 paths); larger batches return QK_ERR_BAD_SIZE before any GPU
@@ -220,7 +302,9 @@ QK_EXPORT int32_t qk_mcm_heston_lr_delta_se_batch(
 
 /* Mixed-model batch: option i is priced with model[i] (QK_MC_*).  Fields a
  * model does not use are ignored and may hold anything (vol for Heston;
- * v0..rho for the BSM models; steps for the terminal models).  Runs as one
+ * v0..rho for the BSM models; steps for the terminal models; seed for the
+ * quasi-Monte Carlo models).  QK_MC_IMPORTANCE_SAMPLING reads its shift from
+ * v0.  Runs as one
  * persistent work-stealing launch.  out_stderr may be NULL. */
 QK_EXPORT int32_t qk_mcm_mixed_price_batch(
     const int32_t* model, const double* spot, const double* strike, const double* t,

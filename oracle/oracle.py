@@ -27,6 +27,8 @@ PU32 = ct.POINTER(U32)
 
 # Model codes shared with the GPU library (QK_MC_* in include/qk_api.h).
 STANDARD, ANTITHETIC, EULER, MILSTEIN, LOCAL_VOL, TERMINAL_PLAIN, HESTON, HESTON_LR_DELTA = range(8)
+CONTROL_VARIATES, IMPORTANCE_SAMPLING, STRATIFIED, QMC_SOBOL, QMC_HALTON = range(8, 13)
+VR_MODELS = (CONTROL_VARIATES, IMPORTANCE_SAMPLING, STRATIFIED, QMC_SOBOL, QMC_HALTON)
 
 
 def _pd(a):
@@ -56,6 +58,12 @@ class Oracle:
             "qko_philox4x32_10": (None, [PU32, PU32, PU32]),
             "qko_philox_normals4": (None, [U64, U32, U32, U32, PD]),
             "qko_philox_price": (D, [I32] + [D] * 11 + [I32, I32, I32, U64, I32, PD]),
+            "qko_control_variates": (D, term),
+            "qko_stratified": (D, term),
+            "qko_importance_sampling": (D, [D] * 6 + [I32, I32, D, U64, PD]),
+            "qko_qmc_sobol": (D, [D] * 6 + [I32, I32, PD]),
+            "qko_qmc_halton": (D, [D] * 6 + [I32, I32, PD]),
+            "qko_philox_vr_price": (D, [I32] + [D] * 7 + [I32, I32, U64, PD]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -64,11 +72,22 @@ class Oracle:
         self.lib = lib
 
     # -- reference pricers (bit-exact) -------------------------------------------
-    def price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps, seed,
-              v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0):
+    def price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps=1, seed=0,
+              v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0, shift=0.0):
         se = D()
         L = self.lib
-        if model == STANDARD:
+        if model == CONTROL_VARIATES:
+            p = L.qko_control_variates(spot, strike, t, vol, r, q, option_type, paths, seed, ct.byref(se))
+        elif model == IMPORTANCE_SAMPLING:
+            p = L.qko_importance_sampling(spot, strike, t, vol, r, q, option_type, paths, shift,
+                                          seed, ct.byref(se))
+        elif model == STRATIFIED:
+            p = L.qko_stratified(spot, strike, t, vol, r, q, option_type, paths, seed, ct.byref(se))
+        elif model == QMC_SOBOL:
+            p = L.qko_qmc_sobol(spot, strike, t, vol, r, q, option_type, paths, ct.byref(se))
+        elif model == QMC_HALTON:
+            p = L.qko_qmc_halton(spot, strike, t, vol, r, q, option_type, paths, ct.byref(se))
+        elif model == STANDARD:
             p = L.qko_standard_mc(spot, strike, t, vol, r, q, option_type, paths, seed, ct.byref(se))
         elif model == ANTITHETIC:
             p = L.qko_antithetic(spot, strike, t, vol, r, q, option_type, paths, seed, ct.byref(se))
@@ -145,6 +164,14 @@ class Oracle:
         self.lib.qko_philox_normals4(seed, c0, c1, c3, _pd(z))
         return z
 
+    def philox_vr_price(self, model, spot, strike, t, vol, r, q, option_type, paths, seed=0,
+                        shift=0.0):
+        """Models 8-12 on the GPU's stream and estimators, FP64."""
+        se = D()
+        p = self.lib.qko_philox_vr_price(model, spot, strike, t, vol, r, q, shift, option_type,
+                                         paths, seed, ct.byref(se))
+        return p, se.value
+
     def philox_price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps, seed,
                      v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0, antithetic=True):
         se = D()
@@ -177,6 +204,16 @@ class Reference:
             "qk_cf_black_scholes_merton_price": (D, [D] * 6 + [I32]),
             "qk_cf_heston_price_cf": (D, [D] * 10 + [I32, I32, D]),
             "qk_cf_heston_price_cf_batch": (I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
+            "qk_mcm_control_variates_price": (D, term),
+            "qk_mcm_stratified_sampling_price": (D, term),
+            "qk_mcm_importance_sampling_price": (D, [D] * 6 + [I32, I32, D, U64]),
+            "qk_mcm_quasi_monte_carlo_sobol_price": (D, [D] * 6 + [I32, I32]),
+            "qk_mcm_quasi_monte_carlo_halton_price": (D, [D] * 6 + [I32, I32]),
+            "qk_mcm_control_variates_price_batch": (I32, [PD] * 6 + [PI32, PI32, PU64, I32, PD]),
+            "qk_mcm_stratified_sampling_price_batch": (I32, [PD] * 6 + [PI32, PI32, PU64, I32, PD]),
+            "qk_mcm_importance_sampling_price_batch": (I32, [PD] * 6 + [PI32, PI32, PD, PU64, I32, PD]),
+            "qk_mcm_quasi_monte_carlo_sobol_price_batch": (I32, [PD] * 6 + [PI32, PI32, I32, PD]),
+            "qk_mcm_quasi_monte_carlo_halton_price_batch": (I32, [PD] * 6 + [PI32, PI32, I32, PD]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -184,9 +221,20 @@ class Reference:
             fn.argtypes = args
         self.lib = lib
 
-    def price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps, seed,
-              v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0):
+    def price(self, model, spot, strike, t, vol, r, q, option_type, paths, steps=1, seed=0,
+              v0=0.0, kappa=0.0, theta=0.0, sigma=0.0, rho=0.0, shift=0.0):
         L = self.lib
+        if model == CONTROL_VARIATES:
+            return L.qk_mcm_control_variates_price(spot, strike, t, vol, r, q, option_type, paths, seed)
+        if model == IMPORTANCE_SAMPLING:
+            return L.qk_mcm_importance_sampling_price(spot, strike, t, vol, r, q, option_type, paths,
+                                                      shift, seed)
+        if model == STRATIFIED:
+            return L.qk_mcm_stratified_sampling_price(spot, strike, t, vol, r, q, option_type, paths, seed)
+        if model == QMC_SOBOL:
+            return L.qk_mcm_quasi_monte_carlo_sobol_price(spot, strike, t, vol, r, q, option_type, paths)
+        if model == QMC_HALTON:
+            return L.qk_mcm_quasi_monte_carlo_halton_price(spot, strike, t, vol, r, q, option_type, paths)
         if model == STANDARD:
             return L.qk_mcm_standard_monte_carlo_price(spot, strike, t, vol, r, q, option_type, paths, seed)
         if model == ANTITHETIC:
@@ -217,6 +265,31 @@ class Reference:
         rc = self.lib.qk_mcm_heston_monte_carlo_price_batch(
             *[_pd(x) for x in a], ot.ctypes.data_as(PI32), pp.ctypes.data_as(PI32),
             st.ctypes.data_as(PI32), sd.ctypes.data_as(PU64), n, _pd(out))
+        if rc != 0:
+            raise RuntimeError(f"reference batch rc={rc}")
+        return out
+
+    def vr_batch(self, model, spot, strike, t, vol, r, q, option_type, paths, seed=None,
+                 shift=None):
+        """The reference's OpenMP batch of a variance-reduction method."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (spot, strike, t, vol, r, q)]
+        ot = np.ascontiguousarray(option_type, np.int32)
+        pp = np.ascontiguousarray(paths, np.int32)
+        n = a[0].shape[0]
+        out = np.empty(n)
+        args = [_pd(x) for x in a] + [ot.ctypes.data_as(PI32), pp.ctypes.data_as(PI32)]
+        name = {CONTROL_VARIATES: "qk_mcm_control_variates_price_batch",
+                STRATIFIED: "qk_mcm_stratified_sampling_price_batch",
+                IMPORTANCE_SAMPLING: "qk_mcm_importance_sampling_price_batch",
+                QMC_SOBOL: "qk_mcm_quasi_monte_carlo_sobol_price_batch",
+                QMC_HALTON: "qk_mcm_quasi_monte_carlo_halton_price_batch"}[model]
+        if model == IMPORTANCE_SAMPLING:
+            sh = np.ascontiguousarray(shift, np.float64)
+            args.append(_pd(sh))
+        if model not in (QMC_SOBOL, QMC_HALTON):
+            sd = np.ascontiguousarray(seed, np.uint64)
+            args.append(sd.ctypes.data_as(PU64))
+        rc = getattr(self.lib, name)(*args, n, _pd(out))
         if rc != 0:
             raise RuntimeError(f"reference batch rc={rc}")
         return out

@@ -440,6 +440,203 @@ double qko_heston_lr_delta(double spot, double strike, double t, double r, doubl
     return disc * sum / (double)paths;
 }
 
+/* ===================================================================== *
+ * 1b. Terminal GBM with the reference's variance-reduction estimators.
+ * ===================================================================== */
+
+/* Acklam's inverse normal CDF as the reference evaluates it
+ * (monte_carlo_methods/common/internal_util.h:42-90; P. J. Acklam, "An
+ * algorithm for computing the inverse normal cumulative distribution
+ * function", 2003): same coefficients, same Horner order. */
+static double acklam_inv(double p) {
+    static const double a1 = -3.969683028665376e+01, a2 = 2.209460984245205e+02,
+                        a3 = -2.759285104469687e+02, a4 = 1.383577518672690e+02,
+                        a5 = -3.066479806614716e+01, a6 = 2.506628277459239e+00;
+    static const double b1 = -5.447609879822406e+01, b2 = 1.615858368580409e+02,
+                        b3 = -1.556989798598866e+02, b4 = 6.680131188771972e+01,
+                        b5 = -1.328068155288572e+01;
+    static const double c1 = -7.784894002430293e-03, c2 = -3.223964580411365e-01,
+                        c3 = -2.400758277161838e+00, c4 = -2.549732539343734e+00,
+                        c5 = 4.374664141464968e+00, c6 = 2.938163982698783e+00;
+    static const double d1 = 7.784695709041462e-03, d2 = 3.224671290700398e-01,
+                        d3 = 2.445134137142996e+00, d4 = 3.754408661907416e+00;
+    const double p_low = 0.02425, p_high = 1.0 - p_low;
+    if (p <= 0.0 || p >= 1.0) return qko_nan();
+    if (p < p_low) {
+        const double t = sqrt(-2.0 * log(p));
+        return (((((c1 * t + c2) * t + c3) * t + c4) * t + c5) * t + c6) /
+               ((((d1 * t + d2) * t + d3) * t + d4) * t + 1.0);
+    }
+    if (p > p_high) {
+        const double t = sqrt(-2.0 * log(1.0 - p));
+        return -(((((c1 * t + c2) * t + c3) * t + c4) * t + c5) * t + c6) /
+               ((((d1 * t + d2) * t + d3) * t + d4) * t + 1.0);
+    }
+    const double t = p - 0.5;
+    const double r = t * t;
+    return (((((a1 * r + a2) * r + a3) * r + a4) * r + a5) * r + a6) * t /
+           (((((b1 * r + b2) * r + b3) * r + b4) * r + b5) * r + 1.0);
+}
+
+/* std::clamp(u, 1e-12, 1 - 1e-12) */
+static double clamp_unit(double u) {
+    return (u < 1e-12) ? 1e-12 : (((1.0 - 1e-12) < u) ? 1.0 - 1e-12 : u);
+}
+
+/* internal_util.h:104-119: bit j of gray(i) contributes 1 << (31 - j). */
+static double sobol_point(uint32_t i) {
+    if (i == 0u) return 0.0;
+    uint32_t gray = i ^ (i >> 1), x = 0u;
+    for (uint32_t bit = 0; gray != 0u; ++bit, gray >>= 1)
+        if (gray & 1u) x ^= (1u << (31u - bit));
+    return ((double)x + 0.5) / 4294967296.0;
+}
+
+/* internal_util.h:121-130: radical inverse in `base`. */
+static double halton_point(uint32_t i, uint32_t base) {
+    double f = 1.0, r = 0.0;
+    while (i > 0u) {
+        f /= (double)base;
+        r += f * (double)(i % base);
+        i /= base;
+    }
+    return r;
+}
+
+/* Standard errors shared with the GPU (none of these exist in the reference):
+ * control variates -- residual variance of payoff - beta * control over
+ * n - 2, from sums of the payoff p and the centred control c = S_T - E[S_T];
+ * the degenerate-control branch falls back to the plain sample variance. */
+static double cv_se(double disc, double sp, double spp, double sc, double scc, double scp,
+                    double n) {
+    const double mp = sp / n, mc = sc / n;
+    const double vc = scc / n - mc * mc, vp = spp / n - mp * mp;
+    if (disc * disc * vc <= QKO_EPS) return n >= 2.0 ? disc * sqrt(smax(vp, 0.0) / (n - 1.0)) : qko_nan();
+    const double cov = scp / n - mc * mp;
+    return disc * sqrt(smax(vp - cov * (cov / vc), 0.0) / (n - 2.0));
+}
+
+/* control_variates.cpp:10-52. */
+double qko_control_variates(double spot, double strike, double t, double vol, double r, double q,
+                            int32_t ot, int32_t paths, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 2) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    const double disc = exp(-r * t);
+    const double expected_x = spot * exp(-q * t);
+    const double mean_st = spot * exp((r - q) * t);
+    double sum_y = 0.0, sum_x = 0.0, sum_xx = 0.0, sum_xy = 0.0;
+    double sp = 0.0, spp = 0.0, sc = 0.0, scc = 0.0, scp = 0.0;
+    for (int32_t i = 0; i < paths; ++i) {
+        const double z = qko_gen_normal(&g);
+        const double st = bsm_terminal(vol, r, q, spot, t, z);
+        const double x = disc * st;
+        const double pay = intrinsic(st, strike, ot);
+        const double y = disc * pay;
+        sum_y += y;
+        sum_x += x;
+        sum_xx += x * x;
+        sum_xy += x * y;
+        const double c = st - mean_st;
+        sp += pay;
+        spp += pay * pay;
+        sc += c;
+        scc += c * c;
+        scp += c * pay;
+    }
+    if (se) *se = cv_se(disc, sp, spp, sc, scc, scp, (double)paths);
+    const double mean_y = sum_y / (double)paths;
+    const double mean_x = sum_x / (double)paths;
+    const double var_x = (sum_xx / (double)paths) - mean_x * mean_x;
+    if (var_x <= QKO_EPS) return mean_y;
+    const double cov_xy = (sum_xy / (double)paths) - mean_x * mean_y;
+    const double beta = cov_xy / var_x;
+    return mean_y - beta * (mean_x - expected_x);
+}
+
+/* importance_sampling.cpp:11-36 driving mc_engine.h:62-75 estimate_terminal. */
+double qko_importance_sampling(double spot, double strike, double t, double vol, double r,
+                               double q, int32_t ot, int32_t paths, double shift, uint64_t seed,
+                               double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 1 || !qko_finite(shift))
+        return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    double sum = 0.0, sq = 0.0;
+    for (int32_t i = 0; i < paths; ++i) {
+        const double z = qko_gen_normal(&g);
+        const double st = bsm_terminal(vol, r, q, spot, t, z + shift);
+        const double y = z + shift;
+        const double weight = exp(-shift * y + 0.5 * shift * shift);
+        const double a = intrinsic(st, strike, ot) * weight;
+        sum += a;
+        sq += a * a;
+    }
+    if (se) *se = se_from_moments(disc, sum, sq, (double)paths);
+    return disc * (sum / (double)paths);
+}
+
+/* stratified_sampling.cpp:11-35; uniform_real_distribution(0, 1) is one
+ * generate_canonical draw, u * (1 - 0) + 0. */
+double qko_stratified(double spot, double strike, double t, double vol, double r, double q,
+                      int32_t ot, int32_t paths, uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 1) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    qko_normal_gen g;
+    qko_gen_init(&g, seed);
+    const double disc = exp(-r * t);
+    double sum = 0.0, dsq = 0.0, prev = 0.0;
+    for (int32_t i = 0; i < paths; ++i) {
+        double u = ((double)i + (qko_gen_canonical(&g) * (1.0 - 0.0) + 0.0)) / (double)paths;
+        u = clamp_unit(u);
+        const double z = acklam_inv(u);
+        const double st = bsm_terminal(vol, r, q, spot, t, z);
+        const double a = intrinsic(st, strike, ot);
+        sum += a;
+        if (i & 1) dsq += (prev - a) * (prev - a);
+        prev = a;
+    }
+    if (se) *se = disc * sqrt(dsq) / (double)paths;
+    return disc * (sum / (double)paths);
+}
+
+/* quasi_monte_carlo.cpp:10-56 (kind 0: Sobol, 1: Halton base 2). */
+static double qmc_price(int kind, double spot, double strike, double t, double vol, double r,
+                        double q, int32_t ot, int32_t paths, double* se) {
+    if (se) *se = qko_nan();
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths <= 1) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    double sum = 0.0, sq = 0.0;
+    for (int32_t i = 1; i <= paths; ++i) {
+        double u = kind == 0 ? sobol_point((uint32_t)i) : halton_point((uint32_t)i, 2u);
+        u = clamp_unit(u);
+        const double z = acklam_inv(u);
+        const double st = bsm_terminal(vol, r, q, spot, t, z);
+        const double a = intrinsic(st, strike, ot);
+        sum += a;
+        sq += a * a;
+    }
+    if (se) *se = se_from_moments(disc, sum, sq, (double)paths);
+    return disc * (sum / (double)paths);
+}
+
+double qko_qmc_sobol(double spot, double strike, double t, double vol, double r, double q,
+                     int32_t ot, int32_t paths, double* se) {
+    return qmc_price(0, spot, strike, t, vol, r, q, ot, paths, se);
+}
+
+double qko_qmc_halton(double spot, double strike, double t, double vol, double r, double q,
+                      int32_t ot, int32_t paths, double* se) {
+    return qmc_price(1, spot, strike, t, vol, r, q, ot, paths, se);
+}
+
 void qko_heston_batch(const double* spot, const double* strike, const double* t,
                       const double* r, const double* q, const double* v0, const double* kappa,
                       const double* theta, const double* sigma, const double* rho,
@@ -469,6 +666,10 @@ void qko_bsm_family_batch(int32_t model, const double* spot, const double* strik
             case 3: p = qko_milstein(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], st, seed[i], &se); break;
             case 4: p = qko_local_vol(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], st, seed[i], &se); break;
             case 5: p = qko_terminal_plain(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], seed[i], &se); break;
+            case 8: p = qko_control_variates(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], seed[i], &se); break;
+            case 10: p = qko_stratified(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], seed[i], &se); break;
+            case 11: p = qko_qmc_sobol(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], &se); break;
+            case 12: p = qko_qmc_halton(spot[i], strike[i], t[i], vol[i], r[i], q[i], ot[i], paths[i], &se); break;
             default: p = qko_nan(); break;
         }
         out[i] = p;
@@ -808,4 +1009,76 @@ double qko_philox_price(int32_t model, double spot, double strike, double t, dou
     }
     if (se) *se = se_from_moments(disc, ysum, ysq, ny);
     return disc * (sum / (double)paths);
+}
+
+/* Philox replay of the variance-reduction models (8-12), FP64, the GPU's
+ * stream and estimators:
+ *   8 control variates, 9 importance sampling: path i uses normal slot i % 4
+ *     of counter (i / 4, 0, 0, 1);
+ *   10 stratified: U_i = (x + 0.5) 2^-32 from word i % 4 of counter
+ *     (i / 4, 0, 0, 2);  11 / 12: the reference's points (no randomness). */
+double qko_philox_vr_price(int32_t model, double spot, double strike, double t, double vol,
+                           double r, double q, double shift, int32_t ot, int32_t paths,
+                           uint64_t seed, double* se) {
+    if (se) *se = qko_nan();
+    const int32_t min_paths = model == 8 ? 3 : 2;
+    if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths < min_paths ||
+        !qko_finite(shift))
+        return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    const double disc = exp(-r * t);
+    const double d0 = (r - q - 0.5 * vol * vol) * t;
+    const double d1 = vol * sqrt(smax(t, 0.0));
+    const double mean_st = spot * exp((r - q) * t);
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    double sp = 0.0, spp = 0.0, sc = 0.0, scc = 0.0, scp = 0.0, dsq = 0.0, prev = 0.0;
+    for (int32_t i = 0; i < paths; ++i) {
+        double z;
+        if (model == 11 || model == 12) {
+            const double u = model == 11 ? sobol_point((uint32_t)i + 1u)
+                                         : halton_point((uint32_t)i + 1u, 2u);
+            z = acklam_inv(clamp_unit(u));
+        } else if (model == 10) {
+            const uint32_t ctr[4] = {(uint32_t)i / 4u, 0u, 0u, 2u};
+            uint32_t x[4];
+            qko_philox4x32_10(ctr, key, x);
+            const double ui = ((double)x[i % 4] + 0.5) * 0x1p-32;
+            z = acklam_inv(clamp_unit(((double)i + ui) / (double)paths));
+        } else {
+            double z4[4];
+            qko_philox_normals4(seed, (uint32_t)i / 4u, 0u, 1u, z4);
+            z = z4[i % 4];
+        }
+        double w = 1.0;
+        if (model == 9) {
+            z = z + shift;
+            w = exp(-shift * z + 0.5 * shift * shift);
+        }
+        const double st = spot * exp(d0 + d1 * z);
+        const double a = intrinsic(st, strike, ot) * w;
+        sp += a;
+        spp += a * a;
+        if (model == 8) {
+            const double c = st - mean_st;
+            sc += c;
+            scc += c * c;
+            scp += c * a;
+        }
+        if (model == 10 && (i & 1)) dsq += (prev - a) * (prev - a);
+        prev = a;
+    }
+    const double n = (double)paths;
+    if (model == 8) {
+        const double mp = sp / n, mc = sc / n, vc = scc / n - mc * mc;
+        if (se) *se = cv_se(disc, sp, spp, sc, scc, scp, n);
+        if (disc * disc * vc <= QKO_EPS) return disc * mp;
+        const double beta = (scp / n - mc * mp) / vc;
+        return disc * (mp - beta * mc);
+    }
+    if (model == 10) {
+        if (se) *se = disc * sqrt(dsq) / n;
+    } else if (se) {
+        *se = se_from_moments(disc, sp, spp, n);
+    }
+    return disc * (sp / n);
 }

@@ -72,6 +72,21 @@ double qko_heston_lr_delta(double spot, double strike, double t, double r, doubl
                            int32_t option_type, int32_t paths, int32_t steps, uint64_t seed,
                            double weight_clip, double* se);
 
+/* Terminal GBM with the variance-reduction estimators (control_variates.cpp,
+ * importance_sampling.cpp, stratified_sampling.cpp, quasi_monte_carlo.cpp).
+ * Standard errors as the GPU defines them (see qk_oracle.c). */
+double qko_control_variates(double spot, double strike, double t, double vol, double r, double q,
+                            int32_t option_type, int32_t paths, uint64_t seed, double* se);
+double qko_importance_sampling(double spot, double strike, double t, double vol, double r,
+                               double q, int32_t option_type, int32_t paths, double shift,
+                               uint64_t seed, double* se);
+double qko_stratified(double spot, double strike, double t, double vol, double r, double q,
+                      int32_t option_type, int32_t paths, uint64_t seed, double* se);
+double qko_qmc_sobol(double spot, double strike, double t, double vol, double r, double q,
+                     int32_t option_type, int32_t paths, double* se);
+double qko_qmc_halton(double spot, double strike, double t, double vol, double r, double q,
+                      int32_t option_type, int32_t paths, double* se);
+
 /* Batch forms (OpenMP over options when built with it).  out_se may be NULL. */
 void qko_heston_batch(const double* spot, const double* strike, const double* t,
                       const double* r, const double* q, const double* v0,
@@ -80,7 +95,8 @@ void qko_heston_batch(const double* spot, const double* strike, const double* t,
                       const int32_t* steps, const uint64_t* seed, int32_t n,
                       double* out, double* out_se);
 /* model: 0 = standard MC (antithetic terminal), 1 = antithetic variates,
- *        2 = Euler, 3 = Milstein, 4 = local vol (constant), 5 = terminal plain */
+ *        2 = Euler, 3 = Milstein, 4 = local vol (constant), 5 = terminal plain,
+ *        8 = control variates, 10 = stratified, 11 = QMC Sobol, 12 = QMC Halton */
 void qko_bsm_family_batch(int32_t model, const double* spot, const double* strike,
                           const double* t, const double* vol, const double* r,
                           const double* q, const int32_t* option_type, const int32_t* paths,
@@ -106,6 +122,12 @@ double qko_philox_price(int32_t model, double spot, double strike, double t, dou
                         double r, double q, double v0, double kappa, double theta,
                         double sigma, double rho, int32_t option_type, int32_t paths,
                         int32_t steps, uint64_t seed, int32_t antithetic, double* se);
+
+/* Variance-reduction models 8-12 (9 = importance sampling with `shift`) on
+ * the GPU's Philox stream, FP64, with the GPU's estimators. */
+double qko_philox_vr_price(int32_t model, double spot, double strike, double t, double vol,
+                           double r, double q, double shift, int32_t option_type, int32_t paths,
+                           uint64_t seed, double* se);
 
 #ifdef __cplusplus
 }

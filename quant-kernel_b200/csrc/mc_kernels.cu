@@ -17,6 +17,9 @@
 //   terminal   mc_engine.h:32-75   + model_concepts.h:93-102
 //   stepwise   mc_engine.h:84-103  + model_concepts.h:136-158, 240-266
 //   Heston     mc_engine.h:113-136 + model_concepts.h:205-226
+//   variance reduction (terminal GBM, FP64 path arithmetic)
+//              control_variates.cpp:10-52, importance_sampling.cpp:11-36,
+//              stratified_sampling.cpp:11-35, quasi_monte_carlo.cpp:10-56
 // Heston keeps log(S/spot) instead of S: the reference's s * exp(a) step with
 // the std::max(s, 1e-12) floor is the same map as x + a floored at
 // log(1e-12/spot), and it removes the per-step exp.
@@ -36,6 +39,7 @@ struct Acc {
     DD sy{0.0, 0.0};
     DD q{0.0, 0.0};
     double lone = 0.0;
+    double cx = 0.0, cxx = 0.0, cxy = 0.0;  // control variates only
     __device__ __forceinline__ void add_pair(double a, double b) {
         const double y = __dmul_rn(0.5, __dadd_rn(a, b));
         sy = dd_add(sy, y);
@@ -47,6 +51,53 @@ struct Acc {
         q = dd_add(q, __dmul_rn(a, a));
     }
 };
+
+// ----------------------------------------------------------------------------
+// Inverse normal CDF: P. J. Acklam's rational approximation (2003; relative
+// error < 1.15e-9), the one the reference evaluates
+// (monte_carlo_methods/common/internal_util.h:42-90).  Coefficients and the
+// Horner order are the published ones so that quasi-Monte Carlo prices, which
+// have no randomness, agree with the reference to rounding.
+// ----------------------------------------------------------------------------
+__device__ __forceinline__ double acklam_inv(double p) {
+    if (p <= 0.0 || p >= 1.0) return __longlong_as_double(0x7FF8000000000000ll);
+    constexpr double a[6] = {-3.969683028665376e+01, 2.209460984245205e+02, -2.759285104469687e+02,
+                             1.383577518672690e+02, -3.066479806614716e+01, 2.506628277459239e+00};
+    constexpr double b[5] = {-5.447609879822406e+01, 1.615858368580409e+02, -1.556989798598866e+02,
+                             6.680131188771972e+01, -1.328068155288572e+01};
+    constexpr double c[6] = {-7.784894002430293e-03, -3.223964580411365e-01, -2.400758277161838e+00,
+                             -2.549732539343734e+00, 4.374664141464968e+00, 2.938163982698783e+00};
+    constexpr double d[4] = {7.784695709041462e-03, 3.224671290700398e-01, 2.445134137142996e+00,
+                             3.754408661907416e+00};
+    constexpr double p_low = 0.02425;
+    const bool lo = p < p_low, hi = p > 1.0 - p_low;
+    if (lo || hi) {
+        const double t = sqrt(-2.0 * log(lo ? p : 1.0 - p));
+        double num = c[0];
+#pragma unroll
+        for (int i = 1; i < 6; ++i) num = num * t + c[i];
+        double den = d[0];
+#pragma unroll
+        for (int i = 1; i < 4; ++i) den = den * t + d[i];
+        den = den * t + 1.0;
+        return (lo ? num : -num) / den;
+    }
+    const double t = p - 0.5;
+    const double r = t * t;
+    double num = a[0];
+#pragma unroll
+    for (int i = 1; i < 6; ++i) num = num * r + a[i];
+    double den = b[0];
+#pragma unroll
+    for (int i = 1; i < 5; ++i) den = den * r + b[i];
+    den = den * r + 1.0;
+    return num * t / den;
+}
+
+// std::clamp(u, 1e-12, 1 - 1e-12) (a NaN stays NaN).
+__device__ __forceinline__ double clamp_unit(double u) {
+    return u < 1e-12 ? 1e-12 : ((1.0 - 1e-12) < u ? 1.0 - 1e-12 : u);
+}
 
 // ----------------------------------------------------------------------------
 // Terminal GBM (models 0, 1, 5).  Unit = quad of four normals (one Philox
@@ -236,34 +287,142 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
 }
 
 // ----------------------------------------------------------------------------
+// Terminal GBM with a variance-reduction estimator (models 8-12).  Unit = quad
+// of four consecutive paths 4u .. 4u+3; the path arithmetic is FP64 like the
+// reference's: S_T = spot exp(d0 + d1 z).
+//   control variates   z from the plain normal stream; sums of the payoff and
+//                      of the centred control c = S_T - E[S_T]
+//   importance         z from the plain normal stream, y = z + shift,
+//                      payoff(S_T(y)) exp(-shift y + shift^2 / 2)
+//   stratified         u = (i + U_i) / n with U_i uniform (Philox stream
+//                      c3 = 2), z = Acklam(u); q collects (y_2k - y_2k+1)^2 of
+//                      neighbouring strata, which are in the same quad
+//   Sobol / Halton     u = the i-th point (1-based) of the base-2 van der
+//                      Corput sequence in Gray-code order (Sobol, dimension
+//                      one) or natural order (Halton base 2), z = Acklam(u)
+// ----------------------------------------------------------------------------
+template <int UPT>
+__device__ __forceinline__ void sim_vr(const McOption& o, uint32_t unit0, uint32_t stride,
+                                       uint32_t k0, uint32_t k1, Acc& acc) {
+    const uint32_t n = (uint32_t)o.paths;
+    const int32_t m = o.model;
+    const double d0 = o.d[0], d1 = o.d[1], shift = o.d[2], mean_st = o.d[3];
+#pragma unroll
+    for (int k = 0; k < UPT; ++k) {
+        const uint32_t unit = unit0 + (uint32_t)k * stride;
+        if (unit * 4u >= n) continue;
+        double z[4];
+        if (m == kQmcSobol || m == kQmcHalton) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t i1 = unit * 4u + (uint32_t)s + 1u;
+                // quasi_monte_carlo.cpp:23-24 / 46-47 with internal_util.h:104-130:
+                // bit j of the (Gray-coded) index goes to bit 31 - j.
+                const uint32_t x = __brev(m == kQmcSobol ? (i1 ^ (i1 >> 1)) : i1);
+                const double u = m == kQmcSobol ? ((double)x + 0.5) / 4294967296.0
+                                                : (double)x * 0x1p-32;
+                z[s] = acklam_inv(clamp_unit(u));
+            }
+        } else if (m == kStratified) {
+            const U4 w = philox4x32_10(unit, 0u, 0u, 2u, k0, k1);
+            const uint32_t bits[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const double ui = ((double)bits[s] + 0.5) * 0x1p-32;
+                const double u = ((double)(unit * 4u + (uint32_t)s) + ui) / (double)n;
+                z[s] = acklam_inv(clamp_unit(u));
+            }
+        } else {
+            float zf[4];
+            normals4(unit, 0u, 1u, k0, k1, zf);
+#pragma unroll
+            for (int s = 0; s < 4; ++s) z[s] = (double)zf[s];
+        }
+        double y[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const bool valid = unit * 4u + (uint32_t)s < n;
+            double zz = z[s];
+            double w = 1.0;
+            if (m == kImportanceSampling) {
+                zz = z[s] + shift;
+                w = exp(-shift * zz + 0.5 * shift * shift);
+            }
+            const double st = o.spot * exp(d0 + d1 * zz);
+            const double pay = payoff(st, o.strike, o.option_type) * w;
+            y[s] = pay;
+            if (!valid) continue;
+            acc.sy = dd_add(acc.sy, pay);
+            if (m != kStratified) acc.q = dd_add(acc.q, pay * pay);
+            if (m == kControlVariates) {
+                const double c = st - mean_st;
+                acc.cx += c;
+                acc.cxx += c * c;
+                acc.cxy += c * pay;
+            }
+        }
+        if (m == kStratified) {
+#pragma unroll
+            for (int s = 0; s < 4; s += 2) {
+                if (unit * 4u + (uint32_t)s + 1u < n) {
+                    const double dy = y[s] - y[s + 1];
+                    acc.q = dd_add(acc.q, dy * dy);
+                }
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
 // Fixed-order CTA reduction of (sy, q) into the tile's slot.
 // ----------------------------------------------------------------------------
-template <int BLOCK>
+template <int BLOCK, bool CV>
 __device__ __forceinline__ void reduce_tile(Acc acc, TilePartial* __restrict__ out, DD* smem) {
     constexpr int W = BLOCK / 32;
     DD a = acc.sy, b = acc.q;
     double lone = acc.lone;  // nonzero in at most one thread: plain sums are exact
+    double cx = acc.cx, cxx = acc.cxx, cxy = acc.cxy;
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         a = dd_merge(a, dd_shfl_down(a, off));
         b = dd_merge(b, dd_shfl_down(b, off));
         lone = __dadd_rn(lone, __shfl_down_sync(0xffffffffu, lone, off));
+        if (CV) {
+            cx = __dadd_rn(cx, __shfl_down_sync(0xffffffffu, cx, off));
+            cxx = __dadd_rn(cxx, __shfl_down_sync(0xffffffffu, cxx, off));
+            cxy = __dadd_rn(cxy, __shfl_down_sync(0xffffffffu, cxy, off));
+        }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (lane == 0) {
         smem[warp] = a;
         smem[W + warp] = b;
         smem[2 * W + warp] = DD{lone, 0.0};
+        if (CV) {
+            smem[3 * W + warp] = DD{cx, cxx};
+            smem[4 * W + warp] = DD{cxy, 0.0};
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
         DD ta = smem[0], tb = smem[W];
         double tl = smem[2 * W].hi;
+        double tx = 0.0, txx = 0.0, txy = 0.0;
+        if (CV) {
+            tx = smem[3 * W].hi;
+            txx = smem[3 * W].lo;
+            txy = smem[4 * W].hi;
+        }
 #pragma unroll
         for (int w = 1; w < W; ++w) {
             ta = dd_merge(ta, smem[w]);
             tb = dd_merge(tb, smem[W + w]);
             tl = __dadd_rn(tl, smem[2 * W + w].hi);
+            if (CV) {
+                tx = __dadd_rn(tx, smem[3 * W + w].hi);
+                txx = __dadd_rn(txx, smem[3 * W + w].lo);
+                txy = __dadd_rn(txy, smem[4 * W + w].hi);
+            }
         }
         TilePartial t;
         t.sy_hi = ta.hi;
@@ -271,7 +430,9 @@ __device__ __forceinline__ void reduce_tile(Acc acc, TilePartial* __restrict__ o
         t.q_hi = tb.hi;
         t.q_lo = tb.lo;
         t.lone = tl;
-        t.pad = 0.0;
+        t.cx = tx;
+        t.cxx = txx;
+        t.cxy = txy;
         *out = t;
     }
     __syncthreads();
@@ -300,6 +461,7 @@ __device__ __forceinline__ void sim_family(const McOption& o, uint32_t unit0, ui
     if (FAMILY == kFamMilstein) sim_stepwise<UPT, ANTI, true>(o, unit0, stride, k0, k1, acc);
     if (FAMILY == kFamHeston) sim_heston<UPT, ANTI, false>(o, unit0, stride, k0, k1, acc);
     if (FAMILY == kFamHestonLr) sim_heston<UPT, ANTI, true>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamVr) sim_vr<UPT>(o, unit0, stride, k0, k1, acc);
 }
 
 // One tile: all UPT * unit_iters units of every thread, then the reduction.
@@ -316,7 +478,16 @@ __device__ __forceinline__ void run_tile(const McOption& o, int64_t tile, TilePa
         if (base >= (uint32_t)o.units) break;
         sim_family<FAMILY, UPT, ANTI>(o, base + threadIdx.x, (uint32_t)BLOCK, k0, k1, acc);
     }
-    reduce_tile<BLOCK>(acc, partials + tile, smem);
+    reduce_tile<BLOCK, FAMILY == kFamVr>(acc, partials + tile, smem);
+}
+
+// The variance-reduction tile as a call: its FP64 path code needs more
+// registers than the persistent kernel's budget, and a call keeps the spills
+// inside it instead of in the other models' loops.
+template <int BLOCK>
+__device__ __noinline__ void run_tile_vr(const McOption& o, int64_t tile, TilePartial* partials,
+                                         DD* smem) {
+    run_tile<kFamVr, BLOCK, kUptVr, false>(o, tile, partials, smem);
 }
 
 // ----------------------------------------------------------------------------
@@ -329,7 +500,7 @@ template <int FAMILY, int BLOCK, int UPT, bool ANTI>
 __global__ void __launch_bounds__(BLOCK)
     mc_simulate_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
                        int32_t n, int64_t n_tiles, TilePartial* __restrict__ partials) {
-    __shared__ DD smem[3 * (BLOCK / 32)];
+    __shared__ DD smem[5 * (BLOCK / 32)];
     for (int64_t tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const int32_t oi = find_option(tile_begin, n, tile);
         const McOption o = opts[oi];
@@ -350,7 +521,7 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
     mc_persistent_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
                          int32_t n, int64_t n_tiles, TilePartial* __restrict__ partials,
                          unsigned long long* __restrict__ work_counter) {
-    __shared__ DD smem[3 * (BLOCK / 32)];
+    __shared__ DD smem[5 * (BLOCK / 32)];
     __shared__ long long s_tile;
     for (;;) {
         if (threadIdx.x == 0) s_tile = (long long)atomicAdd(work_counter, 1ull);
@@ -381,6 +552,13 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
                     run_tile<kFamMilstein, BLOCK, kUptStepwise, true>(o, tile, partials, smem);
                 else
                     run_tile<kFamMilstein, BLOCK, kUptStepwise, false>(o, tile, partials, smem);
+                break;
+            case kControlVariates:
+            case kImportanceSampling:
+            case kStratified:
+            case kQmcSobol:
+            case kQmcHalton:
+                run_tile_vr<BLOCK>(o, tile, partials, smem);
                 break;
             case kHestonLrDelta:
                 if (anti)
@@ -420,33 +598,66 @@ __global__ void __launch_bounds__(256)
         return;
     }
     DD sy{0.0, 0.0}, q{0.0, 0.0};
-    double lone = 0.0;
+    double lone = 0.0, cx = 0.0, cxx = 0.0, cxy = 0.0;
     for (int32_t t = lane; t < o.tiles; t += 32) {
         const TilePartial p = partials[o.tile_begin + t];
         sy = dd_merge(sy, DD{p.sy_hi, p.sy_lo});
         q = dd_merge(q, DD{p.q_hi, p.q_lo});
         lone = __dadd_rn(lone, p.lone);
+        cx = __dadd_rn(cx, p.cx);
+        cxx = __dadd_rn(cxx, p.cxx);
+        cxy = __dadd_rn(cxy, p.cxy);
     }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         sy = dd_merge(sy, dd_shfl_down(sy, off));
         q = dd_merge(q, dd_shfl_down(q, off));
         lone = __dadd_rn(lone, __shfl_down_sync(0xffffffffu, lone, off));
+        cx = __dadd_rn(cx, __shfl_down_sync(0xffffffffu, cx, off));
+        cxx = __dadd_rn(cxx, __shfl_down_sync(0xffffffffu, cxx, off));
+        cxy = __dadd_rn(cxy, __shfl_down_sync(0xffffffffu, cxy, off));
     }
     if (lane == 0) {
         const double s = sy.hi + sy.lo;
         const double qq = q.hi + q.lo;
-        // sum of all path payoffs: two per pair, plus the unpaired path
-        const double total = o.antithetic ? __dadd_rn(2.0 * s, lone) : s;
-        out_price[warp] = o.disc * (total / (double)o.paths);
-        const double ns = (double)o.samples;
-        double se = __longlong_as_double(0x7FF8000000000000ll);
-        if (ns >= 2.0) {
-            const double mean = s / ns;
-            double var = (qq - ns * mean * mean) / (ns - 1.0);
-            if (var < 0.0) var = 0.0;
-            se = o.disc * sqrt(var / ns);
+        const double np = (double)o.paths;
+        const double nan = __longlong_as_double(0x7FF8000000000000ll);
+        double price, se = nan;
+        if (o.model == kControlVariates) {
+            // control_variates.cpp:40-51 with x = disc S_T and y = disc payoff;
+            // the control is summed centred on E[S_T], so mean_x - E[x] is
+            // disc * mc and the disc factors cancel in beta.
+            const double mp = s / np, mc = cx / np;
+            const double vc = cxx / np - mc * mc;
+            const double vp = qq / np - mp * mp;
+            if (o.disc * o.disc * vc <= 1e-12) {
+                price = o.disc * mp;
+                if (np >= 2.0) se = o.disc * sqrt(fmax(vp, 0.0) / (np - 1.0));
+            } else {
+                const double cov = cxy / np - mc * mp;
+                const double beta = cov / vc;
+                price = o.disc * (mp - beta * mc);
+                // residual variance of payoff - beta * control
+                const double res = vp - cov * beta;
+                se = o.disc * sqrt(fmax(res, 0.0) / (np - 2.0));
+            }
+        } else if (o.model == kStratified) {
+            price = o.disc * (s / np);
+            // paired strata: Var(mean) ~ sum over pairs (y_a - y_b)^2 / n^2
+            se = o.disc * sqrt(qq) / np;
+        } else {
+            // sum of all path payoffs: two per pair, plus the unpaired path
+            const double total = o.antithetic ? __dadd_rn(2.0 * s, lone) : s;
+            price = o.disc * (total / np);
+            const double ns = (double)o.samples;
+            if (ns >= 2.0) {
+                const double mean = s / ns;
+                double var = (qq - ns * mean * mean) / (ns - 1.0);
+                if (var < 0.0) var = 0.0;
+                se = o.disc * sqrt(var / ns);
+            }
         }
+        out_price[warp] = price;
         out_se[warp] = se;
     }
 }
@@ -496,6 +707,11 @@ int family_of(int32_t model) {
         case kLocalVol: return kFamEuler;
         case kMilstein: return kFamMilstein;
         case kHestonLrDelta: return kFamHestonLr;
+        case kControlVariates:
+        case kImportanceSampling:
+        case kStratified:
+        case kQmcSobol:
+        case kQmcHalton: return kFamVr;
         default: return kFamHeston;
     }
 }
@@ -509,6 +725,7 @@ cudaError_t launch_simulate(int family, bool anti, int block, int upt, const Sim
         case kFamMilstein: return launch_anti<kFamMilstein>(anti, block, upt, a, st);
         case kFamHeston: return launch_anti<kFamHeston>(anti, block, upt, a, st);
         case kFamHestonLr: return launch_anti<kFamHestonLr>(anti, block, upt, a, st);
+        case kFamVr: return launch_block<kFamVr, false>(block, upt, a, st);
         default: return cudaErrorInvalidValue;
     }
 }

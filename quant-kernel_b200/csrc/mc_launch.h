@@ -16,13 +16,15 @@ enum : int {
     kFamMilstein = 2,
     kFamHeston = 3,
     kFamHestonLr = 4,
-    kNumFamilies = 5
+    kFamVr = 5,  // terminal GBM with a variance-reduction estimator (models 8-12)
+    kNumFamilies = 6
 };
 
 // Units per thread compiled into the persistent mixed-model kernel.
 constexpr int kUptTerminal = 1;
 constexpr int kUptStepwise = 2;
 constexpr int kUptHeston = 2;
+constexpr int kUptVr = 1;
 
 struct SimArgs {
     const McOption* opts;      // device, n records

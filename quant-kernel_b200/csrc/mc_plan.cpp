@@ -5,6 +5,8 @@
 //   standard_monte_carlo.cpp:14-23   antithetic_variates.cpp:14-19
 //   euler_maruyama.cpp:14-19         milstein.cpp:14-19
 //   local_vol_monte_carlo.cpp:61-66  heston_monte_carlo.cpp:17-26
+//   control_variates.cpp:13-18       importance_sampling.cpp:14-20
+//   stratified_sampling.cpp:14-19    quasi_monte_carlo.cpp:13-18, 36-41
 //   option_util.h:27-50, monte_carlo_methods/common/internal_util.h:13-26
 // An invalid option gets NaN and the batch still returns QK_OK
 // (qk_api.cpp:1152-1159 writes per-element results), t <= 1e-12 gives the
@@ -73,6 +75,7 @@ int upt_for(int family, bool persistent, const LaunchConfig& cfg) {
     switch (family) {
         case kFamTerminal: return kUptTerminal;
         case kFamHeston: return kUptHeston;
+        case kFamVr: return kUptVr;
         default: return kUptStepwise;
     }
 }
@@ -116,7 +119,7 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
     o.model = m;
     o.option_type = in.option_type[i];
     o.paths = in.paths[i];
-    o.seed = in.seed[i];
+    o.seed = in.seed ? in.seed[i] : 0;  // the quasi-Monte Carlo calls take no seed
     o.spot = in.spot[i];
     o.strike = in.strike[i];
     o.mode = kModeSimulate;
@@ -220,6 +223,33 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
         o.p[9] = (float)std::log(1e-12 / spot);
         return o;
     }
+    if (m >= kControlVariates && m <= kQmcHalton) {
+        const double vol = in.vol[i], r = in.r[i], q = in.q[i];
+        const double shift = (m == kImportanceSampling) ? (in.shift ? in.shift[i] : in.v0[i]) : 0.0;
+        o.steps = 1;
+        // control variates need three paths (control_variates.cpp:14-15); a
+        // non-finite shift is rejected (importance_sampling.cpp:15-16)
+        const int32_t min_paths = (m == kControlVariates) ? 3 : 2;
+        if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || paths < min_paths ||
+            !finite_bits(shift)) {
+            set_const(o, nan_value());
+            return o;
+        }
+        if (t <= kEps) {
+            set_const(o, intrinsic(spot, strike, ot));
+            return o;
+        }
+        o.disc = std::exp(-r * t);
+        o.antithetic = 0;
+        o.units = (int32_t)(((int64_t)paths + 3) / 4);
+        o.samples = paths;
+        // model_concepts.h:93-102, evaluated in the same order
+        o.d[0] = (r - q - 0.5 * vol * vol) * t;
+        o.d[1] = vol * std::sqrt(smax(t, 0.0));
+        o.d[2] = shift;
+        o.d[3] = spot * std::exp((r - q) * t);
+        return o;
+    }
     set_const(o, nan_value());  // unknown model code
     return o;
 }
@@ -283,7 +313,7 @@ void PinnedBuf::release() {
 LaunchConfig default_config(int family) {
     LaunchConfig c;
     c.block = 256;
-    c.upt = (family == kFamTerminal) ? 1 : 2;
+    c.upt = (family == kFamTerminal || family == kFamVr) ? 1 : 2;
     return c;
 }
 

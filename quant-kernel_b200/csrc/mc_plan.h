@@ -22,6 +22,7 @@ struct BatchInput {
     const double *v0 = nullptr, *kappa = nullptr, *theta = nullptr, *sigma = nullptr,
                  *rho = nullptr;
     const double* weight_clip = nullptr;  // Heston LR delta; null: taken from `vol`
+    const double* shift = nullptr;        // importance sampling; null: taken from `v0`
     const int32_t *option_type = nullptr, *paths = nullptr, *steps = nullptr;
     const uint64_t* seed = nullptr;
     int32_t n = 0;

@@ -17,7 +17,13 @@ enum : int32_t {
     kTerminalPlain = 5,
     kHeston = 6,
     kHestonLrDelta = 7,  // likelihood-ratio delta under the Heston model
-    kNumModels = 8
+    // terminal GBM with a variance-reduction estimator
+    kControlVariates = 8,     // control_variates.cpp:10-52
+    kImportanceSampling = 9,  // importance_sampling.cpp:11-36
+    kStratified = 10,         // stratified_sampling.cpp:11-35
+    kQmcSobol = 11,           // quasi_monte_carlo.cpp:10-32
+    kQmcHalton = 12,          // quasi_monte_carlo.cpp:34-56
+    kNumModels = 13
 };
 
 enum : int32_t { kModeSimulate = 0, kModeConstant = 1 };
@@ -38,6 +44,10 @@ enum : int32_t { kModeSimulate = 0, kModeConstant = 1 };
 //                      p9 = log(1e-12 / spot) (floor of log(S/spot))
 //   Heston LR delta (7): the Heston constants; the record's weight_clip
 //                      bounds the first-step score z1 / (sqrt(v0) sqrt(dt) S0)
+// Variance-reduction models (8-12) keep FP64 constants in d[] (the same bytes):
+//   d0 = (r - q - vol^2/2) t      d1 = vol sqrt(t)
+//   d2 = importance-sampling shift
+//   d3 = spot exp((r - q) t), the mean of S_T (control-variate centre)
 // ---------------------------------------------------------------------------
 struct alignas(16) McOption {
     double spot;
@@ -59,19 +69,25 @@ struct alignas(16) McOption {
     int32_t unit_iters;  // per-thread passes over the tile
     int32_t mode;
     int32_t antithetic;
-    float p[10];
+    union {
+        float p[10];
+        double d[5];
+    };
 };
 static_assert(sizeof(McOption) == 128, "McOption layout");
 
 // Per-tile partial sums: y = pair mean (antithetic) or payoff (plain).  The
 // unpaired last path of an odd antithetic count is kept apart in `lone`: it
-// belongs in the price but not in the pair-mean variance.
+// belongs in the price but not in the pair-mean variance.  Stratified
+// sampling puts the sum of squared differences of paired strata in q; the
+// control-variate model adds plain FP64 sums of the centred control
+// c = S_T - E[S_T]: sum c, sum c^2 and sum c * payoff.
 struct alignas(16) TilePartial {
     double sy_hi, sy_lo;  // sum of y over full samples
     double q_hi, q_lo;    // sum of y^2 over full samples
     double lone;          // payoff of the unpaired path (0 elsewhere)
-    double pad;
+    double cx, cxx, cxy;  // control variates only (0 elsewhere)
 };
-static_assert(sizeof(TilePartial) == 48, "TilePartial layout");
+static_assert(sizeof(TilePartial) == 64, "TilePartial layout");
 
 }  // namespace qkb

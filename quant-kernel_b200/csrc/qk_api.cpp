@@ -177,6 +177,34 @@ int32_t heston_batch(const double* spot, const double* strike, const double* t, 
                      0, out_prices, out_se, where);
 }
 
+// Terminal variance-reduction models.  Null checks in each reference batch's
+// declaration order: (spot, strike, t, vol, r, q, option_type, paths,
+// [shift,] [seed,] out_prices); the quasi-Monte Carlo calls take no seed.
+int32_t vr_batch(int32_t model, const double* spot, const double* strike, const double* t,
+                 const double* vol, const double* r, const double* q, const int32_t* option_type,
+                 const int32_t* paths, const double* shift, const uint64_t* seed, int32_t n,
+                 double* out_prices, double* out_se, bool want_se, const char* where) {
+    const bool has_seed = model != qkb::kQmcSobol && model != qkb::kQmcHalton;
+    const bool has_shift = model == qkb::kImportanceSampling;
+    NamedPtr ptrs[12];
+    int k = 0;
+    for (const NamedPtr& np : {NamedPtr{spot, "spot"}, NamedPtr{strike, "strike"}, NamedPtr{t, "t"},
+                               NamedPtr{vol, "vol"}, NamedPtr{r, "r"}, NamedPtr{q, "q"},
+                               NamedPtr{option_type, "option_type"}, NamedPtr{paths, "paths"}})
+        ptrs[k++] = np;
+    if (has_shift) ptrs[k++] = NamedPtr{shift, "shift"};
+    if (has_seed) ptrs[k++] = NamedPtr{seed, "seed"};
+    ptrs[k++] = NamedPtr{out_prices, "out_prices"};
+    if (want_se) ptrs[k++] = NamedPtr{out_se, "out_stderr"};
+    for (int i = 0; i < k; ++i)
+        if (!ptrs[i].p) return fail_null(ptrs[i].name);
+    if (n <= 0) return fail_size(n);
+    qkb::BatchInput in = bsm_input(model, spot, strike, t, vol, r, q, option_type, paths, nullptr,
+                                   has_seed ? seed : nullptr, n);
+    in.shift = shift;
+    return run_batch(in, 0, out_prices, out_se, where);
+}
+
 // Mixed-model input: checks the arrays that the present models need.
 int32_t mixed_input(const int32_t* model, const double* spot, const double* strike,
                     const double* t, const double* vol, const double* r, const double* q,
@@ -189,12 +217,15 @@ int32_t mixed_input(const int32_t* model, const double* spot, const double* stri
                              {seed, "seed"}};
     if (int32_t rc = check_nulls(base)) return rc;
     if (n <= 0) return fail_size(n);
-    bool need_vol = false, need_heston = false, need_steps = false;
+    bool need_vol = false, need_heston = false, need_steps = false, need_shift = false;
     for (int32_t i = 0; i < n; ++i) {
         const int32_t m = model[i];
         // the LR delta reads its weight clip from `vol`
-        if ((m >= qkb::kStandard && m <= qkb::kTerminalPlain) || m == qkb::kHestonLrDelta)
+        if ((m >= qkb::kStandard && m <= qkb::kTerminalPlain) || m == qkb::kHestonLrDelta ||
+            (m >= qkb::kControlVariates && m <= qkb::kQmcHalton))
             need_vol = true;
+        // importance sampling reads its shift from `v0`
+        if (m == qkb::kImportanceSampling) need_shift = true;
         if (m == qkb::kEuler || m == qkb::kMilstein || m == qkb::kLocalVol || m == qkb::kHeston ||
             m == qkb::kHestonLrDelta)
             need_steps = true;
@@ -207,6 +238,7 @@ int32_t mixed_input(const int32_t* model, const double* spot, const double* stri
         if (int32_t rc = check_nulls(hp)) return rc;
     }
     if (need_steps && !steps) return fail_null("steps");
+    if (need_shift && !v0) return fail_null("v0");
     in->model = model;
     in->spot = spot;
     in->strike = strike;
@@ -493,6 +525,95 @@ double qk_mcm_heston_lr_delta(double spot, double strike, double t, double r, do
     if (qk_mcm_heston_lr_delta_batch(&spot, &strike, &t, &r, &q, &v0, &kappa, &theta, &sigma, &rho,
                                      &option_type, &paths, &steps, &seed, &weight_clip, 1,
                                      &out) != QK_OK)
+        return nan_value();
+    return out;
+}
+
+// ---- terminal variance reduction ---------------------------------------------------
+#define QK_VR_SEEDED(NAME, MODEL)                                                              \
+    int32_t qk_mcm_##NAME##_price_batch(const double* spot, const double* strike, const double* t, \
+                                        const double* vol, const double* r, const double* q,     \
+                                        const int32_t* option_type, const int32_t* paths,        \
+                                        const uint64_t* seed, int32_t n, double* out_prices) {   \
+        return vr_batch(MODEL, spot, strike, t, vol, r, q, option_type, paths, nullptr, seed, n, \
+                        out_prices, nullptr, false, "qk_mcm_" #NAME "_price_batch");            \
+    }                                                                                          \
+    int32_t qk_mcm_##NAME##_price_se_batch(                                                    \
+        const double* spot, const double* strike, const double* t, const double* vol,          \
+        const double* r, const double* q, const int32_t* option_type, const int32_t* paths,    \
+        const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr) {             \
+        return vr_batch(MODEL, spot, strike, t, vol, r, q, option_type, paths, nullptr, seed, n, \
+                        out_prices, out_stderr, true, "qk_mcm_" #NAME "_price_se_batch");       \
+    }                                                                                          \
+    double qk_mcm_##NAME##_price(double spot, double strike, double t, double vol, double r,   \
+                                 double q, int32_t option_type, int32_t paths, uint64_t seed) { \
+        double out = nan_value();                                                              \
+        if (qk_mcm_##NAME##_price_batch(&spot, &strike, &t, &vol, &r, &q, &option_type, &paths, \
+                                        &seed, 1, &out) != QK_OK)                              \
+            return nan_value();                                                                \
+        return out;                                                                            \
+    }
+
+#define QK_VR_QMC(NAME, MODEL)                                                                 \
+    int32_t qk_mcm_##NAME##_price_batch(const double* spot, const double* strike, const double* t, \
+                                        const double* vol, const double* r, const double* q,     \
+                                        const int32_t* option_type, const int32_t* paths,        \
+                                        int32_t n, double* out_prices) {                         \
+        return vr_batch(MODEL, spot, strike, t, vol, r, q, option_type, paths, nullptr, nullptr, \
+                        n, out_prices, nullptr, false, "qk_mcm_" #NAME "_price_batch");         \
+    }                                                                                          \
+    int32_t qk_mcm_##NAME##_price_se_batch(                                                    \
+        const double* spot, const double* strike, const double* t, const double* vol,          \
+        const double* r, const double* q, const int32_t* option_type, const int32_t* paths,    \
+        int32_t n, double* out_prices, double* out_stderr) {                                   \
+        return vr_batch(MODEL, spot, strike, t, vol, r, q, option_type, paths, nullptr, nullptr, \
+                        n, out_prices, out_stderr, true, "qk_mcm_" #NAME "_price_se_batch");    \
+    }                                                                                          \
+    double qk_mcm_##NAME##_price(double spot, double strike, double t, double vol, double r,   \
+                                 double q, int32_t option_type, int32_t paths) {               \
+        double out = nan_value();                                                              \
+        if (qk_mcm_##NAME##_price_batch(&spot, &strike, &t, &vol, &r, &q, &option_type, &paths, \
+                                        1, &out) != QK_OK)                                     \
+            return nan_value();                                                                \
+        return out;                                                                            \
+    }
+
+QK_VR_SEEDED(control_variates, qkb::kControlVariates)
+QK_VR_SEEDED(stratified_sampling, qkb::kStratified)
+QK_VR_QMC(quasi_monte_carlo_sobol, qkb::kQmcSobol)
+QK_VR_QMC(quasi_monte_carlo_halton, qkb::kQmcHalton)
+#undef QK_VR_SEEDED
+#undef QK_VR_QMC
+
+int32_t qk_mcm_importance_sampling_price_batch(const double* spot, const double* strike,
+                                               const double* t, const double* vol, const double* r,
+                                               const double* q, const int32_t* option_type,
+                                               const int32_t* paths, const double* shift,
+                                               const uint64_t* seed, int32_t n,
+                                               double* out_prices) {
+    return vr_batch(qkb::kImportanceSampling, spot, strike, t, vol, r, q, option_type, paths,
+                    shift, seed, n, out_prices, nullptr, false,
+                    "qk_mcm_importance_sampling_price_batch");
+}
+
+int32_t qk_mcm_importance_sampling_price_se_batch(const double* spot, const double* strike,
+                                                  const double* t, const double* vol,
+                                                  const double* r, const double* q,
+                                                  const int32_t* option_type, const int32_t* paths,
+                                                  const double* shift, const uint64_t* seed,
+                                                  int32_t n, double* out_prices,
+                                                  double* out_stderr) {
+    return vr_batch(qkb::kImportanceSampling, spot, strike, t, vol, r, q, option_type, paths,
+                    shift, seed, n, out_prices, out_stderr, true,
+                    "qk_mcm_importance_sampling_price_se_batch");
+}
+
+double qk_mcm_importance_sampling_price(double spot, double strike, double t, double vol, double r,
+                                        double q, int32_t option_type, int32_t paths, double shift,
+                                        uint64_t seed) {
+    double out = nan_value();
+    if (qk_mcm_importance_sampling_price_batch(&spot, &strike, &t, &vol, &r, &q, &option_type,
+                                               &paths, &shift, &seed, 1, &out) != QK_OK)
         return nan_value();
     return out;
 }

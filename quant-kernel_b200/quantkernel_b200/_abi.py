@@ -23,6 +23,11 @@ QK_MC_LOCAL_VOL = 4
 QK_MC_TERMINAL_PLAIN = 5
 QK_MC_HESTON = 6
 QK_MC_HESTON_LR_DELTA = 7
+QK_MC_CONTROL_VARIATES = 8
+QK_MC_IMPORTANCE_SAMPLING = 9  # shift read from v0 in mixed batches and plans
+QK_MC_STRATIFIED = 10
+QK_MC_QMC_SOBOL = 11
+QK_MC_QMC_HALTON = 12
 
 QK_PLAN_PERSISTENT = 0x1
 QK_PLAN_GRAPH = 0x2

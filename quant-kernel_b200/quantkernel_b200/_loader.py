@@ -40,6 +40,10 @@ _step_batch = [PD, PD, PD, PD, PD, PD, PI32, PI32, PI32, PU64, I32, PD]
 _hes_scalar = [D, D, D, D, D, D, D, D, D, D, I32, I32, I32, U64]
 _hes_batch = [PD] * 10 + [PI32, PI32, PI32, PU64, I32, PD]
 _mixed_arrays = [PI32] + [PD] * 11 + [PI32, PI32, PI32, PU64, I32]
+_is_scalar = [D, D, D, D, D, D, I32, I32, D, U64]
+_is_batch = [PD] * 6 + [PI32, PI32, PD, PU64, I32, PD]
+_qmc_scalar = [D, D, D, D, D, D, I32, I32]
+_qmc_batch = [PD] * 6 + [PI32, PI32, I32, PD]
 
 FUNCTION_SIGNATURES = [
     ("qk_abi_version", None, [ct.POINTER(I32), ct.POINTER(I32)]),
@@ -70,6 +74,21 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_heston_lr_delta", D, _hes_scalar + [D]),
     ("qk_mcm_heston_lr_delta_batch", I32, [PD] * 10 + [PI32, PI32, PI32, PU64, PD, I32, PD]),
     ("qk_mcm_heston_lr_delta_se_batch", I32, [PD] * 10 + [PI32, PI32, PI32, PU64, PD, I32, PD, PD]),
+    ("qk_mcm_control_variates_price", D, _term_scalar),
+    ("qk_mcm_control_variates_price_batch", I32, _term_batch),
+    ("qk_mcm_control_variates_price_se_batch", I32, _term_batch + [PD]),
+    ("qk_mcm_importance_sampling_price", D, _is_scalar),
+    ("qk_mcm_importance_sampling_price_batch", I32, _is_batch),
+    ("qk_mcm_importance_sampling_price_se_batch", I32, _is_batch + [PD]),
+    ("qk_mcm_stratified_sampling_price", D, _term_scalar),
+    ("qk_mcm_stratified_sampling_price_batch", I32, _term_batch),
+    ("qk_mcm_stratified_sampling_price_se_batch", I32, _term_batch + [PD]),
+    ("qk_mcm_quasi_monte_carlo_sobol_price", D, _qmc_scalar),
+    ("qk_mcm_quasi_monte_carlo_sobol_price_batch", I32, _qmc_batch),
+    ("qk_mcm_quasi_monte_carlo_sobol_price_se_batch", I32, _qmc_batch + [PD]),
+    ("qk_mcm_quasi_monte_carlo_halton_price", D, _qmc_scalar),
+    ("qk_mcm_quasi_monte_carlo_halton_price_batch", I32, _qmc_batch),
+    ("qk_mcm_quasi_monte_carlo_halton_price_se_batch", I32, _qmc_batch + [PD]),
     ("qk_cf_heston_price_cf", D, [D] * 10 + [I32, I32, D]),
     ("qk_cf_heston_price_cf_batch", I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
     ("qk_mcm_mixed_price_batch", I32, _mixed_arrays + [PD, PD]),

@@ -396,6 +396,121 @@ class QuantKernel:
                                                         sigma, rho, option_type, paths, steps,
                                                         seed, weight_clip), with_se=True)
 
+    # ------------------------------------------------------------------ variance reduction
+    def control_variates_price(self, spot: float, strike: float, t: float, vol: float,
+                               r: float, q: float, option_type: int, paths: int,
+                               seed: int = 42) -> float:
+        """Terminal GBM with S_T as control variate (control_variates.cpp:10-52)."""
+        return self._call_checked("qk_mcm_control_variates_price",
+                                  spot, strike, t, vol, r, q, option_type, paths, seed)
+
+    def control_variates_price_batch(self, spot, strike, t, vol, r, q, option_type, paths,
+                                     seed) -> np.ndarray:
+        return self._call_batch_ctypes("qk_mcm_control_variates_price_batch",
+                                       *self._term_arrays(spot, strike, t, vol, r, q,
+                                                          option_type, paths, seed))
+
+    def control_variates_price_se_batch(self, spot, strike, t, vol, r, q, option_type, paths,
+                                        seed):
+        return self._call_batch_ctypes("qk_mcm_control_variates_price_se_batch",
+                                       *self._term_arrays(spot, strike, t, vol, r, q,
+                                                          option_type, paths, seed),
+                                       with_se=True)
+
+    def stratified_sampling_price(self, spot: float, strike: float, t: float, vol: float,
+                                  r: float, q: float, option_type: int, paths: int,
+                                  seed: int = 42) -> float:
+        """One draw per stratum of [0, 1) (stratified_sampling.cpp:11-35)."""
+        return self._call_checked("qk_mcm_stratified_sampling_price",
+                                  spot, strike, t, vol, r, q, option_type, paths, seed)
+
+    def stratified_sampling_price_batch(self, spot, strike, t, vol, r, q, option_type, paths,
+                                        seed) -> np.ndarray:
+        return self._call_batch_ctypes("qk_mcm_stratified_sampling_price_batch",
+                                       *self._term_arrays(spot, strike, t, vol, r, q,
+                                                          option_type, paths, seed))
+
+    def stratified_sampling_price_se_batch(self, spot, strike, t, vol, r, q, option_type,
+                                           paths, seed):
+        return self._call_batch_ctypes("qk_mcm_stratified_sampling_price_se_batch",
+                                       *self._term_arrays(spot, strike, t, vol, r, q,
+                                                          option_type, paths, seed),
+                                       with_se=True)
+
+    def _is_arrays(self, spot, strike, t, vol, r, q, option_type, paths, shift, seed):
+        s, k, tau, sig, rr, qq, ot, pp, sd = self._term_arrays(spot, strike, t, vol, r, q,
+                                                               option_type, paths, seed)
+        sh = self._as_f64_array(shift, "shift")
+        self._check_same_length(s.shape[0], shift=sh)
+        return s, k, tau, sig, rr, qq, ot, pp, sh, sd
+
+    def importance_sampling_price(self, spot: float, strike: float, t: float, vol: float,
+                                  r: float, q: float, option_type: int, paths: int,
+                                  shift: float, seed: int = 42) -> float:
+        """Normal shifted by `shift` with likelihood-ratio weights
+        (importance_sampling.cpp:11-36)."""
+        return self._call_checked("qk_mcm_importance_sampling_price",
+                                  spot, strike, t, vol, r, q, option_type, paths, shift, seed)
+
+    def importance_sampling_price_batch(self, spot, strike, t, vol, r, q, option_type, paths,
+                                        shift, seed) -> np.ndarray:
+        return self._call_batch_ctypes("qk_mcm_importance_sampling_price_batch",
+                                       *self._is_arrays(spot, strike, t, vol, r, q,
+                                                        option_type, paths, shift, seed))
+
+    def importance_sampling_price_se_batch(self, spot, strike, t, vol, r, q, option_type,
+                                           paths, shift, seed):
+        return self._call_batch_ctypes("qk_mcm_importance_sampling_price_se_batch",
+                                       *self._is_arrays(spot, strike, t, vol, r, q,
+                                                        option_type, paths, shift, seed),
+                                       with_se=True)
+
+    def _qmc_arrays(self, spot, strike, t, vol, r, q, option_type, paths):
+        s = self._as_f64_array(spot, "spot")
+        arrs = dict(strike=self._as_f64_array(strike, "strike"), t=self._as_f64_array(t, "t"),
+                    vol=self._as_f64_array(vol, "vol"), r=self._as_f64_array(r, "r"),
+                    q=self._as_f64_array(q, "q"),
+                    option_type=self._as_i32_array(option_type, "option_type"),
+                    paths=self._as_i32_array(paths, "paths"))
+        self._check_same_length(s.shape[0], **arrs)
+        return (s, *arrs.values())
+
+    def quasi_monte_carlo_sobol_price(self, spot: float, strike: float, t: float, vol: float,
+                                      r: float, q: float, option_type: int, paths: int) -> float:
+        """Sobol points 1..paths through Acklam's inverse normal (quasi_monte_carlo.cpp:10-32)."""
+        return self._call_checked("qk_mcm_quasi_monte_carlo_sobol_price",
+                                  spot, strike, t, vol, r, q, option_type, paths)
+
+    def quasi_monte_carlo_sobol_price_batch(self, spot, strike, t, vol, r, q, option_type,
+                                            paths) -> np.ndarray:
+        return self._call_batch_ctypes("qk_mcm_quasi_monte_carlo_sobol_price_batch",
+                                       *self._qmc_arrays(spot, strike, t, vol, r, q,
+                                                         option_type, paths))
+
+    def quasi_monte_carlo_sobol_price_se_batch(self, spot, strike, t, vol, r, q, option_type,
+                                               paths):
+        return self._call_batch_ctypes("qk_mcm_quasi_monte_carlo_sobol_price_se_batch",
+                                       *self._qmc_arrays(spot, strike, t, vol, r, q,
+                                                         option_type, paths), with_se=True)
+
+    def quasi_monte_carlo_halton_price(self, spot: float, strike: float, t: float, vol: float,
+                                       r: float, q: float, option_type: int, paths: int) -> float:
+        """Halton base-2 points (quasi_monte_carlo.cpp:34-56)."""
+        return self._call_checked("qk_mcm_quasi_monte_carlo_halton_price",
+                                  spot, strike, t, vol, r, q, option_type, paths)
+
+    def quasi_monte_carlo_halton_price_batch(self, spot, strike, t, vol, r, q, option_type,
+                                             paths) -> np.ndarray:
+        return self._call_batch_ctypes("qk_mcm_quasi_monte_carlo_halton_price_batch",
+                                       *self._qmc_arrays(spot, strike, t, vol, r, q,
+                                                         option_type, paths))
+
+    def quasi_monte_carlo_halton_price_se_batch(self, spot, strike, t, vol, r, q, option_type,
+                                                paths):
+        return self._call_batch_ctypes("qk_mcm_quasi_monte_carlo_halton_price_se_batch",
+                                       *self._qmc_arrays(spot, strike, t, vol, r, q,
+                                                         option_type, paths), with_se=True)
+
     # ------------------------------------------------------------------ Heston CF
     def heston_price_cf(self, spot: float, strike: float, t: float, r: float, q: float,
                         v0: float, kappa: float, theta: float, sigma: float, rho: float,

@@ -11,7 +11,9 @@ Cases: random small-size inputs for each Monte Carlo pricer on the hot path
 (odd and even path counts, 1..64 steps), the edge cases the reference's own
 tests and pricers define (t <= 1e-12, zero vol, invalid option type,
 paths <= 1, steps <= 0, NaN inputs that Heston does not reject, extreme rho),
-Heston characteristic-function prices and the reference's BSM closed form.
+the five terminal variance-reduction estimators (control variates,
+importance sampling, stratified, Sobol and Halton quasi-Monte Carlo), Heston
+characteristic-function prices and the reference's BSM closed form.
 """
 
 import json
@@ -25,7 +27,8 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from oracle.oracle import (  # noqa: E402
-    ANTITHETIC, EULER, HESTON, HESTON_LR_DELTA, LOCAL_VOL, MILSTEIN, STANDARD, Reference)
+    ANTITHETIC, EULER, HESTON, HESTON_LR_DELTA, IMPORTANCE_SAMPLING, LOCAL_VOL, MILSTEIN,
+    QMC_HALTON, QMC_SOBOL, STANDARD, VR_MODELS, Reference)
 
 OUT = Path(__file__).resolve().parent / "reference_mc.json"
 
@@ -109,6 +112,38 @@ def main() -> None:
     add(HESTON_LR_DELTA, vol=6.0, v0=0.0, paths=100, steps=4)         # zero score -> 0
     add(HESTON_LR_DELTA, vol=6.0, paths=3, seed=5)                    # odd count
     add(HESTON_LR_DELTA, vol=6.0, paths=1)                            # NaN
+
+    # terminal variance-reduction estimators (own generator: the draws above
+    # and the closed-form lists below keep their values)
+    rng_vr = np.random.default_rng(20261206)
+    for model in VR_MODELS:
+        for _ in range(10):
+            kw = dict(spot=float(rng_vr.uniform(80, 120)), strike=float(rng_vr.uniform(80, 120)),
+                      t=float(rng_vr.uniform(0.1, 2.0)), vol=float(rng_vr.uniform(0.1, 0.5)),
+                      r=float(rng_vr.uniform(0.0, 0.05)), q=float(rng_vr.uniform(0.0, 0.03)),
+                      option_type=int(rng_vr.integers(0, 2)), paths=int(rng_vr.integers(2, 3000)),
+                      steps=1, seed=int(rng_vr.integers(0, 2**63)))
+            if model == IMPORTANCE_SAMPLING:
+                kw["shift"] = float(rng_vr.uniform(-1.0, 1.0))
+            add(model, **kw)
+        extra = {"shift": 0.4} if model == IMPORTANCE_SAMPLING else {}
+        add(model, t=1e-14, spot=110.0, **extra)         # undiscounted intrinsic
+        add(model, t=1e-14, spot=90.0, option_type=1, **extra)
+        add(model, option_type=7, **extra)               # invalid type -> NaN
+        add(model, paths=1, **extra)                     # NaN
+        add(model, paths=2, seed=123, **extra)           # NaN for control variates only
+        add(model, paths=3, seed=123, **extra)
+        add(model, vol=0.0, **extra)                     # no zero-vol branch here
+        add(model, vol=float("nan"), **extra)
+        add(model, spot=-1.0, **extra)
+        add(model, paths=16384, **extra)                 # the reference's QMC test size
+    add(IMPORTANCE_SAMPLING, shift=float("nan"))          # non-finite shift -> NaN
+    add(IMPORTANCE_SAMPLING, shift=float("inf"))
+    add(IMPORTANCE_SAMPLING, shift=0.0, paths=500)
+    add(IMPORTANCE_SAMPLING, shift=2.5, strike=150.0, paths=4000)  # deep OTM call, shifted up
+    for model in (QMC_SOBOL, QMC_HALTON):
+        add(model, paths=1 << 20)                        # 2^20 points
+        add(model, paths=1000003, option_type=1, strike=90.0)
 
     cf = []
     for _ in range(24):

@@ -38,6 +38,12 @@ def test_drop_in_signatures_match_reference_subset():
     """Every reference MC batch/scalar entry on the hot path is declared here."""
     text = HEADER.read_text()
     for name in [
+        "qk_mcm_control_variates_price", "qk_mcm_control_variates_price_batch",
+        "qk_mcm_importance_sampling_price", "qk_mcm_importance_sampling_price_batch",
+        "qk_mcm_stratified_sampling_price", "qk_mcm_stratified_sampling_price_batch",
+        "qk_mcm_quasi_monte_carlo_sobol_price", "qk_mcm_quasi_monte_carlo_sobol_price_batch",
+        "qk_mcm_quasi_monte_carlo_halton_price", "qk_mcm_quasi_monte_carlo_halton_price_batch",
+        "qk_cf_heston_price_cf", "qk_cf_heston_price_cf_batch",
         "qk_mcm_standard_monte_carlo_price", "qk_mcm_standard_monte_carlo_price_batch",
         "qk_mcm_antithetic_variates_price", "qk_mcm_antithetic_variates_price_batch",
         "qk_mcm_euler_maruyama_price", "qk_mcm_euler_maruyama_price_batch",
@@ -94,6 +100,12 @@ BATCHES = {
     "qk_cf_heston_price_cf_batch":
         "spot strike t r q v0 kappa theta sigma rho option_type integration_steps "
         "integration_limit",
+    "qk_mcm_control_variates_price_batch": "spot strike t vol r q option_type paths seed",
+    "qk_mcm_stratified_sampling_price_batch": "spot strike t vol r q option_type paths seed",
+    "qk_mcm_importance_sampling_price_batch":
+        "spot strike t vol r q option_type paths shift seed",
+    "qk_mcm_quasi_monte_carlo_sobol_price_batch": "spot strike t vol r q option_type paths",
+    "qk_mcm_quasi_monte_carlo_halton_price_batch": "spot strike t vol r q option_type paths",
 }
 MC_BATCHES = sorted(k for k in BATCHES if k.startswith("qk_mcm_"))
 INT_ARGS = {"option_type", "paths", "steps", "integration_steps"}
@@ -183,6 +195,13 @@ def test_mixed_batch_requires_arrays_its_models_use(qk):
     rc = qk._lib.qk_mcm_mixed_price_batch(*base, _p(d), _p(d), _p(d), _p(d), _p(d), _p(i), _p(i),
                                           _p(i), _p(u), 0, _p(out), None)
     assert rc == -2
+    # importance sampling reads its shift from v0; the QMC models need no seed
+    # but the mixed call checks it for every batch
+    model2 = np.array([11, 9], np.int32)
+    base2 = [_p(model2)] + base[1:]
+    rc = qk._lib.qk_mcm_mixed_price_batch(*base2, None, None, None, None, None, _p(i), _p(i),
+                                          None, _p(u), n, _p(out), None)
+    assert rc == -1 and qk.get_last_error() == "null pointer: v0"
 
 
 def test_no_gpu_means_runtime_error_not_cpu_fallback(qk):

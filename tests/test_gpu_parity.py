@@ -13,36 +13,14 @@ import math
 
 import numpy as np
 import pytest
-from scipy import stats
+from stat_check import check_z, z_scores
 
 from quantkernel_b200 import workloads
 
 pytestmark = pytest.mark.gpu
 
-P_EXCEED = 2.0 * stats.norm.sf(3.0)  # 0.0027
-
-
-def _z(a, b, se):
-    """z-score; an option whose payoffs are all zero on both sides (deep out of
-    the money) has zero variance and must then agree exactly."""
-    a, b, se = map(np.asarray, (a, b, se))
-    zero = se == 0
-    assert np.all(a[zero] == b[zero])
-    return np.where(zero, 0.0, (a - b) / np.where(zero, 1.0, se))
-
-
-def _check(z, label, zmax=5.0):
-    z = np.asarray(z)
-    assert np.all(np.isfinite(z)), label
-    n = z.size
-    allowed = int(stats.binom.ppf(0.999, n, P_EXCEED))
-    exceed = int((np.abs(z) > 3.0).sum())
-    print(f"{label}: n={n} mean z={z.mean():+.3f} sd z={z.std():.3f} max|z|={np.abs(z).max():.2f} "
-          f"|z|>3: {exceed} (expected {n * P_EXCEED:.2f}, allowed {allowed})")
-    assert exceed <= allowed, label
-    assert np.abs(z).max() < zmax, label
-    # a biased estimator shifts the mean of z; its sd over n options is 1/sqrt(n)
-    assert abs(z.mean()) < 4.0 / math.sqrt(n), label
+_z = z_scores
+_check = check_z
 
 
 def test_bsm_terminal_full_size_vs_closed_form_and_reference(qk, oracle):
@@ -148,6 +126,8 @@ def test_fixture_edge_cases_on_gpu(qk, oracle):
         a = {k: (float.fromhex(v) if isinstance(v, str) else v) for k, v in case["args"].items()}
         want = float.fromhex(case["price"])
         m = case["model"]
+        if "shift" in a:  # importance sampling reads its shift from v0 in plans
+            a["v0"] = a.pop("shift")
         deterministic = (math.isnan(want) or a["t"] <= 1e-12 or a["paths"] <= 1 or
                          (m == 0 and a["vol"] <= 1e-12) or
                          (m == 6 and any(math.isnan(a[k]) for k in ("spot", "strike", "q", "v0"))))

@@ -1,0 +1,243 @@
+"""GPU terminal variance-reduction estimators against the reference.
+
+Models (yluoc/Quant-Kernel monte_carlo_methods/):
+  control variates    control_variates.cpp:10-52
+  importance sampling importance_sampling.cpp:11-36
+  stratified          stratified_sampling.cpp:11-35
+  Sobol / Halton QMC  quasi_monte_carlo.cpp:10-56
+
+Parity bars:
+  * quasi-Monte Carlo has no randomness: GPU == reference to 1e-10 relative
+    (FP64 on both sides; only the order of the payoff sum and the last bit of
+    exp/log differ);
+  * entry checks (NaN, intrinsic value at t <= 1e-12) are exact;
+  * stratified on the same Philox uniforms as the oracle's FP64 replay: 1e-12;
+  * control variates / importance sampling on the same Philox normals (FP32
+    Box-Muller on the GPU, FP64 in the replay): 5e-5 x S + 0.02 x SE;
+  * against the reference's CPU Monte Carlo (mt19937 streams): statistical,
+    z = difference / combined SE with the multiplicity rule of stat_check.
+"""
+
+import json
+import math
+from pathlib import Path
+
+import numpy as np
+import pytest
+from stat_check import check_z, z_scores
+
+from quantkernel_b200 import (QK_MC_CONTROL_VARIATES, QK_MC_IMPORTANCE_SAMPLING,
+                              QK_MC_QMC_HALTON, QK_MC_QMC_SOBOL, QK_MC_STRATIFIED, QK_PLAN_GRAPH,
+                              QK_PLAN_PERSISTENT, workloads)
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.loads((Path(__file__).parent / "golden" / "reference_mc.json").read_text())
+VR = (QK_MC_CONTROL_VARIATES, QK_MC_IMPORTANCE_SAMPLING, QK_MC_STRATIFIED, QK_MC_QMC_SOBOL,
+      QK_MC_QMC_HALTON)
+NAMES = {QK_MC_CONTROL_VARIATES: "control_variates", QK_MC_IMPORTANCE_SAMPLING: "importance_sampling",
+         QK_MC_STRATIFIED: "stratified_sampling", QK_MC_QMC_SOBOL: "quasi_monte_carlo_sobol",
+         QK_MC_QMC_HALTON: "quasi_monte_carlo_halton"}
+
+
+def _args(d):
+    return {k: (float.fromhex(v) if isinstance(v, str) else v) for k, v in d.items()}
+
+
+def _gpu(qk, model, cases, se=False):
+    """Price a list of argument dicts through the model's drop-in batch call."""
+    col = lambda k, dt=np.float64: np.array([c[k] for c in cases], dtype=dt)  # noqa: E731
+    base = [col("spot"), col("strike"), col("t"), col("vol"), col("r"), col("q"),
+            col("option_type", np.int32), col("paths", np.int32)]
+    name = NAMES[model] + ("_price_se_batch" if se else "_price_batch")
+    fn = getattr(qk, name)
+    if model in (QK_MC_QMC_SOBOL, QK_MC_QMC_HALTON):
+        return fn(*base)
+    if model == QK_MC_IMPORTANCE_SAMPLING:
+        return fn(*base, col("shift"), col("seed", np.uint64))
+    return fn(*base, col("seed", np.uint64))
+
+
+def _fixtures(model):
+    out = []
+    for c in GOLDEN["mc_cases"]:
+        if c["model"] == model:
+            out.append((_args(c["args"]), float.fromhex(c["price"])))
+    return out
+
+
+@pytest.mark.parametrize("model", [QK_MC_QMC_SOBOL, QK_MC_QMC_HALTON])
+def test_qmc_equals_reference(qk, model):
+    cases = _fixtures(model)
+    assert len(cases) >= 20
+    got = _gpu(qk, model, [a for a, _ in cases])
+    worst = 0.0
+    for (a, want), g in zip(cases, got):
+        if math.isnan(want):
+            assert math.isnan(g), a
+            continue
+        err = abs(g - want) / max(1.0, abs(want))
+        worst = max(worst, err)
+        assert err < 1e-10, (a, g, want)
+    print(f"model {model}: worst relative difference {worst:.2e} over {len(cases)} cases")
+
+
+@pytest.mark.parametrize("model", VR)
+def test_entry_checks_exact(qk, model):
+    """NaN / intrinsic results of the reference's entry checks, bit for bit."""
+    cases = [(a, w) for a, w in _fixtures(model) if math.isnan(w) or a["t"] <= 1e-12]
+    assert len(cases) >= 4
+    got = _gpu(qk, model, [a for a, _ in cases])
+    for (a, want), g in zip(cases, got):
+        assert (math.isnan(g) and math.isnan(want)) or g == want, (a, g, want)
+
+
+@pytest.mark.parametrize("model", [QK_MC_CONTROL_VARIATES, QK_MC_IMPORTANCE_SAMPLING,
+                                   QK_MC_STRATIFIED])
+def test_same_stream_replay(qk, oracle, model):
+    """GPU vs the oracle's FP64 replay of the GPU's own Philox stream."""
+    rng = np.random.default_rng(300 + model)
+    cases = []
+    for _ in range(24):
+        cases.append(dict(spot=float(rng.uniform(80, 120)), strike=float(rng.uniform(80, 120)),
+                          t=float(rng.uniform(0.1, 2)), vol=float(rng.uniform(0.1, 0.5)),
+                          r=float(rng.uniform(0, 0.05)), q=float(rng.uniform(0, 0.03)),
+                          option_type=int(rng.integers(0, 2)), paths=int(rng.integers(3, 5000)),
+                          seed=int(rng.integers(0, 2**63)), shift=float(rng.uniform(-0.8, 0.8))))
+    got, gse = _gpu(qk, model, cases, se=True)
+    for c, g, s in zip(cases, got, gse):
+        want, wse = oracle.philox_vr_price(model, **c)
+        if model == QK_MC_STRATIFIED:
+            assert abs(g - want) <= 1e-12 * max(1.0, abs(want)), (c, g, want)
+            assert abs(s - wse) <= 1e-9 * max(1e-3, wse), (c, s, wse)
+        else:
+            tol = 5e-5 * c["spot"] + 0.02 * wse
+            assert abs(g - want) <= tol, (c, g, want, tol)
+            assert abs(s - wse) <= 0.02 * wse + 1e-9, (c, s, wse)
+
+
+@pytest.mark.parametrize("model", [QK_MC_CONTROL_VARIATES, QK_MC_IMPORTANCE_SAMPLING,
+                                   QK_MC_STRATIFIED])
+def test_vs_reference_cpu_mc(qk, oracle, model):
+    b = workloads.bsm_terminal(48, paths=20000, seed=60 + model)
+    cases = [dict(spot=float(b["spot"][i]), strike=float(b["strike"][i]), t=float(b["t"][i]),
+                  vol=float(b["vol"][i]), r=float(b["r"][i]), q=float(b["q"][i]),
+                  option_type=int(b["option_type"][i]), paths=int(b["paths"][i]),
+                  seed=int(b["seed"][i]), shift=0.3 * (i % 3)) for i in range(48)]
+    p, se = _gpu(qk, model, cases, se=True)
+    ref = [oracle.price(model, **c) for c in cases]
+    rp = np.array([x for x, _ in ref])
+    rse = np.array([s for _, s in ref])
+    check_z(z_scores(p, rp, np.hypot(se, rse)), f"model {model} GPU vs reference CPU MC")
+
+
+@pytest.mark.parametrize("model", VR)
+def test_vs_bsm_closed_form(qk, oracle, model):
+    b = workloads.bsm_terminal(32, paths=1 << 20, seed=70 + model)
+    cases = [dict(spot=float(b["spot"][i]), strike=float(b["strike"][i]), t=float(b["t"][i]),
+                  vol=float(b["vol"][i]), r=float(b["r"][i]), q=float(b["q"][i]),
+                  option_type=int(b["option_type"][i]), paths=int(b["paths"][i]),
+                  seed=int(b["seed"][i]), shift=0.25) for i in range(32)]
+    p, se = _gpu(qk, model, cases, se=True)
+    cf = np.array([oracle.bsm(c["spot"], c["strike"], c["t"], c["vol"], c["r"], c["q"],
+                              c["option_type"]) for c in cases])
+    if model in (QK_MC_QMC_SOBOL, QK_MC_QMC_HALTON):
+        # deterministic points: the error is the quadrature error, ~1/n
+        err = np.abs(p - cf)
+        print(f"model {model}: max |QMC - BSM| = {err.max():.2e} at 2^20 points")
+        assert err.max() < 2e-3
+    else:
+        if model == QK_MC_STRATIFIED:
+            # at 2^20 strata the standard error (~1e-8 x S) nears the bias of
+            # Acklam's inverse normal (relative error 1.15e-9), which the
+            # reference shares: floor the SE at 1e-9 x S
+            se = np.hypot(se, 1e-9 * np.array([c["spot"] for c in cases]))
+        check_z(z_scores(p, cf, se), f"model {model} GPU vs BSM closed form")
+
+
+def test_reference_python_cases(qk, oracle):
+    """python/tests/test_monte_carlo_api.py:8-58 of the reference, on the GPU."""
+    common = dict(spot=100.0, strike=100.0, t=1.0, vol=0.2, r=0.03, q=0.01, option_type=0)
+    prices = [qk.quasi_monte_carlo_sobol_price(**common, paths=16384),
+              qk.quasi_monte_carlo_halton_price(**common, paths=16384),
+              qk.importance_sampling_price(**common, paths=30000, shift=0.4, seed=7),
+              qk.control_variates_price(**common, paths=30000, seed=7),
+              qk.stratified_sampling_price(**common, paths=30000, seed=7)]
+    assert all(math.isfinite(p) and p > 0.0 for p in prices)
+    bsm = oracle.bsm(**common)
+    assert abs(qk.control_variates_price(**common, paths=60000, seed=11) - bsm) < 0.4
+    assert abs(qk.stratified_sampling_price(**common, paths=60000, seed=11) - bsm) < 0.4
+    assert abs(prices[0] - prices[1]) < 0.75
+
+
+def test_variance_is_reduced(qk):
+    """At equal paths the estimators' standard errors beat independent paths."""
+    n = 16
+    b = workloads.bsm_terminal(n, paths=65536, seed=80)
+    b["strike"] = b["spot"].copy()  # at the money
+    plan = qk.plan(model=np.full(n, 5, np.int32), **b)
+    plan.execute()
+    _, se_plain = plan.results()
+    plan.close()
+    _, se_cv = qk.control_variates_price_se_batch(**b)
+    _, se_st = qk.stratified_sampling_price_se_batch(**b)
+    print("SE ratio vs plain: control variates", np.round(se_cv / se_plain, 3).mean(),
+          "stratified", np.round(se_st / se_plain, 4).mean())
+    # S_T correlates with a call payoff more than with a put's: a bound per
+    # option and one on the mean ratio (observed 0.52)
+    assert np.all(se_cv < se_plain) and (se_cv / se_plain).mean() < 0.7
+    assert np.all(se_st < 0.05 * se_plain)
+
+
+@pytest.mark.parametrize("model", VR)
+def test_batch_equals_scalar_and_plans(qk, model):
+    rng = np.random.default_rng(90 + model)
+    n = 12
+    cases = [dict(spot=float(rng.uniform(90, 110)), strike=float(rng.uniform(90, 110)),
+                  t=float(rng.uniform(0.25, 1)), vol=float(rng.uniform(0.15, 0.4)),
+                  r=float(rng.uniform(0.01, 0.05)), q=float(rng.uniform(0, 0.02)),
+                  option_type=i & 1, paths=1024 + 37 * i, seed=42 + i,
+                  shift=float(rng.uniform(0.1, 0.5))) for i in range(n)]
+    batch = _gpu(qk, model, cases)
+    scalar_fn = getattr(qk, NAMES[model] + "_price")
+    for c, bv in zip(cases, batch):
+        kw = {k: c[k] for k in ("spot", "strike", "t", "vol", "r", "q", "option_type", "paths")}
+        if model == QK_MC_IMPORTANCE_SAMPLING:
+            kw["shift"] = c["shift"]
+        if model not in (QK_MC_QMC_SOBOL, QK_MC_QMC_HALTON):
+            kw["seed"] = c["seed"]
+        assert scalar_fn(**kw) == bv
+    # a plan (graph replay) and the persistent mixed kernel give the same bits
+    arr = {k: np.array([c[k] for c in cases]) for k in ("spot", "strike", "t", "vol", "r", "q")}
+    arr.update(option_type=np.array([c["option_type"] for c in cases], np.int32),
+               paths=np.array([c["paths"] for c in cases], np.int32),
+               seed=np.array([c["seed"] for c in cases], np.uint64),
+               v0=np.array([c["shift"] for c in cases]))
+    for flags in (QK_PLAN_GRAPH, QK_PLAN_PERSISTENT):
+        plan = qk.plan(model=np.full(n, model, np.int32), flags=flags, **arr)
+        plan.execute()
+        plan.execute()
+        got, _ = plan.results()
+        plan.close()
+        assert np.array_equal(got, batch), flags
+
+
+def test_mixed_batch_with_all_models(qk):
+    """All thirteen models in one persistent launch equal their uniform batches."""
+    b = workloads.mixed(n=130, seed=5)
+    model = (np.arange(130) % 13).astype(np.int32)
+    b["model"] = model
+    b["paths"] = np.minimum(b["paths"], 1 << 14).astype(np.int32)
+    b["steps"] = np.minimum(b["steps"], 64).astype(np.int32)
+    # Heston-family rows take the Heston parameters; the LR delta's clip is `vol`
+    b["vol"] = np.where(model == 7, 4.0, b["vol"])
+    b["v0"] = np.where(model == QK_MC_IMPORTANCE_SAMPLING, 0.3, b["v0"])
+    mixed, _ = qk.mixed_price_batch(**b)
+    for m in range(13):
+        idx = np.nonzero(model == m)[0]
+        plan = qk.plan(**{k: v[idx] for k, v in b.items()})
+        plan.execute()
+        want, _ = plan.results()
+        plan.close()
+        assert np.array_equal(mixed[idx], want), m
+    assert np.all(np.isfinite(mixed))
