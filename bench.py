@@ -72,6 +72,8 @@ def parse():
     ap.add_argument("--heston-cf", action="store_true",
                     help="Heston characteristic-function leg only")
     ap.add_argument("--cf-options", type=int, default=65536)
+    ap.add_argument("--vr", action="store_true",
+                    help="variance-reduction leg only (device + e2e; no CPU with --profile)")
     ap.add_argument("--sur-train-n", type=int, default=4_000_000)
     ap.add_argument("--sur-hold-n", type=int, default=100_000)
     ap.add_argument("--sur-epochs", type=int, default=60)
@@ -125,11 +127,54 @@ def _cf_cpu_leg(s):
     print(json.dumps({"options": n, "seconds": dt}))
 
 
+VR_METHODS = {8: "control_variates", 9: "importance_sampling", 10: "stratified_sampling",
+              11: "quasi_monte_carlo_sobol", 12: "quasi_monte_carlo_halton"}
+
+
+def _vr_batch(n=64, paths=1 << 20):
+    from quantkernel_b200 import workloads
+
+    b = workloads.bsm_terminal(n, paths=paths, seed=11)
+    b["shift"] = np.full(n, 0.25)
+    return b
+
+
+def _vr_cpu_leg(s):
+    """The reference's OpenMP batch of each variance-reduction method on the
+    64-option workload with paths scaled to about s["seconds"] per method."""
+    from oracle import oracle as orc
+
+    lib = orc.Reference() if s["impl"] == "reference" else None
+    out = {}
+    for m, name in VR_METHODS.items():
+        paths = 1024
+        while True:
+            b = _vr_batch(paths=paths)
+            t0 = time.perf_counter()
+            if lib is not None:
+                lib.vr_batch(m, b["spot"], b["strike"], b["t"], b["vol"], b["r"], b["q"],
+                             b["option_type"], b["paths"], seed=b["seed"], shift=b["shift"])
+            else:
+                o = orc.Oracle()
+                for i in range(64):
+                    o.price(m, b["spot"][i], b["strike"][i], b["t"][i], b["vol"][i], b["r"][i],
+                            b["q"][i], int(b["option_type"][i]), int(b["paths"][i]),
+                            seed=int(b["seed"][i]), shift=float(b["shift"][i]))
+            dt = time.perf_counter() - t0
+            if dt >= 0.5 * s["seconds"] or paths >= (1 << 20):
+                break
+            paths = min(1 << 20, max(2 * paths, int(paths * s["seconds"] / max(dt, 1e-3))))
+        out[name] = {"paths_per_option": paths, "seconds": dt, "paths_per_s": 64 * paths / dt}
+    print(json.dumps(out))
+
+
 def cpu_leg(spec):
     """Runs in a subprocess with OMP_NUM_THREADS set; prints one JSON line."""
     s = json.loads(spec)
     if s.get("kind") == "heston_cf":
         return _cf_cpu_leg(s)
+    if s.get("kind") == "vr":
+        return _vr_cpu_leg(s)
     target = s["seconds"]
     reps = s.get("reps", 1)
     n_opt, paths = 8, 4096
@@ -308,6 +353,7 @@ def main_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     total_ms = float(t.item())
     prices, se = plan.results()
+    plan_cfg = plan.config()
     assert np.all(np.isfinite(prices)) and np.all(se > 0), "non-finite result"
     launches = plan.stats()["launches"] * args.steps
     if args.profile:
@@ -352,11 +398,10 @@ def main_gpu(args):
         "unit": "Gop/s",
         "frac": achieved / bound_units,
         "traffic": None,
-        "kernel": "mc_simulate_kernel<Heston,256,2,antithetic>",
+        "kernel": "mc_simulate_kernel<Heston,{block},{units_per_thread},antithetic>".format(
+            **plan_cfg),
         "kernel_ms": sim_ms,
-        "measured": {"thread_instructions_per_path_step": 27.9, "xu_per_path_step": 3,
-                     "issue_busy": 0.705, "xu_pipe_busy": 0.607,
-                     "source": "ncu, profiles/heston_simulate_ncu.md"},
+        "measured": {"source": "ncu, profiles/heston_simulate_ncu.md"},
         "note": ("frac > 1: the reference formulas cost 6 XU + 50 ALU per path-step; this "
                  "kernel needs 3 XU + ~25 (antithetic pairs share normals, log-space spot "
                  "drops the per-step exp)"),
@@ -372,6 +417,10 @@ def main_gpu(args):
         for line in prof.read_text().splitlines():
             if line.startswith("dram_bytes_per_launch_full:"):
                 roofline["traffic"] = int(line.split(":")[1]) * n_opt // N_OPT
+            for key in ("thread_instructions_per_path_step", "xu_per_path_step", "issue_busy",
+                        "xu_pipe_busy"):
+                if line.startswith(key + ":"):
+                    roofline["measured"][key] = float(line.split(":")[1])
 
     threads = host_threads()
     try:
@@ -389,6 +438,7 @@ def main_gpu(args):
         extras["mixed"] = mixed_leg(qk)
         extras["bsm_terminal"] = bsm_terminal_leg(qk)
         extras["heston_cf"] = heston_cf_leg(qk)
+        extras["variance_reduction"] = vr_leg(qk)
         if Path(args.sur_checkpoint).exists():
             extras["surrogate"] = surrogate_infer_leg(qk, args.sur_checkpoint,
                                                       mc_prices_per_s=value / (PATHS * STEPS))
@@ -588,23 +638,29 @@ def _time_plan(plan, stream, flush, reps):
 
 def mixed_leg(qk, reps=5):
     """Uneven batch: 4096 options, BSM-Euler / Milstein / local vol / Heston
-    1:1:1:1, paths log-uniform 2^12..2^20, steps 16..512: one persistent
-    work-stealing launch in a CUDA graph (autotuned), against one grid launch
-    per model back to back."""
+    1:1:1:1, paths log-uniform 2^12..2^20, steps 16..512, as one plan in a
+    CUDA graph: the persistent work-stealing kernel, per-family grids, and the
+    autotuner's choice between them; against one plan per model back to back."""
     import torch
 
-    from quantkernel_b200 import (QK_PLAN_AUTOTUNE, QK_PLAN_GRAPH, QK_PLAN_PERSISTENT,
-                                  QK_PLAN_TIMING, workloads)
+    from quantkernel_b200 import (QK_PLAN_AUTOTUNE, QK_PLAN_FAMILY_GRIDS, QK_PLAN_GRAPH,
+                                  QK_PLAN_PERSISTENT, QK_PLAN_TIMING, workloads)
 
     b = workloads.mixed()
     units = workloads.path_steps(b)
     stream = torch.cuda.current_stream()
     assert stream.cuda_stream != 0, "time on a non-default stream"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    plan = qk.plan(**b, flags=QK_PLAN_PERSISTENT | QK_PLAN_GRAPH | QK_PLAN_AUTOTUNE | QK_PLAN_TIMING)
+    plan = qk.plan(**b, flags=QK_PLAN_PERSISTENT | QK_PLAN_GRAPH | QK_PLAN_TIMING)
+    ms_pers = _time_plan(plan, stream, flush, reps)
+    p_pers, _ = plan.results()
+    plan.close()
+    plan = qk.plan(**b, flags=QK_PLAN_FAMILY_GRIDS | QK_PLAN_GRAPH | QK_PLAN_TIMING)
+    ms_grids = _time_plan(plan, stream, flush, reps)
+    plan.close()
+    plan = qk.plan(**b, flags=QK_PLAN_GRAPH | QK_PLAN_AUTOTUNE | QK_PLAN_TIMING)
     ms = _time_plan(plan, stream, flush, reps)
     cfg = plan.config()
-    p_pers, _ = plan.results()
     plan.close()
     per_model = 0.0
     out = np.empty(len(b["model"]))
@@ -617,9 +673,12 @@ def mixed_leg(qk, reps=5):
     assert np.allclose(out, p_pers, rtol=1e-12, atol=0)
     return {"workload": "4096 options, Euler/Milstein/local-vol/Heston 1:1:1:1, paths 2^U[12,20], "
                         "steps 2^U[4,9]", "path_steps": units,
-            "persistent_graph_ms": ms, "path_steps_per_s": units / (ms / 1e3),
-            "per_model_grid_ms": per_model, "speedup_vs_per_model": per_model / ms,
-            "launch_config": cfg}
+            "autotuned_graph_ms": ms, "path_steps_per_s": units / (ms / 1e3),
+            "persistent_graph_ms": ms_pers, "family_grids_graph_ms": ms_grids,
+            "per_model_plans_ms": per_model, "speedup_vs_per_model": per_model / ms,
+            "launch_config": cfg,
+            "launch_config_note": "units_per_thread 0 = persistent kernel, -1 = one grid per "
+                                  "family group"}
 
 
 def bsm_terminal_leg(qk, reps=20):
@@ -643,6 +702,55 @@ def bsm_terminal_leg(qk, reps=20):
     return {"workload": "64 BSM calls/puts x 131072 paths (terminal, antithetic)",
             "ms": ms, "paths_per_s": paths / (ms / 1e3), "e2e_ms": 1e3 * e2e,
             "e2e_paths_per_s": paths / e2e}
+
+
+def vr_leg(qk, reps=5, cpu=True):
+    """64 BSM calls/puts x 2^20 paths for each terminal variance-reduction
+    estimator: device time of a graph-replayed plan (L2 flushed), end to end
+    through the drop-in batch call, and the reference's OpenMP batch on a
+    bounded sample."""
+    import torch
+
+    from quantkernel_b200 import QK_PLAN_GRAPH, QK_PLAN_TIMING
+
+    b = _vr_batch()
+    n = len(b["spot"])
+    paths = int(b["paths"].sum())
+    stream = torch.cuda.current_stream()
+    assert stream.cuda_stream != 0, "time on a non-default stream"
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    res = {"workload": f"{n} BSM calls/puts x 2^20 paths, shift 0.25 (importance sampling)"}
+    for m, name in VR_METHODS.items():
+        arr = {k: b[k] for k in ("spot", "strike", "t", "vol", "r", "q", "option_type", "paths",
+                                 "seed")}
+        plan = qk.plan(model=np.full(n, m, np.int32), v0=b["shift"],
+                       flags=QK_PLAN_GRAPH | QK_PLAN_TIMING, **arr)
+        ms = _time_plan(plan, stream, flush, reps)
+        plan.close()
+        fn = getattr(qk, name + "_price_batch")
+        args = [b[k] for k in ("spot", "strike", "t", "vol", "r", "q", "option_type", "paths")]
+        if m == 9:
+            args.append(b["shift"])
+        if m not in (11, 12):
+            args.append(b["seed"])
+        fn(*args)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn(*args)
+        e2e = (time.perf_counter() - t0) / reps
+        res[name] = {"ms": ms, "paths_per_s": paths / (ms / 1e3), "e2e_ms": 1e3 * e2e,
+                     "e2e_paths_per_s": paths / e2e}
+    if cpu:
+        try:
+            threads = host_threads()
+            c = run_cpu(cpu_kind(), threads, seconds=2.0, kind="vr")
+            for name, v in c.items():
+                res[name]["cpu_baseline"] = {"paths_per_s": v["paths_per_s"], "cores": threads,
+                                             "kind": cpu_kind(),
+                                             "sample": f"64 options x {v['paths_per_option']} paths"}
+        except Exception as exc:
+            res["cpu_baseline_error"] = f"{exc}"[:200]
+    return res
 
 
 def heston_cf_leg(qk, reps=5, n=65536, cpu=True):
@@ -689,6 +797,15 @@ def main():
         return 0
     if args.cpu_leg:
         cpu_leg(args.cpu_leg)
+        return 0
+    if args.vr:
+        import torch
+
+        from quantkernel_b200 import QuantKernel
+
+        torch.cuda.set_stream(torch.cuda.Stream())
+        leg = vr_leg(QuantKernel(), cpu=not args.profile)
+        print(json.dumps({"leg": "variance_reduction", **leg}), flush=True)
         return 0
     if args.heston_cf:
         from quantkernel_b200 import QuantKernel

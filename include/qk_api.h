@@ -215,7 +215,12 @@ QK_EXPORT int32_t qk_get_device(int32_t* device);
 #define QK_PLAN_GRAPH         0x2 /* replay execute() from a captured CUDA graph */
 #define QK_PLAN_NO_ANTITHETIC 0x4 /* stepwise models: independent paths, not pairs */
 #define QK_PLAN_TIMING        0x8 /* record CUDA events around the simulate kernel */
-#define QK_PLAN_AUTOTUNE      0x10 /* choose block size / units per thread by timing */
+#define QK_PLAN_AUTOTUNE      0x10 /* choose block size / units per thread by timing; for
+                                      * batches of several model families also the mode:
+                                      * one persistent kernel or one grid per family (the
+                                      * latter not when QK_PLAN_PERSISTENT is given) */
+#define QK_PLAN_FAMILY_GRIDS  0x20 /* several model families: one grid per family group,
+                                      * back to back, instead of the persistent kernel */
 
 /* Price + standard error batches.  Same inputs as the Part 1 batch calls;
  * out_stderr[i] is the standard error of out_prices[i] (NaN where no
@@ -336,7 +341,9 @@ QK_EXPORT int32_t qk_mcm_plan_device_results(qk_mc_plan* plan, double** d_prices
  * the number of kernels one execute() launches. */
 QK_EXPORT int32_t qk_mcm_plan_stats(qk_mc_plan* plan, double* simulate_ms, int32_t* launches,
                                     int64_t* path_steps);
-/* The launch shape in use: block size, units per thread, persistent CTAs. */
+/* The launch shape in use: block size; units per thread (> 0: one
+ * single-family grid; 0: the persistent kernel; -1: one grid per family
+ * group); CTAs of the persistent kernel. */
 QK_EXPORT int32_t qk_mcm_plan_config(qk_mc_plan* plan, int32_t* block, int32_t* units_per_thread,
                                      int32_t* ctas);
 QK_EXPORT int32_t qk_mcm_plan_destroy(qk_mc_plan* plan);

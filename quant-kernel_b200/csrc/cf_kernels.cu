@@ -92,8 +92,9 @@ __device__ __forceinline__ Cx csqrt_(Cx a) {
 
 struct HestonCf {
     double kappa, theta_k_s2, rho_sigma, sigma2, inv_sigma2, v0, t, drift;
-    // heston.cpp:33-44
-    __device__ Cx operator()(Cx u) const {
+    // heston.cpp:33-44.  Not inlined: the body is large and is called at three
+    // places; one copy keeps the kernel inside the instruction cache.
+    __device__ __noinline__ Cx operator()(Cx u) const {
         const Cx iu = cx(-u.im, u.re);
         const Cx beta = cx(kappa, 0.0) - rho_sigma * iu;
         const Cx d = csqrt_(beta * beta + sigma2 * (iu + u * u));

@@ -31,8 +31,9 @@ struct SimArgs {
     const int64_t* tile_begin; // device, n + 1 entries
     int32_t n;
     int64_t n_tiles;
-    TilePartial* partials;     // device, n_tiles slots
+    TilePartial* partials;     // device, indexed by absolute tile
     int32_t max_ctas;          // grid cap (grid-stride beyond it)
+    int64_t tile0 = 0;         // absolute index of this launch's first tile
 };
 
 int family_of(int32_t model);
@@ -41,9 +42,10 @@ cudaError_t launch_simulate(int family, bool anti, int block, int upt, const Sim
                             cudaStream_t st);
 cudaError_t launch_persistent(int block, const SimArgs& a, unsigned long long* work_counter,
                               cudaStream_t st);
+// out_index (nullable): record k's results go to slot out_index[k].
 cudaError_t launch_finalize(const McOption* opts, int32_t n, const TilePartial* partials,
-                            double* out_price, double* out_se, unsigned long long* work_counter,
-                            cudaStream_t st);
+                            double* out_price, double* out_se, const int32_t* out_index,
+                            unsigned long long* work_counter, cudaStream_t st);
 // Resident CTAs on `device` for a family kernel (family >= 0) or the
 // persistent kernel (family < 0); 0 on error.
 int max_resident_ctas(int family_or_persistent, int block, int upt, int device);

@@ -129,7 +129,7 @@ NoAllocStatus noalloc_heston_batch(const BatchInput& in, double* out_prices, dou
         a.max_ctas = 0x7fffffff;
         e = launch_simulate(kFamHeston, true, kBlock, kUpt, a, 0);
     }
-    if (e == cudaSuccess) e = launch_finalize(d_rec, in.n, d_part, d_price, d_se, nullptr, 0);
+    if (e == cudaSuccess) e = launch_finalize(d_rec, in.n, d_part, d_price, d_se, nullptr, nullptr, 0);
     if (e == cudaSuccess)
         e = cudaMemcpy(out_prices, d_price, sizeof(double) * in.n, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && out_stderr)

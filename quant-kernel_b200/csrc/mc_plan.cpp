@@ -32,6 +32,8 @@ namespace {
 
 constexpr double kEps = 1e-12;
 constexpr int64_t kMaxTilesPerOption = 4096;
+constexpr int64_t kTerminalItersPerThread = 4;
+constexpr int64_t kMinTerminalTiles = 32;
 
 double nan_value() { return std::numeric_limits<double>::quiet_NaN(); }
 
@@ -264,6 +266,18 @@ int32_t tile_option(McOption& o, int block, int upt) {
     const int64_t units = o.units;
     int64_t iters = (units + per_iter * kMaxTilesPerOption - 1) / (per_iter * kMaxTilesPerOption);
     if (iters < 1) iters = 1;
+    // Terminal units (one quad of paths, no time steps) are cheap next to a
+    // tile's fixed cost -- record load, option search and the double-double
+    // CTA reduction -- so large terminal options give each thread several
+    // units, while keeping at least kMinTerminalTiles tiles to spread over
+    // the SMs.  A function of the option alone, like the rest of the
+    // geometry: a batch and a scalar call tile an option the same way.
+    const int fam = family_of(o.model);
+    if (fam == kFamTerminal || fam == kFamVr) {
+        const int64_t cap = units / (per_iter * kMinTerminalTiles);
+        const int64_t want = std::min<int64_t>(kTerminalItersPerThread, cap);
+        if (want > iters) iters = want;
+    }
     const int64_t tile_units = per_iter * iters;
     o.unit_iters = (int32_t)iters;
     o.tiles = (int32_t)((units + tile_units - 1) / tile_units);
@@ -310,9 +324,15 @@ void PinnedBuf::release() {
 
 // ----------------------------------------------------------------------------
 // Default launch shapes (measured on B200; the autotuner may override them).
+// 128-thread CTAs: at the Heston benchmark (1024 options x 262144 paths x 200
+// steps) block 128 ran 2.4% faster than 256 with the same registers (six CTAs
+// of 128 per SM instead of three of 256: finer tiles, a shorter tail), and the
+// autotuner picked it for the mixed-model batch too.  One block size for every
+// family keeps the persistent and single-family tilings identical, so both
+// give the same bits.
 LaunchConfig default_config(int family) {
     LaunchConfig c;
-    c.block = 256;
+    c.block = 128;
     c.upt = (family == kFamTerminal || family == kFamVr) ? 1 : 2;
     return c;
 }
@@ -341,7 +361,8 @@ void load_tune_file_locked() {
     int block = 0, upt = 0;
     // one entry per line: <key> <block> <upt>
     while (std::fscanf(f, "%511s %d %d", key, &block, &upt) == 3) {
-        if ((block == 128 || block == 256) && (upt == 1 || upt == 2 || upt == 4))
+        if ((block == 128 || block == 256) &&
+            (upt == 1 || upt == 2 || upt == 4 || upt == kUptPersistent || upt == kUptFamilyGrids))
             tune_map()[key] = LaunchConfig{block, upt};
     }
     std::fclose(f);
@@ -383,6 +404,8 @@ cudaError_t Plan::release() {
         d_price_.release();
         d_se_.release();
         d_counter_.release();
+        d_out_index_.release();
+        h_out_index_.release();
         h_opts_.release();
         h_tile_begin_.release();
         h_price_.release();
@@ -449,7 +472,9 @@ cudaError_t Plan::build(const BatchInput& in, int32_t flags, std::string* err) {
     anti_ = anti;
     persistent_ = (fam == -1) || (flags & kFlagPersistent);
     if (persistent_) {
-        cfg_ = LaunchConfig{256, 0};
+        const bool grids = (flags & kFlagFamilyGrids) && !(flags & kFlagPersistent);
+        cfg_ = LaunchConfig{default_config(kFamHeston).block,
+                            grids ? kUptFamilyGrids : kUptPersistent};
     } else {
         cfg_ = default_config(family_);
     }
@@ -458,33 +483,85 @@ cudaError_t Plan::build(const BatchInput& in, int32_t flags, std::string* err) {
     LaunchConfig tuned;
     if (tuned_config(key, &tuned)) {
         cfg_.block = tuned.block;
-        if (!persistent_) cfg_.upt = tuned.upt;
+        // a multi-family plan takes the tuned mode unless the caller asked
+        // for the persistent kernel explicitly
+        if (!persistent_ || (tuned.upt <= 0 && !(flags & (kFlagPersistent | kFlagFamilyGrids))))
+            cfg_.upt = tuned.upt;
+        if (persistent_ && cfg_.upt > 0) cfg_.upt = kUptPersistent;
     }
     e = layout_tiles(cfg_);
     if (e != cudaSuccess) return e;
     if ((flags & kFlagAutotune) && n_tiles_ > 0) {
         e = autotune();
         if (e != cudaSuccess) return e;
-        LaunchConfig store = cfg_;
-        if (persistent_) store.upt = 1;
-        store_tuned_config(key, store);
+        store_tuned_config(key, cfg_);
     }
     (void)err;
     return cudaSuccess;
 }
 
+// Work order of the persistent kernel: heavy families first, and within a
+// family the costliest tiles first, so that the last tiles handed out are
+// short ones (a small tail) and co-resident CTAs mostly run the same code.
+static int family_rank(int fam) {
+    switch (fam) {
+        case kFamHeston:
+        case kFamHestonLr: return 0;
+        case kFamMilstein: return 1;
+        case kFamEuler: return 2;
+        case kFamVr: return 3;
+        default: return 4;  // terminal
+    }
+}
+
 cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
     const int32_t n = n_;
-    int64_t total = 0;
-    std::vector<int64_t> begin((size_t)n + 1);
+    // tile geometry per option (independent of the order)
     for (int32_t i = 0; i < n; ++i) {
         McOption& o = opts_[(size_t)i];
-        begin[(size_t)i] = total;
+        tile_option(o, cfg.block, upt_for(family_of(o.model), persistent_, cfg));
+    }
+    order_.resize((size_t)n);
+    for (int32_t i = 0; i < n; ++i) order_[(size_t)i] = i;
+    if (persistent_) {
+        auto tile_cost = [&](const McOption& o) {
+            return (double)o.unit_iters * (double)std::max(o.steps, 1);
+        };
+        std::stable_sort(order_.begin(), order_.end(), [&](int32_t a, int32_t b) {
+            const McOption& oa = opts_[(size_t)a];
+            const McOption& ob = opts_[(size_t)b];
+            const int ra = family_rank(family_of(oa.model)), rb = family_rank(family_of(ob.model));
+            if (ra != rb) return ra < rb;
+            const int fa = family_of(oa.model), fb = family_of(ob.model);
+            if (fa != fb) return fa < fb;  // Heston before its LR-delta variant
+            if (oa.antithetic != ob.antithetic) return oa.antithetic > ob.antithetic;
+            return tile_cost(oa) > tile_cost(ob);
+        });
+    }
+    int64_t total = 0;
+    std::vector<int64_t> begin((size_t)n + 1);
+    for (int32_t k = 0; k < n; ++k) {
+        McOption& o = opts_[(size_t)order_[(size_t)k]];
+        begin[(size_t)k] = total;
         o.tile_begin = total;
-        total += tile_option(o, cfg.block, upt_for(family_of(o.model), persistent_, cfg));
+        total += o.tiles;
     }
     begin[(size_t)n] = total;
     n_tiles_ = total;
+    groups_.clear();
+    if (persistent_) {
+        for (int32_t k = 0; k < n; ++k) {
+            const McOption& o = opts_[(size_t)order_[(size_t)k]];
+            if (o.tiles <= 0) continue;  // constant results: finalize only
+            const int fam = family_of(o.model);
+            const bool anti = o.antithetic != 0;
+            if (groups_.empty() || groups_.back().family != fam || groups_.back().anti != anti ||
+                groups_.back().opt_hi != k)
+                groups_.push_back(Group{fam, anti, k, k, o.tile_begin, o.tile_begin});
+            groups_.back().opt_hi = k + 1;
+            groups_.back().tile_hi = o.tile_begin + o.tiles;
+        }
+    }
 
     cudaError_t e;
     const size_t opt_bytes = sizeof(McOption) * (size_t)std::max(n, 1);
@@ -497,15 +574,27 @@ cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
     if ((e = d_counter_.ensure(sizeof(unsigned long long))) != cudaSuccess) return e;
     if ((e = h_opts_.ensure(opt_bytes)) != cudaSuccess) return e;
     if ((e = h_tile_begin_.ensure(tb_bytes)) != cudaSuccess) return e;
+    const size_t ix_bytes = sizeof(int32_t) * (size_t)std::max(n, 1);
+    if (persistent_) {
+        if ((e = d_out_index_.ensure(ix_bytes)) != cudaSuccess) return e;
+        if ((e = h_out_index_.ensure(ix_bytes)) != cudaSuccess) return e;
+    }
     // The previous upload from these staging buffers may still be in flight.
     if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return e;
-    std::memcpy(h_opts_.p, opts_.data(), sizeof(McOption) * (size_t)n);
+    McOption* h_rec = static_cast<McOption*>(h_opts_.p);
+    for (int32_t k = 0; k < n; ++k) h_rec[k] = opts_[(size_t)order_[(size_t)k]];
     std::memcpy(h_tile_begin_.p, begin.data(), tb_bytes);
+    if (persistent_) {
+        std::memcpy(h_out_index_.p, order_.data(), sizeof(int32_t) * (size_t)n);
+        if ((e = cudaMemcpyAsync(d_out_index_.p, h_out_index_.p, sizeof(int32_t) * (size_t)n,
+                                 cudaMemcpyHostToDevice, stream_)) != cudaSuccess)
+            return e;
+    }
     if ((e = cudaMemcpyAsync(d_opts_.p, h_opts_.p, sizeof(McOption) * (size_t)n, cudaMemcpyHostToDevice, stream_)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(d_tile_begin_.p, h_tile_begin_.p, tb_bytes, cudaMemcpyHostToDevice, stream_)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(d_counter_.p, 0, sizeof(unsigned long long), stream_)) != cudaSuccess) return e;
     counter_ready_ = true;
-    if (persistent_) {
+    if (persistent_ && cfg.upt == kUptPersistent) {
         max_ctas_ = max_resident_ctas(-1, cfg.block, 0, device_);
         if (max_ctas_ <= 0) return cudaErrorInvalidConfiguration;
     } else {
@@ -526,15 +615,34 @@ cudaError_t Plan::launch_all(cudaStream_t st, bool timing) {
     unsigned long long* counter = static_cast<unsigned long long*>(d_counter_.p);
     cudaError_t e = cudaSuccess;
     if (timing && (e = cudaEventRecord(ev0_, st)) != cudaSuccess) return e;
+    const bool use_counter = persistent_ && cfg_.upt == kUptPersistent;
     if (n_tiles_ > 0) {
-        if (persistent_)
+        if (use_counter) {
             e = launch_persistent(cfg_.block, a, counter, st);
-        else
+        } else if (persistent_) {
+            // one grid per (family, antithetic) group, back to back
+            for (const Group& g : groups_) {
+                SimArgs ga = a;
+                ga.opts = a.opts + g.opt_lo;
+                ga.tile_begin = a.tile_begin + g.opt_lo;
+                ga.n = g.opt_hi - g.opt_lo;
+                ga.tile0 = g.tile_lo;
+                ga.n_tiles = g.tile_hi - g.tile_lo;
+                e = launch_simulate(g.family, g.anti, cfg_.block,
+                                    upt_for(g.family, true, cfg_), ga, st);
+                if (e != cudaSuccess) return e;
+            }
+        } else {
             e = launch_simulate(family_, anti_, cfg_.block, cfg_.upt, a, st);
+        }
         if (e != cudaSuccess) return e;
     }
     if (timing && (e = cudaEventRecord(ev1_, st)) != cudaSuccess) return e;
-    return launch_finalize(a.opts, n_, a.partials, d_price(), d_se(), persistent_ ? counter : nullptr, st);
+    // persistent plans hold the records in work order; the finalize kernel
+    // scatters results back to the caller's order
+    const int32_t* out_index = persistent_ ? static_cast<const int32_t*>(d_out_index_.p) : nullptr;
+    return launch_finalize(a.opts, n_, a.partials, d_price(), d_se(), out_index,
+                           use_counter ? counter : nullptr, st);
 }
 
 cudaError_t Plan::capture_graph() {
@@ -617,7 +725,11 @@ cudaError_t Plan::sync_stats() {
 cudaError_t Plan::autotune() {
     std::vector<LaunchConfig> cands;
     if (persistent_) {
-        cands = {LaunchConfig{128, 0}, LaunchConfig{256, 0}};
+        cands = {LaunchConfig{128, kUptPersistent}, LaunchConfig{256, kUptPersistent}};
+        if (!(flags_ & kFlagPersistent)) {
+            cands.push_back(LaunchConfig{128, kUptFamilyGrids});
+            cands.push_back(LaunchConfig{256, kUptFamilyGrids});
+        }
     } else {
         for (int b : {128, 256})
             for (int u : {1, 2, 4}) cands.push_back(LaunchConfig{b, u});

@@ -34,6 +34,7 @@ enum : int32_t {
     kFlagNoAntithetic = 0x4,
     kFlagTiming = 0x8,
     kFlagAutotune = 0x10,
+    kFlagFamilyGrids = 0x20,
 };
 
 // Grow-only device / pinned host allocations.
@@ -49,6 +50,13 @@ struct PinnedBuf {
     cudaError_t ensure(size_t bytes);
     void release();
 };
+
+// upt > 0: one single-family grid with `upt` units per thread.  For plans
+// over several families: upt == kUptPersistent runs one persistent
+// work-stealing kernel, upt == kUptFamilyGrids one grid per family group
+// (the autotuner picks between them).
+constexpr int kUptPersistent = 0;
+constexpr int kUptFamilyGrids = -1;
 
 struct LaunchConfig {
     int block = 256;
@@ -75,7 +83,10 @@ public:
     int64_t n_tiles() const { return n_tiles_; }
     int64_t path_steps() const { return path_steps_; }
     double last_simulate_ms() const { return last_ms_; }
-    int launches() const { return (n_tiles_ > 0 ? 1 : 0) + 1; }
+    int launches() const {
+        if (n_tiles_ <= 0) return 1;
+        return (cfg_.upt == kUptFamilyGrids ? (int)groups_.size() : 1) + 1;
+    }
     int block() const { return cfg_.block; }
     int upt() const { return cfg_.upt; }
     int ctas() const { return max_ctas_; }
@@ -108,8 +119,16 @@ private:
     bool counter_ready_ = false;
 
     std::vector<McOption> opts_;       // host copy (units/tiles filled per layout)
-    DevBuf d_opts_, d_tile_begin_, d_partials_, d_price_, d_se_, d_counter_;
-    PinnedBuf h_opts_, h_tile_begin_, h_price_, h_se_;
+    std::vector<int32_t> order_;       // device record k is option order_[k]
+    struct Group {                     // options of one (family, antithetic) pair
+        int family;
+        bool anti;
+        int32_t opt_lo, opt_hi;        // record range in work order
+        int64_t tile_lo, tile_hi;
+    };
+    std::vector<Group> groups_;        // filled for multi-family plans
+    DevBuf d_opts_, d_tile_begin_, d_partials_, d_price_, d_se_, d_counter_, d_out_index_;
+    PinnedBuf h_opts_, h_tile_begin_, h_price_, h_se_, h_out_index_;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;

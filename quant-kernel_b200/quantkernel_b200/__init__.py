@@ -6,6 +6,7 @@ package, backed by hand-written sm_100a CUDA kernels in libqk_b200.so.
 
 from ._abi import *  # noqa: F401,F403
 from ._abi import ABI_MAJOR, ABI_MINOR, QK_CALL, QK_PUT
+from .accelerator import QuantAccelerator
 from .engine import (
     McPlan,
     QKBadSizeError,
@@ -22,6 +23,7 @@ __all__ = [
     "QK_CALL",
     "QK_PUT",
     "McPlan",
+    "QuantAccelerator",
     "QKBadSizeError",
     "QKError",
     "QKInvalidInputError",

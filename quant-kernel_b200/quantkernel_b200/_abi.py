@@ -34,3 +34,4 @@ QK_PLAN_GRAPH = 0x2
 QK_PLAN_NO_ANTITHETIC = 0x4
 QK_PLAN_TIMING = 0x8
 QK_PLAN_AUTOTUNE = 0x10
+QK_PLAN_FAMILY_GRIDS = 0x20

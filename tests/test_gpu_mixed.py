@@ -9,8 +9,8 @@ import numpy as np
 import pytest
 
 from quantkernel_b200 import (QK_MC_EULER, QK_MC_HESTON, QK_MC_LOCAL_VOL, QK_MC_MILSTEIN,
-                              QK_PLAN_AUTOTUNE, QK_PLAN_GRAPH, QK_PLAN_PERSISTENT,
-                              QK_PLAN_TIMING, workloads)
+                              QK_PLAN_AUTOTUNE, QK_PLAN_FAMILY_GRIDS, QK_PLAN_GRAPH,
+                              QK_PLAN_PERSISTENT, QK_PLAN_TIMING, workloads)
 
 pytestmark = pytest.mark.gpu
 
@@ -50,14 +50,25 @@ def test_plan_graph_persistent_autotune_agree(qk):
     base.execute()
     p0, s0 = base.results()
     for flags in (QK_PLAN_GRAPH, QK_PLAN_PERSISTENT | QK_PLAN_GRAPH | QK_PLAN_TIMING,
+                  QK_PLAN_FAMILY_GRIDS, QK_PLAN_FAMILY_GRIDS | QK_PLAN_GRAPH,
                   QK_PLAN_AUTOTUNE, QK_PLAN_AUTOTUNE | QK_PLAN_GRAPH):
         plan = qk.plan(**b, flags=flags)
         for _ in range(3):  # graph replays are deterministic
             plan.execute()
             p, s = plan.results()
-            np.testing.assert_allclose(p, p0, rtol=1e-13, atol=0)
+            if flags & QK_PLAN_AUTOTUNE:  # the tuner may change the block size
+                np.testing.assert_allclose(p, p0, rtol=1e-13, atol=0)
+            else:  # same tile geometry in every mode: bit for bit
+                np.testing.assert_array_equal(p, p0)
         st = plan.stats()
-        assert st["launches"] == 2
+        cfg = plan.config()
+        if flags & QK_PLAN_FAMILY_GRIDS:
+            assert cfg["units_per_thread"] == -1
+        if flags & QK_PLAN_PERSISTENT:
+            assert cfg["units_per_thread"] == 0
+        # persistent: simulate + finalize; family grids: one grid per family
+        # (Euler with local vol, Milstein, Heston) + finalize
+        assert st["launches"] == (4 if cfg["units_per_thread"] == -1 else 2)
         plan.close()
     base.close()
 
