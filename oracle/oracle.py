@@ -57,6 +57,7 @@ class Oracle:
             "qko_normals": (None, [U64, I32, PD]),
             "qko_philox4x32_10": (None, [PU32, PU32, PU32]),
             "qko_philox_normals4": (None, [U64, U32, U32, U32, PD]),
+            "qko_philox_normals6": (None, [U64, U32, U32, U32, PD]),
             "qko_philox_price": (D, [I32] + [D] * 11 + [I32, I32, I32, U64, I32, PD]),
             "qko_control_variates": (D, term),
             "qko_stratified": (D, term),
@@ -158,6 +159,11 @@ class Oracle:
         o = (U32 * 4)()
         self.lib.qko_philox4x32_10(c, k, o)
         return list(o)
+
+    def philox_normals6(self, seed, c0, c1, c3):
+        z = np.empty(6)
+        self.lib.qko_philox_normals6(seed, c0, c1, c3, _pd(z))
+        return z
 
     def philox_normals4(self, seed, c0, c1, c3):
         z = np.empty(4)

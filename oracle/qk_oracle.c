@@ -830,7 +830,10 @@ double qko_heston_cf_price(double spot, double strike, double t, double r, doubl
  * Terminal models: normal k of the option lives at unit k / 4, block 0,
  *   slot k % 4 (k = pair index, or path index when plain).
  * One-factor stepwise models: step j of unit u is block j / 4, slot j % 4.
- * Heston: step j of unit u is block j / 2; z1 = slot 2(j%2), z2 = next slot.
+ * Heston: one call gives six normals, three Box-Muller pairs with 23-bit
+ *   radii from x0 >> 9, x1 >> 9, x2 >> 9 and angles of 16, 16 and 18 bits
+ *   from x3 & 0xFFFF, x3 >> 16 and (x0 & 0x1FF) | (x1 & 0x1FF) << 9;
+ *   step j of unit u is block j / 3, (z1, z2) = pair j % 3.
  * ===================================================================== */
 void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
     uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
@@ -857,6 +860,25 @@ static void box_muller(uint32_t xa, uint32_t xb, double* za, double* zb) {
     *zb = rad * sin(M_PI * g);
 }
 
+/* Box-Muller from a 23-bit radius word and an n-bit angle word. */
+static void box_muller_bits(uint32_t ub, uint32_t gb, int n, double* za, double* zb) {
+    const double u = ((double)ub + 0.5) * 0x1p-23;
+    const double g = ((double)gb + 0.5) * ldexp(1.0, -(n - 1)) - 1.0;
+    const double rad = sqrt(-2.0 * log(u));
+    *za = rad * cos(M_PI * g);
+    *zb = rad * sin(M_PI * g);
+}
+
+void qko_philox_normals6(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[6]) {
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    const uint32_t ctr[4] = {c0, c1, 0u, c3};
+    uint32_t x[4];
+    qko_philox4x32_10(ctr, key, x);
+    box_muller_bits(x[0] >> 9, x[3] & 0xFFFFu, 16, &z[0], &z[1]);
+    box_muller_bits(x[1] >> 9, x[3] >> 16, 16, &z[2], &z[3]);
+    box_muller_bits(x[2] >> 9, (x[0] & 0x1FFu) | ((x[1] & 0x1FFu) << 9), 18, &z[4], &z[5]);
+}
+
 void qko_philox_normals4(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[4]) {
     const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
     const uint32_t ctr[4] = {c0, c1, 0u, c3};
@@ -880,11 +902,11 @@ static double replay_path(int32_t model, double spot, double t, double vol, doub
     const double sqrt_dt = sqrt(dt);
     if (model == 6 || model == 7) {
         const double rho_comp = sqrt(smax(1.0 - rho * rho, 0.0));
-        double s = spot, v = v0;
+        double s = spot, v = v0, z6[6];
         for (int32_t j = 0; j < steps; ++j) {
-            if ((j & 1) == 0) qko_philox_normals4(seed, unit, (uint32_t)(j >> 1), c3, z4);
-            const double z1 = sg * z4[2 * (j & 1)];
-            const double z2 = sg * z4[2 * (j & 1) + 1];
+            if (j % 3 == 0) qko_philox_normals6(seed, unit, (uint32_t)(j / 3), c3, z6);
+            const double z1 = sg * z6[2 * (j % 3)];
+            const double z2 = sg * z6[2 * (j % 3) + 1];
             const double v_pos = smax(v, 0.0);
             const double sqrt_v = sqrt(v_pos);
             const double dw1 = sqrt_dt * z1;
@@ -931,9 +953,9 @@ double qko_philox_price(int32_t model, double spot, double strike, double t, dou
         const int32_t units = antithetic ? paths - paths / 2 : paths;
         const int32_t n_pairs = paths / 2;
         for (int32_t u = 0; u < units; ++u) {
-            double z4[4];
-            qko_philox_normals4(seed, (uint32_t)u, 0u, antithetic ? 0u : 1u, z4);
-            double w = (sqrt_v0 > 1e-15) ? z4[0] / (sqrt_v0 * sqrt_dt * spot) : 0.0;
+            double z6[6];
+            qko_philox_normals6(seed, (uint32_t)u, 0u, antithetic ? 0u : 1u, z6);
+            double w = (sqrt_v0 > 1e-15) ? z6[0] / (sqrt_v0 * sqrt_dt * spot) : 0.0;
             w = smax(-clip, smin(clip, w));
             const double a = intrinsic(replay_path(6, spot, t, vol, r, q, v0, kappa, theta, sigma,
                                                    rho, steps, seed, (uint32_t)u,

@@ -115,6 +115,8 @@ double qko_heston_cf_price(double spot, double strike, double t, double r, doubl
 void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* The GPU's normal with index k of stream (seed, c0, c1, c3); see qk_oracle.c. */
 void qko_philox_normals4(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[4]);
+/* The Heston kernels' six normals of one call (three Box-Muller pairs). */
+void qko_philox_normals6(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[6]);
 /* model as in qko_bsm_family_batch, plus 6 = Heston (uses v0..rho; vol ignored)
  * and 7 = Heston likelihood-ratio delta (vol holds weight_clip).
  * antithetic: 1 = pairs (GPU default), 0 = independent paths. */

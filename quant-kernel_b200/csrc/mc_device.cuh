@@ -99,6 +99,38 @@ __device__ __forceinline__ void normals4(uint32_t unit, uint32_t block, uint32_t
     box_muller(x.z, x.w, z[2], z[3]);
 }
 
+// Box-Muller from a 23-bit radius word and an n-bit angle word:
+//   u = (ub + 1/2) 2^-23,  g = (gb + 1/2) 2^-(n-1) - 1  (gscale = 2^-(n-1),
+//   goff = 2^-n - 1, both exact in FP32 for n <= 23).
+__device__ __forceinline__ void box_muller_bits(uint32_t ub, uint32_t gb, float gscale, float goff,
+                                                float& za, float& zb) {
+    const float u = fma_rn(__uint2float_rn(ub), 0x1p-23f, 0x1p-24f);
+    const float g = fma_rn(__uint2float_rn(gb), gscale, goff);
+    const float w = -1.38629436111989061883f * ptx_lg2(u);  // -2 ln u
+    const float rad = ptx_sqrt(w);
+    const float ang = 3.14159265358979323846f * g;
+    za = rad * ptx_cos(ang);
+    zb = rad * ptx_sin(ang);
+}
+
+// Six normals from one Philox call: three Box-Muller pairs, each with a
+// 23-bit radius (the top 23 bits of x, y, z) and an angle of 16, 16 and 18
+// bits (the low and high halves of w; the low 9 bits of x and of y).  Every
+// output bit of the call is used once.  pair(p) computes pair p on demand, so
+// only the four words stay live across the three steps they feed.
+struct Philox6 {
+    U4 x;
+    __device__ __forceinline__ void pair(int p, float& za, float& zb) const {
+        if (p == 0)
+            box_muller_bits(x.x >> 9, x.w & 0xFFFFu, 0x1p-15f, 0x1p-16f - 1.0f, za, zb);
+        else if (p == 1)
+            box_muller_bits(x.y >> 9, x.w >> 16, 0x1p-15f, 0x1p-16f - 1.0f, za, zb);
+        else
+            box_muller_bits(x.z >> 9, (x.x & 0x1FFu) | ((x.y & 0x1FFu) << 9), 0x1p-17f,
+                            0x1p-18f - 1.0f, za, zb);
+    }
+};
+
 // ---------------------------------------------------------------------------
 // Double-double accumulation (Knuth TwoSum).  A non-finite sum drops its error
 // term so that inf stays inf instead of turning into NaN.

@@ -205,7 +205,8 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 //   v' = max(v (1 - kappa dt) + kappa theta dt
 //            + sigma sqrt(dt) sqrt(v) (rho z1 + sqrt(1-rho^2) z2), 0)
 // v >= 0 after every step (and v0 >= 0 is validated), so the reference's
-// v_pos = max(v, 0) is v itself.  One Philox call feeds two steps of a unit.
+// v_pos = max(v, 0) is v itself.  One Philox call feeds three steps of a unit
+// (six normals: Philox6).
 // ----------------------------------------------------------------------------
 //
 // LR = true: the likelihood-ratio delta of heston_lr_delta.cpp:37-132.  Each
@@ -232,21 +233,21 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         vd[k] = v0;
         zfirst[k] = 0.0f;
     }
-    for (int32_t j = 0; j < steps; j += 2) {
-        float z[UPT][4];
+    uint32_t blk = 0;  // step block j / 3
+    for (int32_t j = 0; j < steps; j += 3, ++blk) {
+        Philox6 r[UPT];
 #pragma unroll
-        for (int k = 0; k < UPT; ++k) normals4(unit0 + (uint32_t)k * stride, (uint32_t)(j >> 1), c3, k0, k1, z[k]);
-        if (LR && j == 0) {
+        for (int k = 0; k < UPT; ++k)
+            r[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk, 0u, c3, k0, k1);
+        const int32_t m = (steps - j) < 3 ? (steps - j) : 3;
 #pragma unroll
-            for (int k = 0; k < UPT; ++k) zfirst[k] = z[k][0];
-        }
-        const int32_t m = (steps - j) < 2 ? (steps - j) : 2;
-#pragma unroll
-        for (int s = 0; s < 2; ++s) {
+        for (int s = 0; s < 3; ++s) {
             if (s < m) {
 #pragma unroll
                 for (int k = 0; k < UPT; ++k) {
-                    const float z1 = z[k][2 * s], z2 = z[k][2 * s + 1];
+                    float z1, z2;
+                    r[k].pair(s, z1, z2);
+                    if (LR && j == 0 && s == 0) zfirst[k] = z1;
                     const float sz1 = sqdt * z1;
                     const float xw = fma_rn(xr, z1, xc * z2);
                     {

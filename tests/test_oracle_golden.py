@@ -181,6 +181,35 @@ def test_philox_box_muller_layout(oracle):
     assert abs(zs.mean()) < 0.02 and abs(zs.var() - 1.0) < 0.02
 
 
+def test_philox_six_normal_layout(oracle):
+    """The Heston kernels draw three Box-Muller pairs per Philox call: 23-bit
+    radii from the top of words 0-2, angles of 16, 16 and 18 bits from word 3
+    and the low 9 bits of words 0 and 1."""
+    from scipy import stats
+
+    seed = 0xFEDCBA9876543210
+    key = [seed & 0xFFFFFFFF, seed >> 32]
+    for c0, c1, c3 in [(0, 0, 0), (3, 11, 1), (2**31 + 5, 66, 0)]:
+        x = _philox_py([c0, c1, 0, c3], key)
+        z = oracle.philox_normals6(seed, c0, c1, c3)
+        want = []
+        for ub, gb, n in ((x[0] >> 9, x[3] & 0xFFFF, 16), (x[1] >> 9, x[3] >> 16, 16),
+                          (x[2] >> 9, (x[0] & 0x1FF) | ((x[1] & 0x1FF) << 9), 18)):
+            u = (ub + 0.5) * 2.0**-23
+            g = (gb + 0.5) * 2.0**-(n - 1) - 1.0
+            rad = math.sqrt(-2.0 * math.log(u))
+            want += [rad * math.cos(math.pi * g), rad * math.sin(math.pi * g)]
+        assert np.allclose(z, want, rtol=0, atol=1e-14)
+    zs = np.stack([oracle.philox_normals6(seed, i, 0, 0) for i in range(40000)])
+    flat = zs.ravel()
+    assert abs(flat.mean()) < 0.01 and abs(flat.var() - 1.0) < 0.01
+    # each of the six slots is N(0, 1) and the slots are uncorrelated
+    for k in range(6):
+        assert stats.kstest(zs[:, k], "norm").pvalue > 1e-4, k
+    c = np.corrcoef(zs.T)
+    assert np.abs(c - np.eye(6)).max() < 0.03
+
+
 def test_philox_replay_estimator_is_statistically_the_reference(oracle):
     """The replay (the GPU's stream in FP64) and the reference (mt19937) price the
     same option within 4 combined standard errors, for every model."""
