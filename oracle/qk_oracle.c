@@ -829,7 +829,8 @@ double qko_heston_cf_price(double spot, double strike, double t, double r, doubl
  *     (x2, x3) -> n2, n3 the same way.
  * Terminal models: normal k of the option lives at unit k / 4, block 0,
  *   slot k % 4 (k = pair index, or path index when plain).
- * One-factor stepwise models: step j of unit u is block j / 4, slot j % 4.
+ * One-factor stepwise models: six normals per call as for Heston below;
+ *   step j of unit u is block j / 6, normal j % 6.
  * Heston: one call gives six normals, three Box-Muller pairs with 23-bit
  *   radii from x0 >> 9, x1 >> 9, x2 >> 9 and angles of 16, 16 and 18 bits
  *   from x3 & 0xFFFF, x3 >> 16 and (x0 & 0x1FF) | (x1 & 0x1FF) << 9;
@@ -917,11 +918,11 @@ static double replay_path(int32_t model, double spot, double t, double vol, doub
         }
         return s;
     }
-    double s = spot;
+    double s = spot, z6[6];
     const double drift = r - q;
     for (int32_t j = 0; j < steps; ++j) {
-        if ((j & 3) == 0) qko_philox_normals4(seed, unit, (uint32_t)(j >> 2), c3, z4);
-        const double dw = sqrt_dt * (sg * z4[j & 3]);
+        if (j % 6 == 0) qko_philox_normals6(seed, unit, (uint32_t)(j / 6), c3, z6);
+        const double dw = sqrt_dt * (sg * z6[j % 6]);
         if (model == 3)
             s = smax(1e-12, s + drift * s * dt + vol * s * dw + 0.5 * vol * vol * s * (dw * dw - dt));
         else

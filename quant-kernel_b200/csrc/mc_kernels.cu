@@ -142,7 +142,8 @@ __device__ __forceinline__ void sim_terminal(const McOption& o, uint32_t unit0, 
 // State is s = S/spot in FP32 and the step is the reference's additive form
 //   s' = max(s + s * inc, 1e-12/spot),  inc = (r-q)dt + vol sqrt(dt) z
 //   [Milstein: + c (z^2 - 1), c = vol^2 dt / 2]
-// evaluated as one fused s + s * inc.  One Philox call feeds four steps.
+// evaluated as one fused s + s * inc.  One Philox call feeds six steps
+// (Philox6: three Box-Muller pairs).
 // ----------------------------------------------------------------------------
 template <int UPT, bool ANTI, bool MIL>
 __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, uint32_t stride,
@@ -157,18 +158,21 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
         su[k] = 1.0f;
         sd[k] = 1.0f;
     }
-    for (int32_t j = 0; j < steps; j += 4) {
-        float z[UPT][4];
+    uint32_t blk = 0;  // step block j / 6
+    for (int32_t j = 0; j < steps; j += 6, ++blk) {
+        Philox6 r[UPT];
 #pragma unroll
-        for (int k = 0; k < UPT; ++k) normals4(unit0 + (uint32_t)k * stride, (uint32_t)(j >> 2), c3, k0, k1, z[k]);
-        const int32_t m = (steps - j) < 4 ? (steps - j) : 4;
+        for (int k = 0; k < UPT; ++k)
+            r[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk, 0u, c3, k0, k1);
+        const int32_t m = (steps - j) < 6 ? (steps - j) : 6;
+        float zp[UPT][2];
 #pragma unroll
-        for (int s = 0; s < 4; ++s) {
+        for (int s = 0; s < 6; ++s) {
             if (s < m) {
 #pragma unroll
                 for (int k = 0; k < UPT; ++k) {
-                    const float zz = z[k][s];
-                    float iu, id;
+                    if ((s & 1) == 0) r[k].pair(s >> 1, zp[k][0], zp[k][1]);
+                    const float zz = zp[k][s & 1];                    float iu, id;
                     if (MIL) {
                         iu = fma_rn(fma_rn(c, zz, b), zz, m0);
                         id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
