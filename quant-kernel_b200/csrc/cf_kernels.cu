@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "mc_plan.h"
+#include "qk_fault.h"
 
 namespace qkb {
 
@@ -271,6 +272,7 @@ cudaError_t launch_heston_cf(const CfOption* d_opts, int32_t n, double* d_out, c
         }
     }
     if (n <= 0) return cudaSuccess;
+    if ((e = injected_fault(kFaultLaunch)) != cudaSuccess) return e;
     heston_cf_kernel<<<n, 128, 0, st>>>(d_opts, n, d_out);
     return cudaGetLastError();
 }
@@ -294,6 +296,7 @@ struct CfScratch {
 }  // namespace
 
 cudaError_t heston_cf_price_host(const CfOption* h_opts, int32_t n, double* out) {
+    NvtxRange range("qk.heston_cf");
     if (n <= 0) return cudaSuccess;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -318,6 +321,7 @@ cudaError_t heston_cf_price_host(const CfOption* h_opts, int32_t n, double* out)
     if ((e = launch_heston_cf(static_cast<const CfOption*>(s.d_opts.p), n,
                               static_cast<double*>(s.d_out.p), s.st)) != cudaSuccess)
         return e;
+    if ((e = injected_fault(kFaultCopy)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(s.h_out.p, s.d_out.p, pb, cudaMemcpyDeviceToHost, s.st)) != cudaSuccess)
         return e;
     if ((e = cudaStreamSynchronize(s.st)) != cudaSuccess) return e;

@@ -25,6 +25,7 @@
 #include <mutex>
 
 #include "mc_launch.h"
+#include "qk_fault.h"
 
 namespace qkb {
 
@@ -289,7 +290,8 @@ cudaError_t DevBuf::ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
     release();
     size_t want = std::max<size_t>(bytes, 256);
-    cudaError_t e = cudaMalloc(&p, want);
+    cudaError_t e = injected_fault(kFaultAlloc);
+    if (e == cudaSuccess) e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
         cap = 0;
@@ -307,7 +309,8 @@ cudaError_t PinnedBuf::ensure(size_t bytes) {
     if (bytes <= cap && p) return cudaSuccess;
     release();
     size_t want = std::max<size_t>(bytes, 256);
-    cudaError_t e = cudaMallocHost(&p, want);
+    cudaError_t e = injected_fault(kFaultAlloc);
+    if (e == cudaSuccess) e = cudaMallocHost(&p, want);
     if (e != cudaSuccess) {
         p = nullptr;
         cap = 0;
@@ -437,6 +440,7 @@ cudaError_t Plan::ensure_stream() {
 }
 
 cudaError_t Plan::build(const BatchInput& in, int32_t flags, std::string* err) {
+    NvtxRange range("qk.build");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -605,6 +609,7 @@ cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
 }
 
 cudaError_t Plan::launch_all(cudaStream_t st, bool timing) {
+    if (cudaError_t fe = injected_fault(kFaultLaunch)) return fe;
     SimArgs a;
     a.opts = static_cast<const McOption*>(d_opts_.p);
     a.tile_begin = static_cast<const int64_t*>(d_tile_begin_.p);
@@ -657,6 +662,7 @@ cudaError_t Plan::capture_graph() {
 }
 
 cudaError_t Plan::execute(cudaStream_t stream) {
+    NvtxRange range("qk.execute");
     if (device_ < 0) return cudaErrorInvalidResourceHandle;
     DeviceGuard g(device_);
     cudaStream_t st = stream ? stream : stream_;
@@ -688,7 +694,9 @@ cudaError_t Plan::execute(cudaStream_t stream) {
 }
 
 cudaError_t Plan::results(double* out_price, double* out_se) {
+    NvtxRange range("qk.results");
     if (device_ < 0) return cudaErrorInvalidResourceHandle;
+    if (cudaError_t fe = injected_fault(kFaultCopy)) return fe;
     DeviceGuard g(device_);
     cudaStream_t st = last_stream_ ? last_stream_ : stream_;
     const size_t bytes = sizeof(double) * (size_t)n_;

@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "../../include/qk_abi.h"
+#include "qk_fault.h"
 
 namespace qkb {
 
@@ -35,7 +36,8 @@ int32_t fail_size(int64_t n) {
 }
 
 int32_t fail_cuda(cudaError_t e, const char* where) {
-    set_error_fmt("cuda error: %s (%s) in %s", cudaGetErrorName(e), cudaGetErrorString(e), where);
+    set_error_fmt("cuda error: %s (%s) in %s%s", cudaGetErrorName(e), cudaGetErrorString(e), where,
+                  take_injected_flag() ? " [injected]" : "");
     return QK_ERR_RUNTIME_INIT;
 }
 
