@@ -180,6 +180,40 @@ def test_python_errors_map_like_reference(qk):
         qk.standard_monte_carlo_price_batch([[100]], [100], [1], [0.2], [0.05], [0], [0], [10], [1])
 
 
+@pytest.mark.parametrize("call", [
+    lambda qk: qk.control_variates_price_batch([100, 100], [100], [1], [0.2], [0.05], [0], [0],
+                                               [10], [1]),
+    lambda qk: qk.stratified_sampling_price_batch([100], [100], [1], [0.2], [0.05], [0], [0],
+                                                  [10, 10], [1]),
+    lambda qk: qk.importance_sampling_price_batch([100], [100], [1], [0.2], [0.05], [0], [0], [10],
+                                                  [0.1, 0.2], [1]),
+    lambda qk: qk.quasi_monte_carlo_sobol_price_batch([100], [100, 90], [1], [0.2], [0.05], [0],
+                                                      [0], [10]),
+    lambda qk: qk.quasi_monte_carlo_halton_price_batch([100], [100], [1], [0.2], [0.05], [0],
+                                                       [0, 1], [10]),
+    lambda qk: qk.heston_price_cf_batch([100], [100], [1], [0.05], [0], [0.04], [2], [0.04], [0.3],
+                                        [-0.7], [0], [1024], [120.0, 80.0]),
+])
+def test_ragged_inputs_rejected_before_the_library(qk, call):
+    """Ragged arrays are a caller error the Python layer reports (ValueError)
+    before any C call, as the reference engine does (engine.py:120-141)."""
+    with pytest.raises(ValueError, match="length mismatch"):
+        call(qk)
+
+
+@pytest.mark.parametrize("fn,nargs", [("control_variates_price_batch", 9),
+                                      ("importance_sampling_price_batch", 10),
+                                      ("stratified_sampling_price_batch", 9),
+                                      ("quasi_monte_carlo_sobol_price_batch", 8),
+                                      ("quasi_monte_carlo_halton_price_batch", 8),
+                                      ("heston_price_cf_batch", 13)])
+def test_empty_batches_are_bad_size(qk, fn, nargs):
+    from quantkernel_b200 import QKBadSizeError
+
+    with pytest.raises(QKBadSizeError):
+        getattr(qk, fn)(*([[]] * nargs))
+
+
 def test_mixed_batch_requires_arrays_its_models_use(qk):
     n = 2
     model = np.array([2, 6], np.int32)
