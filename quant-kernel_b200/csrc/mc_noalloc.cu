@@ -52,8 +52,12 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;                               // serialises calls (and set-up)
 unsigned char* g_scratch_dev[kMaxDevices] = {};  // per-device address, set once
 
-constexpr int kBlock = 256;  // the regular Heston launch shape: same tiles,
-constexpr int kUpt = 2;      // same sums, same results
+// Fixed launch shape: 256 threads x 2 pairs = 512 antithetic pairs per tile,
+// the unit the tile limit is stated in.  The regular entry uses 128-thread
+// CTAs; the same paths summed in other tile groups agree to ~1e-15 relative
+// (double-double sums), not always bit for bit.
+constexpr int kBlock = 256;
+constexpr int kUpt = 2;
 
 // Device address of the scratch array on `dev` (the current device).
 cudaError_t scratch_address(int dev, unsigned char** out) {
