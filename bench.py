@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--cf-options", type=int, default=65536)
     ap.add_argument("--vr", action="store_true",
                     help="variance-reduction leg only (device + e2e; no CPU with --profile)")
+    ap.add_argument("--sur-device-rows", type=int, default=0,
+                    help="time device-resident surrogate inference on this many rows and exit")
     ap.add_argument("--sur-train-n", type=int, default=4_000_000)
     ap.add_argument("--sur-hold-n", type=int, default=100_000)
     ap.add_argument("--sur-epochs", type=int, default=60)
@@ -579,18 +581,7 @@ def surrogate_infer_leg(qk, checkpoint, n_query=1_000_000, n_judge=10_000, mc_pr
     f = features_of(*(b[k] for k in keys))
     inbox = src == 0
     rows = torch.from_numpy(sur.feature_rows(f[inbox]).view(np.int16)).cuda()
-    y = torch.empty(rows.shape[0], dtype=torch.float32, device="cuda")
-    st = torch.cuda.current_stream()
-    for _ in range(3):
-        sur.predict_device(rows.data_ptr(), rows.shape[0], y.data_ptr(), st.cuda_stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(st)
-    reps = 10
-    for _ in range(reps):
-        sur.predict_device(rows.data_ptr(), rows.shape[0], y.data_ptr(), st.cuda_stream)
-    e1.record(st)
-    torch.cuda.synchronize()
-    dev_s = e0.elapsed_time(e1) / 1e3 / reps
+    dev_s = _time_sur_device(sur, rows, False)
     sur_dev_rate = rows.shape[0] / dev_s
     # judge: 1e4 in-box queries re-priced by MC at 200 x 262144
     jidx = rng.choice(np.nonzero(inbox)[0], n_judge, replace=False)
@@ -704,6 +695,46 @@ def bsm_terminal_leg(qk, reps=20):
             "e2e_paths_per_s": paths / e2e}
 
 
+def _time_sur_device(sur, rows, layered, reps=10):
+    import torch
+
+    st = torch.cuda.Stream()
+    y = torch.empty(rows.shape[0], dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(st):
+        for _ in range(3):
+            sur.predict_device(rows.data_ptr(), rows.shape[0], y.data_ptr(), st.cuda_stream,
+                               layered=layered)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            sur.predict_device(rows.data_ptr(), rows.shape[0], y.data_ptr(), st.cuda_stream,
+                               layered=layered)
+        e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / reps
+
+
+def surrogate_device_leg(qk, checkpoint, n_rows):
+    """Device-resident inference on n_rows box-uniform normalised rows: the
+    fused kernel and the layer-by-layer GEMMs, CUDA events on a dedicated
+    stream."""
+    import torch
+
+    from quantkernel_b200.surrogate import HestonSurrogate, features_of, sample_box
+
+    sur = HestonSurrogate(qk, seed=0)
+    sur.load(checkpoint)
+    b = sample_box(n_rows, 99)
+    f = features_of(*(b[k] for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta",
+                                      "sigma", "rho")))
+    rows = torch.from_numpy(sur.feature_rows(f).view(np.int16)).cuda()
+    fused = _time_sur_device(sur, rows, False)
+    layered = _time_sur_device(sur, rows, True)
+    return {"rows": n_rows, "fused_ms": 1e3 * fused, "fused_prices_per_s": n_rows / fused,
+            "fused_tflops": n_rows / fused * SUR_FLOP_PER_ROW / 1e12,
+            "layered_ms": 1e3 * layered, "layered_prices_per_s": n_rows / layered}
+
+
 def vr_leg(qk, reps=5, cpu=True):
     """64 BSM calls/puts x 2^20 paths for each terminal variance-reduction
     estimator: device time of a graph-replayed plan (L2 flushed), end to end
@@ -797,6 +828,12 @@ def main():
         return 0
     if args.cpu_leg:
         cpu_leg(args.cpu_leg)
+        return 0
+    if args.sur_device_rows:
+        from quantkernel_b200 import QuantKernel
+
+        print(json.dumps({"leg": "surrogate_device", **surrogate_device_leg(
+            QuantKernel(), args.sur_checkpoint, args.sur_device_rows)}), flush=True)
         return 0
     if args.vr:
         import torch

@@ -387,6 +387,11 @@ QK_EXPORT int32_t qk_sur_heston_predict(qk_sur_model* model, const double* featu
  * y = price / S (DEVICE, fp32); asynchronous on `stream` (NULL = model's). */
 QK_EXPORT int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows, int64_t n,
                                                float* y, void* stream);
+/* The same inference as three layer-by-layer GEMM launches per 65,536 rows
+ * (activations round-trip through device memory): the reference the fused
+ * kernel behind qk_sur_heston_predict_device is tested against (same bits). */
+QK_EXPORT int32_t qk_sur_heston_predict_device_layered(qk_sur_model* model, const void* x_rows,
+                                                       int64_t n, float* y, void* stream);
 /* Normalised bf16 rows [n][64] (HOST output buffer of n*64 uint16). */
 QK_EXPORT int32_t qk_sur_heston_features(qk_sur_model* model, const double* features, int64_t n,
                                          void* out_rows);

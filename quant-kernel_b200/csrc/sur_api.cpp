@@ -148,6 +148,17 @@ int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows, in
                       "qk_sur_heston_predict_device");
 }
 
+int32_t qk_sur_heston_predict_device_layered(qk_sur_model* model, const void* x_rows, int64_t n,
+                                             float* y, void* stream) {
+    if (!model) return qkb::fail_null("model");
+    if (!x_rows) return qkb::fail_null("x_rows");
+    if (!y) return qkb::fail_null("y");
+    if (n <= 0) return qkb::fail_size(n);
+    return sur_status(model->m.predict_device(static_cast<const __nv_bfloat16*>(x_rows), n, y,
+                                              static_cast<cudaStream_t>(stream), true),
+                      "qk_sur_heston_predict_device_layered");
+}
+
 int32_t qk_sur_heston_features(qk_sur_model* model, const double* features, int64_t n,
                                void* out_rows) {
     if (!model) return qkb::fail_null("model");

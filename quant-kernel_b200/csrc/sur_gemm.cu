@@ -15,6 +15,7 @@ constexpr int kBM = 128;
 constexpr int kBK = 64;                       // 64 bf16 = 128 B = one swizzle row
 constexpr uint32_t kSpinLimit = 1u << 25;     // bounded mbarrier polls (seconds)
 constexpr uint32_t kABytes = kBM * kBK * 2;   // 16 KiB
+constexpr int kSurHidden = 256;               // hidden width of the surrogate MLP
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -112,7 +113,14 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// sigmoid(z) = (1 + tanh(z / 2)) / 2 with the MUFU tanh (one special-function
+// op; |error| ~ 2^-11, below the bf16 rounding every activation gets next).
+__device__ __forceinline__ float tanh_approx(float x) {
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sigmoidf_(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
 
 // 32 bf16 values to 64 contiguous bytes.
 __device__ __forceinline__ void store_bf16x32(__nv_bfloat16* dst, const float (&v)[32]) {
@@ -200,17 +208,25 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
             }
         }
     } else {  // kEpiLast: BN == N (the whole hidden row is in this CTA)
-        float y = 0.0f;
-#pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
-            tmem_ld32(tbase + c * 32, v);
-            const int col0 = c * 32;
+        // head dot product as four partial sums over columns 64g .. 64g + 63,
+        // combined in order -- the summation the fused inference kernel uses
+        float part[4];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const float z = v[j] + __ldg(a.bias + col0 + j);
-                y = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), y);
+        for (int g = 0; g < 4; ++g) {
+            float p = 0.0f;  // one fmaf chain over the group's 64 columns
+#pragma unroll 1
+            for (int cc = 0; cc < 2; ++cc) {
+                const int col0 = (2 * g + cc) * 32;
+                tmem_ld32(tbase + col0, v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float z = v[j] + __ldg(a.bias + col0 + j);
+                    p = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), p);
+                }
             }
+            part[g] = p;
         }
+        float y = ((part[0] + part[1]) + part[2]) + part[3];
         y += __ldg(a.b4);
         if (live) a.y_out[row] = y;
         if (a.target != nullptr) {
@@ -355,6 +371,253 @@ __global__ void __launch_bounds__(128, 1)
     }
 }
 
+
+// ----------------------------------------------------------------------------
+// Fused MLP inference.  One persistent CTA per SM (512 threads) walks 128-row
+// tiles: layer 1 (K = 64), layer 2 and layer 3 (K = 256) run back to back on
+// one TMEM accumulator (128 x 256 fp32); each hidden activation tile goes
+// from TMEM through the bias + SiLU epilogue into shared memory, written in
+// the 128-byte-swizzled K-major layout the next layer's MMA reads as its A
+// operand, so activations never leave the SM.  Weights stream from L2 through
+// a 4-slot ring of 32 KiB k-blocks (W1, W2[0..3], W3[0..3] per tile: nine
+// loads); the next tile's input rows are prefetched during layer 2.
+//
+// Ring schedule (loads are numbered wl = 9 t + i within the CTA): a load is
+// issued only when the previous user of its slot (load wl - 4) belongs to a
+// layer whose accumulator is already complete -- loads 0-3 at the start of a
+// tile (previous users: the last tile's W3), load 4 after layer 1, loads 5-8
+// after layer 2 -- so the producer never waits on work issued later.
+// The arithmetic and summation order are those of the layer-by-layer GEMMs
+// (kEpiFwd, kEpiLast), so the results are the same bits.
+// ----------------------------------------------------------------------------
+constexpr int kIWSlots = 4;
+constexpr uint32_t kWBlock = 256 * kBK * 2;        // 32 KiB: 256 rows x 64 bf16
+constexpr uint32_t kHBytes = 4 * kABytes;          // 64 KiB: 128 rows x 256 bf16
+constexpr size_t kInferSmem = kHBytes + kABytes + kIWSlots * kWBlock + 1024;
+constexpr int kInferThreads = 512;                 // 16 warps: 4 per TMEM lane quarter
+
+// 32 activations (columns col0 .. col0 + 31 of tile row r) into the layout a
+// 128-byte-swizzle TMA load would produce: k-block col / 64, row r at 128 r,
+// 16-byte chunk c at (c ^ (r & 7)) * 16.
+__device__ __forceinline__ void store_h_sw128(uint8_t* hbuf, int r, int col0, const float (&v)[32]) {
+    uint8_t* row = hbuf + (col0 >> 6) * kABytes + r * 128;
+    const int c0 = (col0 & 63) >> 3;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        __nv_bfloat162 p[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) p[j] = __floats2bfloat162_rn(v[q * 8 + 2 * j], v[q * 8 + 2 * j + 1]);
+        *reinterpret_cast<uint4*>(row + (((c0 + q) ^ (r & 7)) << 4)) = *reinterpret_cast<uint4*>(p);
+    }
+}
+
+__global__ void __launch_bounds__(kInferThreads, 1)
+    mlp_infer_kernel(const __grid_constant__ CUtensorMap tx, const __grid_constant__ CUtensorMap tw1,
+                     const __grid_constant__ CUtensorMap tw2, const __grid_constant__ CUtensorMap tw3,
+                     const InferArgs a) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                               ~static_cast<uintptr_t>(1023));
+    uint8_t* hbuf = smem;
+    uint8_t* xbuf = smem + kHBytes;
+    uint8_t* wbuf = xbuf + kABytes;
+    __shared__ __align__(8) uint64_t xfull, accbar, drain;
+    __shared__ __align__(8) uint64_t wfull[kIWSlots];
+    __shared__ __align__(8) uint64_t wempty[kIWSlots];
+    __shared__ float sb1[kSurHidden], sb2[kSurHidden], sb3[kSurHidden], sw4[kSurHidden];
+    __shared__ float part[4][kBM];  // head partial sums per column group
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // epilogue mapping: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its tile
+    // rows) and columns 64 (w / 4) .. + 63 (its column group)
+    const int q = warp & 3, grp = warp >> 2;
+    const int r = q * 32 + lane;
+    const int64_t n_tiles = (a.n + kBM - 1) / kBM;
+
+    if (tid < kSurHidden) {
+        sb1[tid] = a.b1[tid];
+        sb2[tid] = a.b2[tid];
+        sb3[tid] = a.b3[tid];
+        sw4[tid] = a.w4[tid];
+    }
+    if (tid == 0) {
+        mbar_init(smem_u32(&xfull), 1);
+        mbar_init(smem_u32(&accbar), 1);
+        mbar_init(smem_u32(&drain), 1);
+        for (int s = 0; s < kIWSlots; ++s) {
+            mbar_init(smem_u32(&wfull[s]), 1);
+            mbar_init(smem_u32(&wempty[s]), 1);
+        }
+        abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(256u)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16);
+    const float b4 = __ldg(a.b4);
+    constexpr uint32_t idesc = idesc_bf16<256>();
+
+    // producer state (thread 0) and MMA state (thread 32)
+    uint32_t wl = 0, wc = 0, ap = 0, xl = 0;
+    int last_round[kIWSlots] = {-1, -1, -1, -1};
+    bool x_pending = false;        // an input-row load not yet consumed
+    uint32_t x_pending_parity = 0;
+
+    auto load_w = [&](const CUtensorMap* m, int kx) -> bool {
+        const uint32_t s = wl % kIWSlots, round = wl / kIWSlots;
+        if (round > 0 && !mbar_wait(smem_u32(&wempty[s]), (round - 1) & 1)) return false;
+        mbar_expect_tx(smem_u32(&wfull[s]), kWBlock);
+        tma_load_2d(smem_u32(wbuf + s * kWBlock), m, kx, 0, smem_u32(&wfull[s]));
+        last_round[s] = static_cast<int>(round);
+        ++wl;
+        return true;
+    };
+    auto load_x = [&](int64_t tile) {  // load number xl; tile iteration xl waits on it
+        mbar_expect_tx(smem_u32(&xfull), kABytes);
+        tma_load_2d(smem_u32(xbuf), &tx, 0, static_cast<int>(tile * kBM), smem_u32(&xfull));
+        x_pending = true;
+        x_pending_parity = xl & 1;
+        ++xl;
+    };
+    auto mma_layer = [&](const uint8_t* abase, int nkb) -> bool {
+        for (int kb = 0; kb < nkb; ++kb) {
+            const uint32_t s = wc % kIWSlots;
+            if (!mbar_wait(smem_u32(&wfull[s]), (wc / kIWSlots) & 1)) return false;
+            fence_after();
+            const uint32_t sa = smem_u32(abase + kb * kABytes), sb = smem_u32(wbuf + s * kWBlock);
+#pragma unroll
+            for (int kk = 0; kk < kBK / 16; ++kk)
+                umma_bf16(tmem, desc_sw128(sa + kk * 32), desc_sw128(sb + kk * 32), idesc,
+                          (kb | kk) != 0 ? 1u : 0u);
+            umma_commit(smem_u32(&wempty[s]));
+            ++wc;
+        }
+        umma_commit(smem_u32(&accbar));
+        return true;
+    };
+    auto fail = [&](int code) {
+        abort_flag = 1;
+        atomicExch(a.err, code);
+    };
+    // all threads: the layer's accumulator is complete
+    auto acc_ready = [&]() -> bool {
+        __syncwarp();
+        const bool ok = mbar_wait(smem_u32(&accbar), ap & 1);
+        ++ap;
+        __syncwarp();
+        fence_after();
+        if (!ok && lane == 0) fail(13);
+        __syncthreads();
+        return abort_flag == 0;
+    };
+    auto epi_hidden = [&](const float* bias) {
+        float v[32];
+#pragma unroll 1
+        for (int cc = 0; cc < 2; ++cc) {
+            const int col0 = (2 * grp + cc) * 32;
+            tmem_ld32(tbase + col0, v);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const float z = v[j] + bias[col0 + j];
+                v[j] = z * sigmoidf_(z);
+            }
+            store_h_sw128(hbuf, r, col0, v);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        fence_before();
+        __syncthreads();
+    };
+
+    int it = 0;
+    for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+        // layer 1: H = silu(X W1^T + b1)
+        if (tid == 0) {
+            if (it == 0) load_x(t);
+            if (!(load_w(&tw1, 0) && load_w(&tw2, 0) && load_w(&tw2, 64) && load_w(&tw2, 128)))
+                fail(11);
+        } else if (tid == 32) {
+            if (!mbar_wait(smem_u32(&xfull), it & 1) || !mma_layer(xbuf, 1)) fail(12);
+        }
+        if (!acc_ready()) break;
+        if (tid == 0) x_pending = false;  // consumed by layer 1
+        epi_hidden(sb1);
+        // layer 2: H = silu(H W2^T + b2); the next tile's rows load meanwhile
+        if (tid == 0) {
+            if (t + gridDim.x < n_tiles) load_x(t + gridDim.x);
+            if (!load_w(&tw2, 192)) fail(11);
+        } else if (tid == 32) {
+            fence_after();
+            if (!mma_layer(hbuf, 4)) fail(12);
+        }
+        if (!acc_ready()) break;
+        epi_hidden(sb2);
+        // layer 3 and the head: y = silu(H W3^T + b3) . w4 + b4
+        if (tid == 0) {
+            if (!(load_w(&tw3, 0) && load_w(&tw3, 64) && load_w(&tw3, 128) && load_w(&tw3, 192)))
+                fail(11);
+        } else if (tid == 32) {
+            fence_after();
+            if (!mma_layer(hbuf, 4)) fail(12);
+        }
+        if (!acc_ready()) break;
+        {
+            float v[32];
+            float p = 0.0f;  // one fmaf chain over this group's 64 columns
+#pragma unroll 1
+            for (int cc = 0; cc < 2; ++cc) {
+                const int col0 = (2 * grp + cc) * 32;
+                tmem_ld32(tbase + col0, v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float z = v[j] + sb3[col0 + j];
+                    p = fmaf(z * sigmoidf_(z), sw4[col0 + j], p);
+                }
+            }
+            part[grp][r] = p;
+        }
+        fence_before();
+        __syncthreads();
+        if (grp == 0) {
+            const float y = (((part[0][r] + part[1][r]) + part[2][r]) + part[3][r]) + b4;
+            const int64_t row = t * kBM + r;
+            if (row < a.n) a.y[row] = y;
+        }
+        // part[] is next written after two more barriers of the next tile
+    }
+
+    // Teardown.  After an abort: the producer waits (bounded) for the loads
+    // it issued, the MMA thread for its MMAs (a commit on `drain`), then the
+    // accumulator is freed.
+    if (abort_flag) {
+        if (tid == 0) {
+            for (int s = 0; s < kIWSlots; ++s)
+                if (last_round[s] >= 0) mbar_wait(smem_u32(&wfull[s]), last_round[s] & 1);
+            if (x_pending) mbar_wait(smem_u32(&xfull), x_pending_parity);
+        } else if (tid == 32) {
+            umma_commit(smem_u32(&drain));
+            mbar_wait(smem_u32(&drain), 0);
+        }
+    }
+    fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u)
+                     : "memory");
+    }
+}
+
 template <int BN, int EPI>
 cudaError_t launch_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArgs& a, int splits,
                      cudaStream_t st) {
@@ -372,6 +635,22 @@ cudaError_t launch_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArg
 }
 
 }  // namespace
+
+cudaError_t launch_mlp_infer(const CUtensorMap& tx, const CUtensorMap& tw1, const CUtensorMap& tw2,
+                             const CUtensorMap& tw3, const InferArgs& a, int ctas, cudaStream_t st) {
+    static std::once_flag once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(once, [] {
+        attr_err = cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(kInferSmem));
+    });
+    if (attr_err != cudaSuccess) return attr_err;
+    if (a.n <= 0) return cudaSuccess;
+    const int64_t tiles = (a.n + kBM - 1) / kBM;
+    const int grid = static_cast<int>(tiles < ctas ? tiles : ctas);
+    mlp_infer_kernel<<<grid, kInferThreads, kInferSmem, st>>>(tx, tw1, tw2, tw3, a);
+    return cudaGetLastError();
+}
 
 bool make_tmap_bf16(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
                     uint32_t box_rows) {

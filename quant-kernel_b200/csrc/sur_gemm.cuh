@@ -51,6 +51,23 @@ struct GemmArgs {
     int* err;                    // error word (0 = ok)
 };
 
+// Fused MLP inference: y[i] = w4 . silu(W3 silu(W2 silu(W1 x_i + b1) + b2) + b3) + b4
+// for normalised bf16 rows x [n][64] (see sur_gemm.cu, mlp_infer_kernel).
+struct InferArgs {
+    int64_t n;               // rows
+    const float* b1;         // [256]
+    const float* b2;
+    const float* b3;
+    const float* w4;
+    const float* b4;         // [1]
+    float* y;                // [n]
+    int* err;                // error word (0 = ok)
+};
+// tx: x [n][64] (box 64 x 128); tw1: W1 [256][64]; tw2, tw3: [256][256]
+// (boxes 64 x 256).  ctas: persistent grid size (one CTA per SM).
+cudaError_t launch_mlp_infer(const CUtensorMap& tx, const CUtensorMap& tw1, const CUtensorMap& tw2,
+                             const CUtensorMap& tw3, const InferArgs& a, int ctas, cudaStream_t st);
+
 // Host side: tensor maps over bf16 row-major [rows][cols] (cols contiguous).
 bool make_tmap_bf16(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
                     uint32_t box_rows);

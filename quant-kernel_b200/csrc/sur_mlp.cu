@@ -513,8 +513,27 @@ cudaError_t SurModel::ensure_predict_buffers(int64_t rows) {
     return cudaSuccess;
 }
 
-cudaError_t SurModel::predict_device(const __nv_bfloat16* x, int64_t n, float* y, cudaStream_t st) {
+cudaError_t SurModel::predict_device(const __nv_bfloat16* x, int64_t n, float* y, cudaStream_t st,
+                                     bool layered) {
     DeviceGuard g(device_);
+    if (!layered) {
+        if (sm_count_ <= 0)
+            QK_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
+        CUtensorMap tx, tw1, tw2, tw3;
+        if (!(tmap(&tx, x, n, kSurInPad, 128) && tmap(&tw1, W1b_, kSurHid, kSurInPad, 256) &&
+              tmap(&tw2, W2b_, kSurHid, kSurHid, 256) && tmap(&tw3, W3b_, kSurHid, kSurHid, 256)))
+            return cudaErrorInvalidValue;
+        InferArgs ia{};
+        ia.n = n;
+        ia.b1 = P_ + SurLayout::b1;
+        ia.b2 = P_ + SurLayout::b2;
+        ia.b3 = P_ + SurLayout::b3;
+        ia.w4 = P_ + SurLayout::w4;
+        ia.b4 = P_ + SurLayout::b4;
+        ia.y = y;
+        ia.err = &state_->err;
+        return launch_mlp_infer(tx, tw1, tw2, tw3, ia, sm_count_, st);
+    }
     QK_TRY(ensure_predict_buffers(std::min<int64_t>(n, kPredChunk)));
     for (int64_t off = 0; off < n; off += kPredChunk) {
         const int64_t m = std::min<int64_t>(kPredChunk, n - off);

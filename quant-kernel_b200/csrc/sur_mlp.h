@@ -63,8 +63,11 @@ public:
                       float* out_epoch_loss);
     // price / spot of calls for raw features, host in and out.
     cudaError_t predict(const double* features, int64_t n, double* out);
-    // Device-resident inference on normalised bf16 rows [n][64].
-    cudaError_t predict_device(const __nv_bfloat16* x_rows, int64_t n, float* y, cudaStream_t st);
+    // Device-resident inference on normalised bf16 rows [n][64]: the fused
+    // kernel (all three layers per 128-row tile in one persistent launch), or
+    // with layered = true the layer-by-layer GEMMs it is tested against.
+    cudaError_t predict_device(const __nv_bfloat16* x_rows, int64_t n, float* y, cudaStream_t st,
+                               bool layered = false);
     // One forward + backward without an update: loss and the 134,401 gradients.
     cudaError_t gradients(const double* features, const double* target, int n, double* grads,
                           double* loss);
@@ -114,6 +117,7 @@ private:
     cudaGraphExec_t step_graph_ = nullptr;
     // inference buffers
     int64_t pred_rows_ = 0;
+    int sm_count_ = 0;
     __nv_bfloat16 *PX_ = nullptr, *PH1_ = nullptr, *PH2_ = nullptr;
     float* Py_ = nullptr;
 };

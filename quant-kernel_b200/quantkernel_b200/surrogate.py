@@ -86,11 +86,13 @@ class HestonSurrogate:
         self._check(self.lib.qk_sur_heston_predict(self._h, _pd(f), f.shape[0], _pd(out)), "predict")
         return out
 
-    def predict_device(self, x_rows_ptr, n, y_ptr, stream=0):
-        self._check(self.lib.qk_sur_heston_predict_device(self._h, ct.c_void_p(x_rows_ptr), int(n),
-                                                          ct.c_void_p(y_ptr),
-                                                          ct.c_void_p(stream) if stream else None),
-                    "predict_device")
+    def predict_device(self, x_rows_ptr, n, y_ptr, stream=0, layered=False):
+        """Device rows in, device price/S out.  The fused kernel by default;
+        layered=True runs the layer-by-layer GEMMs it is tested against."""
+        fn = (self.lib.qk_sur_heston_predict_device_layered if layered
+              else self.lib.qk_sur_heston_predict_device)
+        self._check(fn(self._h, ct.c_void_p(x_rows_ptr), int(n), ct.c_void_p(y_ptr),
+                       ct.c_void_p(stream) if stream else None), "predict_device")
 
     def feature_rows(self, features):
         """Normalised bf16 rows [n][64] as uint16 (host)."""

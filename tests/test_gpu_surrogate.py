@@ -157,3 +157,34 @@ def test_trained_network_gain_over_monte_carlo(qk, data):
           f"(x{sur_rate / mc_rate:.0f}); |err|/S mean {err.mean():.2e}")
     # end to end through host arrays (the device-resident ratio is ~1e4)
     assert sur_rate > 50 * mc_rate
+
+
+def test_fused_inference_equals_layered_gemms(qk, data):
+    """The fused inference kernel (three layers per 128-row tile, activations
+    kept in shared memory) gives the bits of the layer-by-layer GEMMs, for
+    batch sizes that leave partial tiles and more tiles than SMs, and matches
+    the FP64 oracle forward to bf16 accuracy."""
+    import torch
+
+    (f, t, _, _), (hf, _, _, _) = data
+    sur = HestonSurrogate(qk, seed=13)
+    sur.set_dataset(f, t)
+    sur.train(epochs=2, batch=1024, lr=2e-3, shuffle_seed=3)
+    for n in (1, 127, 128, 129, 5000, 148 * 128 * 3 + 77):
+        rows = np.tile(sur.feature_rows(hf), (n // hf.shape[0] + 1, 1))[:n]
+        x = torch.from_numpy(rows.view(np.int16)).cuda()
+        y_f = torch.full((n,), float("nan"), dtype=torch.float32, device="cuda")
+        y_l = torch.full((n,), float("nan"), dtype=torch.float32, device="cuda")
+        sur.predict_device(x.data_ptr(), n, y_f.data_ptr())
+        sur.predict_device(x.data_ptr(), n, y_l.data_ptr(), layered=True)
+        torch.cuda.synchronize()
+        a, b = y_f.cpu().numpy(), y_l.cpu().numpy()
+        assert np.all(np.isfinite(a)), n
+        assert np.array_equal(a, b), (n, np.abs(a - b).max())
+    # against the FP64 forward with the FP32 master weights on the same bf16
+    # inputs: the GPU rounds weights and activations to bf16 (8-bit mantissa)
+    p = sur.parameters()
+    xin = mo.bf16_bits_to_float(sur.feature_rows(hf))[:, :9]
+    y_ref, _ = mo.forward(p, xin)
+    err = np.abs(sur.predict(hf) - y_ref)
+    assert err.max() < 5e-3 and err.mean() < 1e-3, (err.max(), err.mean())
