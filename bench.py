@@ -207,6 +207,17 @@ def cpu_kind():
     return "reference" if orc.reference_available() else "port"
 
 
+def cpu_model():
+    """The host CPU's model name (/proc/cpuinfo), for the baseline record."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -236,7 +247,7 @@ def reference_arm(args):
         "config": {"workload": WORKLOAD, "options": N_OPT, "paths": PATHS, "steps": STEPS,
                    "cpu_sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "sample": sample},
+                         "cpu_model": cpu_model(), "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "prices_per_sec": value / (PATHS * STEPS),
     }
@@ -430,7 +441,10 @@ def main_gpu(args):
         cs = cres["samples"][0]
         cpu_value = cs["path_steps"] / cs["seconds"]
         cpu = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": cpu_kind(),
+               "cpu_model": cpu_model(),
                "sample": f"64 options x {cres['paths']} paths x {STEPS} steps of the workload"}
+        c1 = run_cpu(cpu_kind(), 1, seconds=4.0)["samples"][0]
+        cpu["value_1_core"] = c1["path_steps"] / c1["seconds"]
     except Exception as exc:  # the CPU baseline never blocks the GPU line
         cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": cpu_kind(),
                "sample": f"failed: {exc}"[:200]}

@@ -184,6 +184,22 @@ QK_EXPORT int32_t qk_cf_heston_price_cf_batch(
     const double* rho, const int32_t* option_type, const int32_t* integration_steps,
     const double* integration_limit, int32_t n, double* out_prices);
 
+/* qk_api.h:463-468 (cos_method.cpp:30-58: Fang-Oosterlee COS expansion with
+ * the Heston log-price characteristic function, n_terms cosine terms on
+ * [c1 -/+ truncation_width sqrt(max(v0, theta) t)]; FP64 on the GPU, one CTA
+ * per option) */
+QK_EXPORT double qk_ftm_cos_fang_oosterlee_heston_price(double spot, double strike, double t,
+                                                        double r, double q, double v0,
+                                                        double kappa, double theta, double sigma,
+                                                        double rho, int32_t option_type,
+                                                        int32_t n_terms, double truncation_width);
+/* qk_api.h:498-505 */
+QK_EXPORT int32_t qk_ftm_cos_fang_oosterlee_heston_price_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* n_terms,
+    const double* truncation_width, int32_t n, double* out_prices);
+
 /* ======================================================================= *
  * Part 2 -- additions in ABI 2.13 (no counterpart in the reference)
  * ======================================================================= */

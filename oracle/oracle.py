@@ -54,6 +54,8 @@ class Oracle:
             "qko_bsm_family_batch": (None, [I32] + [PD] * 6 + [PI32, PI32, PI32, PU64, I32, PD, PD]),
             "qko_bsm_price": (D, [D] * 6 + [I32]),
             "qko_heston_cf_price": (D, [D] * 10 + [I32, I32, D]),
+            "qko_heston_cos_price": (D, [D] * 10 + [I32, I32, D]),
+            "qko_heston_cos_error_scale": (D, [D] * 10 + [I32, I32, D]),
             "qko_normals": (None, [U64, I32, PD]),
             "qko_philox4x32_10": (None, [PU32, PU32, PU32]),
             "qko_philox_normals4": (None, [U64, U32, U32, U32, PD]),
@@ -147,6 +149,18 @@ class Oracle:
         return self.lib.qko_heston_cf_price(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
                                             option_type, integration_steps, integration_limit)
 
+    def heston_cos(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                   n_terms=256, truncation_width=10.0):
+        return self.lib.qko_heston_cos_price(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                                             option_type, n_terms, truncation_width)
+
+    def heston_cos_error_scale(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
+                               option_type, n_terms=256, truncation_width=10.0):
+        """First-order rounding-error scale of the COS price: exp(-r t) sum_k
+        |term_k| (1 + size of term k's exponent parts before they cancel)."""
+        return self.lib.qko_heston_cos_error_scale(spot, strike, t, r, q, v0, kappa, theta, sigma,
+                                               rho, option_type, n_terms, truncation_width)
+
     # -- streams ------------------------------------------------------------------
     def normals(self, seed, n):
         out = np.empty(n)
@@ -210,6 +224,7 @@ class Reference:
             "qk_cf_black_scholes_merton_price": (D, [D] * 6 + [I32]),
             "qk_cf_heston_price_cf": (D, [D] * 10 + [I32, I32, D]),
             "qk_cf_heston_price_cf_batch": (I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
+            "qk_ftm_cos_fang_oosterlee_heston_price": (D, [D] * 10 + [I32, I32, D]),
             "qk_mcm_control_variates_price": (D, term),
             "qk_mcm_stratified_sampling_price": (D, term),
             "qk_mcm_importance_sampling_price": (D, [D] * 6 + [I32, I32, D, U64]),
@@ -307,6 +322,12 @@ class Reference:
                   integration_steps=1024, integration_limit=120.0):
         return self.lib.qk_cf_heston_price_cf(spot, strike, t, r, q, v0, kappa, theta, sigma, rho,
                                               option_type, integration_steps, integration_limit)
+
+    def heston_cos(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                   n_terms=256, truncation_width=10.0):
+        return self.lib.qk_ftm_cos_fang_oosterlee_heston_price(
+            spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type, n_terms,
+            truncation_width)
 
     def heston_cf_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
                         integration_steps, integration_limit):

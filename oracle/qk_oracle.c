@@ -813,6 +813,115 @@ double qko_heston_cf_price(double spot, double strike, double t, double r, doubl
     return call - spot * exp(-q * t) + strike * exp(-r * t);
 }
 
+/* cos_method.cpp:30-58 (Heston COS, Fang-Oosterlee) with the Heston log-price
+ * characteristic function of charfn_concepts.h:54-78 and the sum of
+ * cos_method.h:13-57, in the same expression order. */
+static double complex heston_log_charfn(double spot, double r, double q, double v0, double kappa,
+                                        double theta, double sigma, double rho, double complex u,
+                                        double t, double* mag) {
+    const double complex i = CMPLX(0.0, 1.0);
+    const double complex iu = i * u;
+    const double complex a = kappa - rho * sigma * iu;
+    const double complex b = sigma * sigma * (iu + u * u);
+    const double complex d = csqrt(a * a + b);
+    const double complex g = (a - d) / (a + d);
+    const double complex edt = cexp(-d * t);
+    const double complex lg = clog((1.0 - g * edt) / (1.0 - g));
+    const double complex C = (kappa * theta / (sigma * sigma)) * ((a - d) * t - 2.0 * lg);
+    const double complex D = ((a - d) / (sigma * sigma)) * (1.0 - edt) / (1.0 - g * edt);
+    if (mag) {
+        /* Sizes of the exponent's parts before they cancel.  a - d is a
+         * difference of two numbers of size |a| + |d|, so its rounding error
+         * is of that size, and 1/sigma^2 carries it into C and D. */
+        const double ad = cabs(a) + cabs(d);
+        *mag = cabs(u) * (fabs(log(spot)) + fabs((r - q) * t)) +
+               fabs(kappa * theta / (sigma * sigma)) * (ad * t + 2.0 * (cabs(lg) + 1.0)) +
+               fabs(v0) * ad / (sigma * sigma) * cabs(1.0 - edt) / cabs(1.0 - g * edt);
+    }
+    return cexp(iu * log(spot) + iu * (r - q) * t + C + D * v0);
+}
+
+/* The COS price, and in *err_scale (when not NULL) a first-order scale of its
+ * rounding error: exp(-r t) sum_k |w_k f_k u_k| (1 + M_k), M_k the size of
+ * term k's exponent parts (and of its phase u a) before they cancel.  An
+ * absolute error e in an exponent is a relative error e in its exp(), so
+ * another correctly working evaluation (other libm, other summation order)
+ * lands within a modest multiple of DBL_EPSILON x this scale. */
+static double heston_cos_impl(double spot, double strike, double t, double r, double q, double v0,
+                              double kappa, double theta, double sigma, double rho, int32_t ot,
+                              int32_t n_terms, double truncation_width, double* err_scale);
+
+double qko_heston_cos_price(double spot, double strike, double t, double r, double q, double v0,
+                            double kappa, double theta, double sigma, double rho, int32_t ot,
+                            int32_t n_terms, double truncation_width) {
+    return heston_cos_impl(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, ot, n_terms,
+                           truncation_width, NULL);
+}
+
+double qko_heston_cos_error_scale(double spot, double strike, double t, double r, double q,
+                              double v0, double kappa, double theta, double sigma, double rho,
+                              int32_t ot, int32_t n_terms, double truncation_width) {
+    double a = 0.0;
+    heston_cos_impl(spot, strike, t, r, q, v0, kappa, theta, sigma, rho, ot, n_terms,
+                    truncation_width, &a);
+    return a;
+}
+
+static double heston_cos_impl(double spot, double strike, double t, double r, double q, double v0,
+                              double kappa, double theta, double sigma, double rho, int32_t ot,
+                              int32_t n_terms, double truncation_width, double* err_scale) {
+    if (!valid_option_type(ot)) return qko_nan();
+    if (!qko_finite(spot) || !qko_finite(strike) || !qko_finite(t) || !qko_finite(r) ||
+        !qko_finite(q) || !qko_finite(v0) || !qko_finite(kappa) || !qko_finite(theta) ||
+        !qko_finite(sigma) || !qko_finite(rho) || !qko_finite(truncation_width))
+        return qko_nan();
+    if (spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0) return qko_nan();
+    if (t <= QKO_EPS) return intrinsic(spot, strike, ot);
+    if (n_terms < 8 || truncation_width <= 0.0) return qko_nan();
+    const double eff_var = smax(v0, theta);
+    const double c1 = log(spot) + (r - q - 0.5 * eff_var) * t;
+    const double c2 = eff_var * t;
+    const double a = c1 - truncation_width * sqrt(smax(c2, 0.0));
+    const double b = c1 + truncation_width * sqrt(smax(c2, 0.0));
+    if (!(b > a + QKO_EPS)) return qko_nan();
+    const double log_strike = log(strike);
+    const double c = (log_strike < a ? a : log_strike) > b ? b : (log_strike < a ? a : log_strike);
+    const double dd = b;
+    double call = 0.0;
+    if (c < dd) {
+        const double interval = b - a;
+        const double inv = 1.0 / interval;
+        double sum = 0.0;
+        for (int32_t k = 0; k < n_terms; ++k) {
+            const double u = (double)k * M_PI * inv;
+            double chi, psi;
+            if (k == 0) {
+                chi = exp(dd) - exp(c);
+                psi = dd - c;
+            } else {
+                const double ud = u * (dd - a), uc = u * (c - a);
+                const double exp_d = exp(dd), exp_c = exp(c);
+                chi = ((cos(ud) * exp_d - cos(uc) * exp_c) + u * (sin(ud) * exp_d - sin(uc) * exp_c)) /
+                      (1.0 + u * u);
+                psi = (sin(ud) - sin(uc)) / u;
+            }
+            const double u_k = 2.0 * inv * (chi - strike * psi);
+            double mag = 0.0;
+            const double complex phi = heston_log_charfn(spot, r, q, v0, kappa, theta, sigma, rho,
+                                                         CMPLX(u, 0.0), t, err_scale ? &mag : NULL);
+            const double f_k = creal(phi * cexp(-CMPLX(0.0, 1.0) * (u * a)));
+            const double weight = (k == 0) ? 0.5 : 1.0;
+            sum += weight * f_k * u_k;
+            if (err_scale) *err_scale += fabs(weight * f_k * u_k) * (1.0 + mag + fabs(u * a));
+        }
+        call = exp(-r * t) * sum;
+        if (err_scale) *err_scale *= exp(-r * t);
+    }
+    call = smax(0.0, call);
+    if (ot == QKO_CALL) return call;
+    return call - spot * exp(-q * t) + strike * exp(-r * t);
+}
+
 /* ===================================================================== *
  * 3. Philox replay.
  *

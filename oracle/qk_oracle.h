@@ -111,6 +111,15 @@ double qko_heston_cf_price(double spot, double strike, double t, double r, doubl
                            int32_t option_type, int32_t integration_steps,
                            double integration_limit);
 
+/* cos_method.cpp:30-58: Heston price by the Fang-Oosterlee COS expansion. */
+double qko_heston_cos_price(double spot, double strike, double t, double r, double q,
+                            double v0, double kappa, double theta, double sigma, double rho,
+                            int32_t option_type, int32_t n_terms, double truncation_width);
+/* First-order rounding-error scale of the COS price (defined in qk_oracle.c). */
+double qko_heston_cos_error_scale(double spot, double strike, double t, double r, double q,
+                              double v0, double kappa, double theta, double sigma, double rho,
+                              int32_t option_type, int32_t n_terms, double truncation_width);
+
 /* ---- 3. Philox replay of the GPU stream --------------------------------- */
 void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 /* The GPU's normal with index k of stream (seed, c0, c1, c3); see qk_oracle.c. */

@@ -1,5 +1,6 @@
-// cf_kernels.cu -- batch Heston characteristic-function pricer on the GPU.
+// cf_kernels.cu -- batch Heston Fourier pricers on the GPU.
 //
+// 1. Characteristic-function price (heston_cf_kernel):
 // Restates yluoc/Quant-Kernel closed_form_semi_analytical/heston/heston.cpp:7-53
 // (little-trap characteristic function) and the P1/P2 integration of
 // closed_form_semi_analytical/common/internal_util.h:80-142:
@@ -9,6 +10,12 @@
 // fixed order, so results are deterministic.  The rule's nodes and weights are
 // computed on the host (Newton on the Legendre recurrence) and held in
 // constant memory.
+//
+// 2. COS expansion (heston_cos_kernel): yluoc/Quant-Kernel
+// fourier_transform_methods/cos_method/cos_method.cpp:30-58 with the
+// log-price characteristic function of common/charfn_concepts.h:54-78 and
+// the cosine sum of cos_method.h:13-57: n_terms terms on [a, b], one CTA per
+// option, terms round-robin over the threads, FP64, fixed-order reduction.
 #include "cf_kernels.h"
 
 #include <cmath>
@@ -182,6 +189,107 @@ __global__ void __launch_bounds__(128)
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// COS expansion.  Complex arithmetic in the reference's expression order
+// (std::complex products and real-complex mixes), so the terms agree with the
+// reference's to rounding.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ Cx cmul(Cx a, Cx b) {
+    return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
+}
+// real - complex as std::complex does it: (x - re, 0 - im)
+__device__ __forceinline__ Cx rsub(double x, Cx a) { return cx(x - a.re, 0.0 - a.im); }
+__device__ __forceinline__ Cx scale(Cx a, double s) { return cx(a.re * s, a.im * s); }
+
+struct HestonLogCf {
+    double spot_log, r, q, v0, kappa, theta, sigma, rho;
+    // charfn_concepts.h:57-77: phi(u, t) of log S_t
+    __device__ __noinline__ Cx operator()(Cx u, double t) const {
+        const Cx iu = cmul(cx(0.0, 1.0), u);
+        const Cx rs_iu = scale(iu, rho * sigma);
+        const Cx a = rsub(kappa, rs_iu);
+        const Cx b = scale(iu + cmul(u, u), sigma * sigma);
+        const Cx d = csqrt_(cmul(a, a) + b);
+        const Cx amd = a - d;
+        const Cx g = amd / (a + d);
+        const Cx edt = cexp_(scale(cx(-d.re, -d.im), t));
+        const Cx lg = clog_(rsub(1.0, cmul(g, edt)) / rsub(1.0, g));
+        const Cx C = scale(scale(amd, t) - scale(lg, 2.0), kappa * theta / (sigma * sigma));
+        const Cx D = cmul(cx(amd.re / (sigma * sigma), amd.im / (sigma * sigma)), rsub(1.0, edt)) /
+                     rsub(1.0, cmul(g, edt));
+        return cexp_(scale(iu, spot_log) + scale(scale(iu, r - q), t) + C + scale(D, v0));
+    }
+};
+
+__global__ void __launch_bounds__(128)
+    heston_cos_kernel(const CfOption* __restrict__ opts, int32_t n, double* __restrict__ out) {
+    __shared__ double ss[128];
+    const int32_t i = blockIdx.x;
+    if (i >= n) return;
+    const CfOption o = opts[i];
+    if (o.mode != 0) {
+        if (threadIdx.x == 0) out[i] = o.const_price;
+        return;
+    }
+    const double kPi = 3.1415926535897932384626433832795;
+    const double a = o.limit, b = o.hi;
+    const double lk = log(o.strike);
+    const double cm = lk < a ? a : lk;   // std::min(std::max(log K, a), b)
+    const double c = b < cm ? b : cm;
+    const double dd = b;
+    const bool summed = c < dd;
+    double s = 0.0;
+    if (summed) {
+        HestonLogCf phi;
+        phi.spot_log = log(o.spot);
+        phi.r = o.r;
+        phi.q = o.q;
+        phi.v0 = o.v0;
+        phi.kappa = o.kappa;
+        phi.theta = o.theta;
+        phi.sigma = o.sigma;
+        phi.rho = o.rho;
+        const double interval = b - a;
+        const double inv = 1.0 / interval;
+        const double exp_d = exp(dd), exp_c = exp(c);
+        for (int32_t k = threadIdx.x; k < o.panels; k += blockDim.x) {
+            const double u = static_cast<double>(k) * kPi * inv;
+            double chi, psi;
+            if (k == 0) {
+                chi = exp_d - exp_c;
+                psi = dd - c;
+            } else {
+                double sd, cd, sc, cc;
+                sincos(u * (dd - a), &sd, &cd);
+                sincos(u * (c - a), &sc, &cc);
+                chi = ((cd * exp_d - cc * exp_c) + u * (sd * exp_d - sc * exp_c)) / (1.0 + u * u);
+                psi = (sd - sc) / u;
+            }
+            const double u_k = 2.0 * inv * (chi - o.strike * psi);
+            const Cx f = phi(cx(u, 0.0), o.t);
+            // Re(phi * exp(-i u a)) = Re(phi * (cos ua, -sin ua))
+            double sa, ca;
+            sincos(u * a, &sa, &ca);
+            const double f_k = f.re * ca - f.im * (-sa);
+            const double weight = (k == 0) ? 0.5 : 1.0;
+            s += weight * f_k * u_k;
+        }
+    }
+    ss[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 64; off > 0; off >>= 1) {
+        if (threadIdx.x < off) ss[threadIdx.x] += ss[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double call = summed ? exp(-o.r * o.t) * ss[0] : 0.0;
+        call = (0.0 < call) ? call : 0.0;  // std::max(0.0, call): NaN -> 0
+        out[i] = o.option_type == 0 ? call
+                                    : call - o.spot * exp(-o.q * o.t) + o.strike * exp(-o.r * o.t);
+    }
+}
+
 // 64-point Gauss-Legendre nodes (the 32 positive ones) and weights.
 void gl64(double* x, double* w) {
     const int n = 64;
@@ -256,6 +364,58 @@ CfOption pack_cf_option(double spot, double strike, double t, double r, double q
     return o;
 }
 
+CfOption pack_cos_option(double spot, double strike, double t, double r, double q, double v0,
+                         double kappa, double theta, double sigma, double rho, int32_t ot,
+                         int32_t n_terms, double width) {
+    CfOption o;
+    std::memset(&o, 0, sizeof o);
+    o.method = kCfMethodCos;
+    o.mode = 1;
+    o.const_price = std::numeric_limits<double>::quiet_NaN();
+    // cos_method.cpp:38-48 (no range checks on kappa, theta, sigma, rho)
+    if (!(ot == 0 || ot == 1)) return o;
+    if (!finite_(spot) || !finite_(strike) || !finite_(t) || !finite_(r) || !finite_(q) ||
+        !finite_(v0) || !finite_(kappa) || !finite_(theta) || !finite_(sigma) || !finite_(rho) ||
+        !finite_(width))
+        return o;
+    if (spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0) return o;
+    if (t <= 1e-12) {
+        o.const_price = intrinsic_(spot, strike, ot);
+        return o;
+    }
+    if (n_terms < 8 || width <= 0.0) return o;
+    // cos_method.cpp:50-55: truncation interval from max(v0, theta)
+    const double eff_var = (v0 < theta) ? theta : v0;
+    const double c1 = std::log(spot) + (r - q - 0.5 * eff_var) * t;
+    const double c2 = eff_var * t;
+    const double half = width * std::sqrt((c2 < 0.0) ? 0.0 : c2);
+    const double a = c1 - half, b = c1 + half;
+    if (!(b > a + 1e-12)) return o;  // cos_method.h:22
+    o.mode = 0;
+    o.spot = spot;
+    o.strike = strike;
+    o.t = t;
+    o.r = r;
+    o.q = q;
+    o.v0 = v0;
+    o.kappa = kappa;
+    o.theta = theta;
+    o.sigma = sigma;
+    o.rho = rho;
+    o.limit = a;
+    o.hi = b;
+    o.option_type = ot;
+    o.panels = n_terms;
+    return o;
+}
+
+cudaError_t launch_heston_cos(const CfOption* d_opts, int32_t n, double* d_out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (cudaError_t e = injected_fault(kFaultLaunch)) return e;
+    heston_cos_kernel<<<n, 128, 0, st>>>(d_opts, n, d_out);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_heston_cf(const CfOption* d_opts, int32_t n, double* d_out, cudaStream_t st) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -318,9 +478,12 @@ cudaError_t heston_cf_price_host(const CfOption* h_opts, int32_t n, double* out)
     std::memcpy(s.h_opts.p, h_opts, ob);
     if ((e = cudaMemcpyAsync(s.d_opts.p, s.h_opts.p, ob, cudaMemcpyHostToDevice, s.st)) != cudaSuccess)
         return e;
-    if ((e = launch_heston_cf(static_cast<const CfOption*>(s.d_opts.p), n,
-                              static_cast<double*>(s.d_out.p), s.st)) != cudaSuccess)
-        return e;
+    e = h_opts[0].method == kCfMethodCos
+            ? launch_heston_cos(static_cast<const CfOption*>(s.d_opts.p), n,
+                                static_cast<double*>(s.d_out.p), s.st)
+            : launch_heston_cf(static_cast<const CfOption*>(s.d_opts.p), n,
+                               static_cast<double*>(s.d_out.p), s.st);
+    if (e != cudaSuccess) return e;
     if ((e = injected_fault(kFaultCopy)) != cudaSuccess) return e;
     if ((e = cudaMemcpyAsync(s.h_out.p, s.d_out.p, pb, cudaMemcpyDeviceToHost, s.st)) != cudaSuccess)
         return e;

@@ -642,6 +642,39 @@ int32_t qk_cf_heston_price_cf_batch(const double* spot, const double* strike, co
     return e == cudaSuccess ? QK_OK : fail_cuda(e, "qk_cf_heston_price_cf_batch");
 }
 
+// ---- Heston COS expansion ----------------------------------------------------------
+int32_t qk_ftm_cos_fang_oosterlee_heston_price_batch(
+    const double* spot, const double* strike, const double* t, const double* r, const double* q,
+    const double* v0, const double* kappa, const double* theta, const double* sigma,
+    const double* rho, const int32_t* option_type, const int32_t* n_terms,
+    const double* truncation_width, int32_t n, double* out_prices) {
+    const NamedPtr ptrs[] = {{spot, "spot"}, {strike, "strike"}, {t, "t"}, {r, "r"}, {q, "q"},
+                             {v0, "v0"}, {kappa, "kappa"}, {theta, "theta"}, {sigma, "sigma"},
+                             {rho, "rho"}, {option_type, "option_type"}, {n_terms, "n_terms"},
+                             {truncation_width, "truncation_width"}, {out_prices, "out_prices"}};
+    if (int32_t rc = check_nulls(ptrs)) return rc;
+    if (n <= 0) return fail_size(n);
+    std::vector<qkb::CfOption> recs(static_cast<size_t>(n));
+    for (int32_t i = 0; i < n; ++i)
+        recs[i] = qkb::pack_cos_option(spot[i], strike[i], t[i], r[i], q[i], v0[i], kappa[i],
+                                       theta[i], sigma[i], rho[i], option_type[i], n_terms[i],
+                                       truncation_width[i]);
+    cudaError_t e = qkb::heston_cf_price_host(recs.data(), n, out_prices);
+    return e == cudaSuccess ? QK_OK : fail_cuda(e, "qk_ftm_cos_fang_oosterlee_heston_price_batch");
+}
+
+double qk_ftm_cos_fang_oosterlee_heston_price(double spot, double strike, double t, double r,
+                                              double q, double v0, double kappa, double theta,
+                                              double sigma, double rho, int32_t option_type,
+                                              int32_t n_terms, double truncation_width) {
+    double out = nan_value();
+    if (qk_ftm_cos_fang_oosterlee_heston_price_batch(&spot, &strike, &t, &r, &q, &v0, &kappa,
+                                                     &theta, &sigma, &rho, &option_type, &n_terms,
+                                                     &truncation_width, 1, &out) != QK_OK)
+        return nan_value();
+    return out;
+}
+
 double qk_cf_heston_price_cf(double spot, double strike, double t, double r, double q, double v0,
                              double kappa, double theta, double sigma, double rho,
                              int32_t option_type, int32_t integration_steps,

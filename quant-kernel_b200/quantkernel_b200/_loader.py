@@ -90,6 +90,8 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_quasi_monte_carlo_halton_price_batch", I32, _qmc_batch),
     ("qk_mcm_quasi_monte_carlo_halton_price_se_batch", I32, _qmc_batch + [PD]),
     ("qk_cf_heston_price_cf", D, [D] * 10 + [I32, I32, D]),
+    ("qk_ftm_cos_fang_oosterlee_heston_price", D, [D] * 10 + [I32, I32, D]),
+    ("qk_ftm_cos_fang_oosterlee_heston_price_batch", I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
     ("qk_cf_heston_price_cf_batch", I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
     ("qk_mcm_mixed_price_batch", I32, _mixed_arrays + [PD, PD]),
     ("qk_mcm_plan_create", I32, _mixed_arrays + [I32, ct.POINTER(VP)]),

@@ -57,6 +57,7 @@ class QuantAccelerator:
         "quasi_monte_carlo_sobol_price": "quasi_monte_carlo_sobol_price_batch",
         "quasi_monte_carlo_halton_price": "quasi_monte_carlo_halton_price_batch",
         "heston_price_cf": "heston_price_cf_batch",
+        "cos_method_fang_oosterlee_heston_price": "cos_method_fang_oosterlee_heston_price_batch",
     }
 
     # Monte Carlo methods that the mixed-model launch can price together
@@ -103,7 +104,7 @@ class QuantAccelerator:
             return "native_batch"
         raise RuntimeError(f"backend='{self.backend}' not supported for method '{method}' "
                            f"(quantkernel_b200 implements the Monte Carlo path and the Heston "
-                           f"characteristic-function pricer)")
+                           f"characteristic-function and COS pricers)")
 
     def _scalar_defaults(self, method: str) -> dict[str, Any]:
         d = self._defaults.get(method)
@@ -144,8 +145,8 @@ class QuantAccelerator:
 
         All Monte Carlo jobs go into one mixed-model batch -- one persistent
         work-stealing launch over every option's tiles, so a few long Heston
-        jobs and many short terminal ones finish together; Heston
-        characteristic-function jobs go into one batch call.  Results come
+        jobs and many short terminal ones finish together; the Heston Fourier
+        jobs go into one batch call per method.  Results come
         back in request order; with ``with_stderr`` a second array holds the
         Monte Carlo standard errors (NaN for closed-form jobs).
         """
@@ -154,14 +155,18 @@ class QuantAccelerator:
         stderr = np.full(n, np.nan)
         if n == 0:
             return (prices, stderr) if with_stderr else prices
-        mc_idx, cf_idx = [], []
+        mc_idx: list[int] = []
+        fourier_idx: dict[str, list[int]] = {}
         for i, (method, _) in enumerate(requests):
             if not hasattr(self.qk, method):
                 raise AttributeError(f"Unknown method: {method}")
             self.suggest_strategy(method, 1)
-            (mc_idx if method in self._MIXED_MODELS else cf_idx).append(i)
-        if cf_idx:
-            prices[cf_idx] = self.price_batch("heston_price_cf", [requests[i][1] for i in cf_idx])
+            if method in self._MIXED_MODELS:
+                mc_idx.append(i)
+            else:
+                fourier_idx.setdefault(method, []).append(i)
+        for method, idx in fourier_idx.items():
+            prices[idx] = self.price_batch(method, [requests[i][1] for i in idx])
         if mc_idx:
             m = len(mc_idx)
             cols = {k: np.zeros(m) for k in ("spot", "strike", "t", "vol", "r", "q", "v0",

@@ -538,6 +538,35 @@ class QuantKernel:
         self._check_same_length(s.shape[0], **arrs)
         return self._call_batch_ctypes("qk_cf_heston_price_cf_batch", s, *arrs.values())
 
+    def cos_method_fang_oosterlee_heston_price(self, spot: float, strike: float, t: float,
+                                               r: float, q: float, v0: float, kappa: float,
+                                               theta: float, sigma: float, rho: float,
+                                               option_type: int, n_terms: int = 256,
+                                               truncation_width: float = 10.0) -> float:
+        """Heston price by the COS expansion (cos_method.cpp:30-58; engine.py:742-750)."""
+        return self._call_checked("qk_ftm_cos_fang_oosterlee_heston_price", spot, strike, t, r, q,
+                                  v0, kappa, theta, sigma, rho, option_type, n_terms,
+                                  truncation_width)
+
+    def cos_method_fang_oosterlee_heston_price_batch(self, spot, strike, t, r, q, v0, kappa,
+                                                     theta, sigma, rho, option_type, n_terms,
+                                                     truncation_width) -> np.ndarray:
+        """Batch of the COS pricer on the GPU, one CTA per option (engine.py:752-778)."""
+        s = self._as_f64_array(spot, "spot")
+        arrs = dict(
+            strike=self._as_f64_array(strike, "strike"), t=self._as_f64_array(t, "t"),
+            r=self._as_f64_array(r, "r"), q=self._as_f64_array(q, "q"),
+            v0=self._as_f64_array(v0, "v0"), kappa=self._as_f64_array(kappa, "kappa"),
+            theta=self._as_f64_array(theta, "theta"), sigma=self._as_f64_array(sigma, "sigma"),
+            rho=self._as_f64_array(rho, "rho"),
+            option_type=self._as_i32_array(option_type, "option_type"),
+            n_terms=self._as_i32_array(n_terms, "n_terms"),
+            truncation_width=self._as_f64_array(truncation_width, "truncation_width"),
+        )
+        self._check_same_length(s.shape[0], **arrs)
+        return self._call_batch_ctypes("qk_ftm_cos_fang_oosterlee_heston_price_batch", s,
+                                       *arrs.values())
+
     # ------------------------------------------------------------------ mixed / plans
     def _mixed_arrays(self, model, spot, strike, t, vol, r, q, v0, kappa, theta, sigma, rho,
                       option_type, paths, steps, seed):

@@ -242,12 +242,60 @@ def main() -> None:
                integration_steps=int(rng_w.choice([16, 64, 200, 512, 1024, 2048])),
                integration_limit=float(rng_w.choice([30.0, 120.0, 300.0])))
 
+    # Heston COS expansion (cos_method.cpp:30-58): settings, entry checks and
+    # the degenerate parameters the COS entry does not reject
+    cos = []
+
+    def add_cos(**kw):
+        a = dict(spot=100.0, strike=100.0, t=1.0, r=0.03, q=0.01, v0=0.04, kappa=2.0,
+                 theta=0.04, sigma=0.3, rho=-0.7, option_type=0, n_terms=256,
+                 truncation_width=10.0)
+        a.update(kw)
+        cos.append({"args": {k: (hx(v) if isinstance(v, float) else int(v)) for k, v in a.items()},
+                    "price": hx(ref.heston_cos(**a))})
+
+    rng_cos = np.random.default_rng(20261207)
+    for _ in range(60):
+        add_cos(spot=float(rng_cos.uniform(50, 150)), strike=float(rng_cos.uniform(40, 200)),
+                t=float(rng_cos.uniform(0.02, 5)), r=float(rng_cos.uniform(-0.01, 0.08)),
+                q=float(rng_cos.uniform(0, 0.05)), v0=float(rng_cos.uniform(0, 0.3)),
+                kappa=float(rng_cos.uniform(0.05, 8)), theta=float(rng_cos.uniform(0, 0.3)),
+                sigma=float(rng_cos.uniform(0.02, 2)), rho=float(rng_cos.uniform(-0.99, 0.99)),
+                option_type=int(rng_cos.integers(0, 2)),
+                n_terms=int(rng_cos.choice([8, 16, 64, 128, 256, 512, 1024])),
+                truncation_width=float(rng_cos.choice([2.0, 6.0, 10.0, 14.0])))
+    for ot in (0, 1):  # the reference's own case (test_heston_fourier.py:18-21)
+        add_cos(option_type=ot)
+    add_cos(n_terms=7)                    # < 8 -> NaN
+    add_cos(truncation_width=0.0)         # <= 0 -> NaN
+    add_cos(truncation_width=-1.0)
+    add_cos(option_type=2)
+    add_cos(t=1e-14, spot=110.0)          # intrinsic
+    add_cos(t=0.0, spot=90.0, option_type=1)
+    add_cos(t=-0.1)
+    add_cos(spot=0.0)
+    add_cos(v0=-0.01)
+    add_cos(v0=0.0)
+    add_cos(v0=0.0, theta=0.0)            # empty interval -> NaN
+    add_cos(sigma=0.0)                    # NaN sum -> max(0, NaN) = 0
+    add_cos(sigma=0.0, option_type=1)
+    add_cos(kappa=0.0)
+    add_cos(kappa=-1.0)
+    add_cos(rho=1.0)
+    add_cos(rho=-1.0)
+    add_cos(sigma=-0.3)
+    add_cos(r=float("nan"))
+    add_cos(truncation_width=float("inf"))
+    add_cos(strike=1000.0)                # log K beyond b: no sum, call 0
+    add_cos(strike=1.0, option_type=1)
+
     doc = {
         "source": "yluoc/Quant-Kernel C ABI, compiled from cpp/src by oracle/Makefile (ref)",
         "generator": "tests/golden/make_golden.py",
         "mc_cases": cases,
         "heston_cf": cf,
         "heston_cf_edges": cf_edges,
+        "heston_cos": cos,
         "bsm_cf_reference_as_cdf": bsm,
     }
     OUT.write_text(json.dumps(doc, indent=1))

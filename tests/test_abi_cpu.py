@@ -44,6 +44,7 @@ def test_drop_in_signatures_match_reference_subset():
         "qk_mcm_quasi_monte_carlo_sobol_price", "qk_mcm_quasi_monte_carlo_sobol_price_batch",
         "qk_mcm_quasi_monte_carlo_halton_price", "qk_mcm_quasi_monte_carlo_halton_price_batch",
         "qk_cf_heston_price_cf", "qk_cf_heston_price_cf_batch",
+        "qk_ftm_cos_fang_oosterlee_heston_price", "qk_ftm_cos_fang_oosterlee_heston_price_batch",
         "qk_mcm_standard_monte_carlo_price", "qk_mcm_standard_monte_carlo_price_batch",
         "qk_mcm_antithetic_variates_price", "qk_mcm_antithetic_variates_price_batch",
         "qk_mcm_euler_maruyama_price", "qk_mcm_euler_maruyama_price_batch",
@@ -100,6 +101,8 @@ BATCHES = {
     "qk_cf_heston_price_cf_batch":
         "spot strike t r q v0 kappa theta sigma rho option_type integration_steps "
         "integration_limit",
+    "qk_ftm_cos_fang_oosterlee_heston_price_batch":
+        "spot strike t r q v0 kappa theta sigma rho option_type n_terms truncation_width",
     "qk_mcm_control_variates_price_batch": "spot strike t vol r q option_type paths seed",
     "qk_mcm_stratified_sampling_price_batch": "spot strike t vol r q option_type paths seed",
     "qk_mcm_importance_sampling_price_batch":
@@ -108,7 +111,7 @@ BATCHES = {
     "qk_mcm_quasi_monte_carlo_halton_price_batch": "spot strike t vol r q option_type paths",
 }
 MC_BATCHES = sorted(k for k in BATCHES if k.startswith("qk_mcm_"))
-INT_ARGS = {"option_type", "paths", "steps", "integration_steps"}
+INT_ARGS = {"option_type", "paths", "steps", "integration_steps", "n_terms"}
 
 
 def _call(qk, fn, names, null=None, n=1, out=True, se=None):

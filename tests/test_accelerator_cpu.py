@@ -22,7 +22,7 @@ MC_METHODS = [
 
 def test_native_batch_for_every_supported_method(qk):
     accel = QuantAccelerator(qk=qk, backend="gpu")
-    for m in MC_METHODS + ["heston_price_cf"]:
+    for m in MC_METHODS + ["heston_price_cf", "cos_method_fang_oosterlee_heston_price"]:
         assert accel.suggest_strategy(m, 1) == "native_batch"
         assert accel.suggest_strategy(m, 100000) == "native_batch"
         assert hasattr(qk, accel._NATIVE_BATCH_METHODS[m])
@@ -61,6 +61,8 @@ def test_job_columns_take_scalar_defaults(qk):
     assert cols["seed"] == [42]
     cf = accel._columns("heston_price_cf", [{"spot": 100.0}])
     assert cf["integration_steps"] == [1024] and cf["integration_limit"] == [120.0]
+    cos = accel._columns("cos_method_fang_oosterlee_heston_price", [{"spot": 100.0}])
+    assert cos["n_terms"] == [256] and cos["truncation_width"] == [10.0]
 
 
 def test_no_gpu_raises_instead_of_cpu_result(qk):

@@ -9,6 +9,8 @@ from quantkernel_b200 import QK_CALL, QK_PUT, QuantAccelerator
 
 pytestmark = pytest.mark.gpu
 
+FOURIER = ("heston_price_cf", "cos_method_fang_oosterlee_heston_price")
+
 
 def _jobs(method, n, rng):
     out = []
@@ -16,14 +18,15 @@ def _jobs(method, n, rng):
         j = dict(spot=float(rng.uniform(90, 110)), strike=float(rng.uniform(90, 110)),
                  t=float(rng.uniform(0.25, 1.5)), r=float(rng.uniform(0.0, 0.05)),
                  q=float(rng.uniform(0.0, 0.02)), option_type=QK_CALL if i % 2 == 0 else QK_PUT)
-        heston = method in ("heston_monte_carlo_price", "heston_lr_delta", "heston_price_cf")
+        heston = method in ("heston_monte_carlo_price", "heston_lr_delta", "heston_price_cf",
+                            "cos_method_fang_oosterlee_heston_price")
         if heston:
             j.update(v0=float(rng.uniform(0.02, 0.08)), kappa=float(rng.uniform(1, 3)),
                      theta=float(rng.uniform(0.02, 0.08)), sigma=float(rng.uniform(0.2, 0.6)),
                      rho=float(rng.uniform(-0.8, -0.2)))
         else:
             j["vol"] = float(rng.uniform(0.15, 0.4))
-        if method != "heston_price_cf":
+        if method not in FOURIER:
             j["paths"] = int(rng.integers(2000, 20000))
             if method not in ("quasi_monte_carlo_sobol_price", "quasi_monte_carlo_halton_price"):
                 j["seed"] = int(rng.integers(0, 2**40))
@@ -70,7 +73,7 @@ def test_price_many_mixed_launch_equals_per_method_batches(qk):
         # double-double sums make results independent of the launch shape up to
         # the final rounding; the control-variate moments are plain FP64
         np.testing.assert_allclose(prices[idx], want, rtol=1e-13, atol=0, err_msg=method)
-        if method == "heston_price_cf":
+        if method in FOURIER:
             assert np.all(np.isnan(se[idx]))
         else:
             assert np.all(se[idx] >= 0), method

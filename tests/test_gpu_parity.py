@@ -141,3 +141,18 @@ def test_fixture_edge_cases_on_gpu(qk, oracle):
         assert (math.isnan(got[0]) and math.isnan(want)) or got[0] == want, (case, got[0], want)
         checked += 1
     assert checked >= 40
+
+
+def test_full_heston_benchmark_vs_reference_cpu_mc(qk):
+    """Every one of the benchmark's 1024 Heston prices (262144 paths x 200
+    steps) against the reference's own CPU Monte Carlo on the same inputs
+    (tests/golden/heston_full_reference.json, produced by the oracle that equals
+    the reference bit for bit): z = difference / combined SE."""
+    import json
+    from pathlib import Path
+
+    doc = json.loads((Path(__file__).parent / "golden" / "heston_full_reference.json").read_text())
+    ref_p = np.array([float.fromhex(x) for x in doc["price"]])
+    ref_se = np.array([float.fromhex(x) for x in doc["stderr"]])
+    p, se = qk.heston_monte_carlo_price_se_batch(**workloads.heston())
+    _check(_z(p, ref_p, np.hypot(se, ref_se)), "Heston benchmark workload GPU vs reference CPU MC")

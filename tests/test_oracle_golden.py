@@ -84,6 +84,37 @@ def test_heston_cf_edges_match_reference(oracle, i):
         assert abs(got - want) < 1e-8 * max(1.0, abs(want)), (a, got, want)
 
 
+@pytest.mark.parametrize("i", range(len(GOLDEN["heston_cos"])))
+def test_heston_cos_matches_reference_bitwise(oracle, i):
+    """The COS restatement (cos_method.cpp:30-58) equals the reference bit for
+    bit: same characteristic-function expression order, same sequential sum,
+    including its NaN and max(0, NaN) = 0 outcomes on degenerate inputs."""
+    case = GOLDEN["heston_cos"][i]
+    a = _args(case["args"])
+    want = float.fromhex(case["price"])
+    got = oracle.heston_cos(**a)
+    assert _same(got, want), (a, got, want)
+    # the rounding scale the GPU parity bar uses bounds the call price it sums to
+    s = oracle.heston_cos_error_scale(**a)
+    if a["option_type"] == 0 and math.isfinite(want) and want > 0.0 and s > 0.0:
+        assert s >= want * (1 - 1e-12), (a, s)
+
+
+def test_heston_cos_agrees_with_cf(oracle):
+    """Two independent Fourier methods of the reference agree on well-posed
+    inputs (the COS method is the CF oracle's independent check)."""
+    rng = np.random.default_rng(41)
+    for _ in range(40):
+        a = dict(spot=100.0, strike=float(rng.uniform(70, 130)), t=float(rng.uniform(0.25, 2)),
+                 r=float(rng.uniform(0, 0.05)), q=0.0, v0=float(rng.uniform(0.01, 0.09)),
+                 kappa=float(rng.uniform(0.5, 5)), theta=float(rng.uniform(0.01, 0.09)),
+                 sigma=float(rng.uniform(0.1, 1.0)), rho=float(rng.uniform(-0.9, 0.0)),
+                 option_type=int(rng.integers(0, 2)))
+        cf = oracle.heston_cf(**a, integration_steps=4096, integration_limit=300.0)
+        cos = oracle.heston_cos(**a, n_terms=1024, truncation_width=12.0)
+        assert abs(cf - cos) < 2e-4, (a, cf, cos)
+
+
 def test_heston_cf_converged_and_small_volvol_limit(oracle):
     base = dict(spot=100.0, strike=105.0, t=1.0, r=0.03, q=0.01, v0=0.04, kappa=1.5,
                 theta=0.04, sigma=1e-4, rho=-0.5, option_type=0)
