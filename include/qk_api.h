@@ -380,10 +380,16 @@ QK_EXPORT int32_t qk_sur_gemm_bf16(const void* a, const void* b, float* c, int32
  * activations, FP32 accumulation, FP32 master weights) from the features
  *   f = (S/K, T, r, q, v0, kappa, theta, sigma, rho)
  * to the Heston call price / S.  Inputs are normalised to [-1, 1] over the
- * training box [box_lo, box_hi] (a dimension with lo == hi maps to 0).  It is
+ * training box [box_lo, box_hi] (a dimension with lo == hi maps to 0).  The
+ * network learns a residual: price / S = base + MLP, with base the
+ * Black-Scholes call / S at the Heston mean variance over [0, T],
+ *   vbar = theta + (v0 - theta) (1 - exp(-kappa T)) / (kappa T),
+ * computed in FP64 from the raw features (targets given to set_dataset and
+ * gradients are price / S; the model subtracts the base itself).  It is
  * trained on the GPU by the library's own tcgen05 forward/backward GEMMs and
  * Adam kernels on labels the caller produces (normally this library's Heston
- * Monte Carlo).  All arrays are host arrays; features are row-major n x 9. */
+ * Monte Carlo).  Arrays are host arrays unless marked DEVICE; features are
+ * row-major n x 9. */
 typedef struct qk_sur_model qk_sur_model;
 
 QK_EXPORT int32_t qk_sur_heston_create(const double* box_lo, const double* box_hi, uint64_t seed,
@@ -399,18 +405,29 @@ QK_EXPORT int32_t qk_sur_heston_train(qk_sur_model* model, int32_t epochs, int32
 /* price / S for each row of features (no box check). */
 QK_EXPORT int32_t qk_sur_heston_predict(qk_sur_model* model, const double* features, int64_t n,
                                         double* out);
-/* Device-resident inference: x_rows = normalised bf16 rows [n][64] (DEVICE),
- * y = price / S (DEVICE, fp32); asynchronous on `stream` (NULL = model's). */
-QK_EXPORT int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows, int64_t n,
-                                               float* y, void* stream);
+/* Device-resident inference: x_rows = normalised bf16 rows [n][64] (DEVICE,
+ * 16-byte aligned), base = the rows' base (DEVICE, fp32; NULL only for a
+ * model loaded from a checkpoint without a base), y = price / S (DEVICE,
+ * fp32); asynchronous on `stream` (NULL = model's). */
+QK_EXPORT int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows,
+                                               const float* base, int64_t n, float* y,
+                                               void* stream);
 /* The same inference as three layer-by-layer GEMM launches per 65,536 rows
  * (activations round-trip through device memory): the reference the fused
  * kernel behind qk_sur_heston_predict_device is tested against (same bits). */
 QK_EXPORT int32_t qk_sur_heston_predict_device_layered(qk_sur_model* model, const void* x_rows,
-                                                       int64_t n, float* y, void* stream);
-/* Normalised bf16 rows [n][64] (HOST output buffer of n*64 uint16). */
+                                                       const float* base, int64_t n, float* y,
+                                                       void* stream);
+/* Normalised bf16 rows [n][64] (HOST output buffer of n*64 uint16) and, when
+ * out_base is not NULL, each row's base (n floats). */
 QK_EXPORT int32_t qk_sur_heston_features(qk_sur_model* model, const double* features, int64_t n,
-                                         void* out_rows);
+                                         void* out_rows, float* out_base);
+/* The same on the device: features n x 9 FP64 (DEVICE) -> rows [n][64] bf16
+ * (DEVICE, 16-byte aligned) and base (DEVICE, n floats), one launch,
+ * asynchronous on `stream` (NULL = model's).  Rows equal qk_sur_heston_features'
+ * bit for bit; the base can differ in the last FP32 bit (device exp/erfc). */
+QK_EXPORT int32_t qk_sur_heston_features_device(qk_sur_model* model, const double* features,
+                                                int64_t n, void* rows, float* base, void* stream);
 /* Loss (mean squared error) and its 134,401 gradients for one batch (n a
  * multiple of 128), without an update; replaces the model's dataset. */
 QK_EXPORT int32_t qk_sur_heston_gradients(qk_sur_model* model, const double* features,

@@ -2,10 +2,13 @@
 of its mean-squared-error gradients, in numpy.
 
 TEST INFRASTRUCTURE ONLY: the checker for the GPU's tcgen05 forward/backward
-kernels.  The reference library has no such network; this is the plain
-mathematics of the architecture the surrogate specifies.  Parameter order:
+kernels and for the residual's Black-Scholes base.  The reference library has
+no such network; this is the plain mathematics of the architecture the
+surrogate specifies.  Parameter order:
 W1[256][9], b1, W2[256][256], b2, W3[256][256], b3, w4[256], b4.
 """
+
+import math
 
 import numpy as np
 
@@ -64,6 +67,26 @@ def loss_and_grads(p, x, t):
     dz1 = (dz2 @ w["W2"]) * dsilu(z1)
     g["W1"], g["b1"] = dz1.T @ x, dz1.sum(0)
     return loss, pack(g)
+
+
+def bsm_mean_var_base(f):
+    """The residual's base for feature rows f (n x 9: S/K, T, r, q, v0, kappa,
+    theta, sigma, rho): the Black-Scholes call / S at the Heston mean variance
+    over [0, T], theta + (v0 - theta)(1 - exp(-kappa T))/(kappa T), in FP64."""
+    f = np.asarray(f, np.float64)
+    out = np.empty(f.shape[0])
+    for i, (m, T, r, q, v0, kappa, theta) in enumerate(f[:, :7]):
+        x = kappa * T
+        w = -math.expm1(-x) / x if x > 1e-12 else 1.0
+        vbar = max(theta + (v0 - theta) * w, 0.0)
+        sd = math.sqrt(vbar * T)
+        dq, dk = math.exp(-q * T), math.exp(-r * T) / m
+        if not sd > 1e-12:
+            out[i] = max(dq - dk, 0.0)
+            continue
+        d1 = (math.log(m) + (r - q) * T) / sd + 0.5 * sd
+        out[i] = dq * 0.5 * math.erfc(-d1 / math.sqrt(2.0)) - dk * 0.5 * math.erfc(-(d1 - sd) / math.sqrt(2.0))
+    return out
 
 
 def bf16_bits_to_float(bits):

@@ -137,36 +137,51 @@ int32_t qk_sur_heston_predict(qk_sur_model* model, const double* features, int64
     return sur_status(model->m.predict(features, n, out), "qk_sur_heston_predict");
 }
 
-int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows, int64_t n, float* y,
-                                     void* stream) {
+int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows, const float* base,
+                                     int64_t n, float* y, void* stream) {
     if (!model) return qkb::fail_null("model");
     if (!x_rows) return qkb::fail_null("x_rows");
+    if (!base && model->m.base_kind() != qkb::kSurBaseNone) return qkb::fail_null("base");
     if (!y) return qkb::fail_null("y");
     if (n <= 0) return qkb::fail_size(n);
-    return sur_status(model->m.predict_device(static_cast<const __nv_bfloat16*>(x_rows), n, y,
+    return sur_status(model->m.predict_device(static_cast<const __nv_bfloat16*>(x_rows), base, n, y,
                                               static_cast<cudaStream_t>(stream)),
                       "qk_sur_heston_predict_device");
 }
 
-int32_t qk_sur_heston_predict_device_layered(qk_sur_model* model, const void* x_rows, int64_t n,
-                                             float* y, void* stream) {
+int32_t qk_sur_heston_predict_device_layered(qk_sur_model* model, const void* x_rows,
+                                             const float* base, int64_t n, float* y, void* stream) {
     if (!model) return qkb::fail_null("model");
     if (!x_rows) return qkb::fail_null("x_rows");
+    if (!base && model->m.base_kind() != qkb::kSurBaseNone) return qkb::fail_null("base");
     if (!y) return qkb::fail_null("y");
     if (n <= 0) return qkb::fail_size(n);
-    return sur_status(model->m.predict_device(static_cast<const __nv_bfloat16*>(x_rows), n, y,
+    return sur_status(model->m.predict_device(static_cast<const __nv_bfloat16*>(x_rows), base, n, y,
                                               static_cast<cudaStream_t>(stream), true),
                       "qk_sur_heston_predict_device_layered");
 }
 
 int32_t qk_sur_heston_features(qk_sur_model* model, const double* features, int64_t n,
-                               void* out_rows) {
+                               void* out_rows, float* out_base) {
     if (!model) return qkb::fail_null("model");
     if (!features) return qkb::fail_null("features");
     if (!out_rows) return qkb::fail_null("out_rows");
     if (n <= 0) return qkb::fail_size(n);
     model->m.normalise(features, n, static_cast<__nv_bfloat16*>(out_rows));
+    if (out_base) model->m.base_host(features, n, out_base);
     return QK_OK;
+}
+
+int32_t qk_sur_heston_features_device(qk_sur_model* model, const double* features, int64_t n,
+                                      void* rows, float* base, void* stream) {
+    if (!model) return qkb::fail_null("model");
+    if (!features) return qkb::fail_null("features");
+    if (!rows) return qkb::fail_null("rows");
+    if (!base) return qkb::fail_null("base");
+    if (n <= 0) return qkb::fail_size(n);
+    return sur_status(model->m.features_device(features, n, static_cast<__nv_bfloat16*>(rows), base,
+                                               static_cast<cudaStream_t>(stream)),
+                      "qk_sur_heston_features_device");
 }
 
 int32_t qk_sur_heston_gradients(qk_sur_model* model, const double* features, const double* target,

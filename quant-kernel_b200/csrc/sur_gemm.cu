@@ -228,7 +228,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
         }
         float y = ((part[0] + part[1]) + part[2]) + part[3];
         y += __ldg(a.b4);
-        if (live) a.y_out[row] = y;
+        if (live) a.y_out[row] = a.base ? y + __ldg(a.base + row) : y;
         if (a.target != nullptr) {
             const float dy = live ? a.loss_scale * (y - a.target[row]) : 0.0f;
             if (live) a.dy_out[row] = dy;
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         if (grp == 0) {
             const float y = (((part[0][r] + part[1][r]) + part[2][r]) + part[3][r]) + b4;
             const int64_t row = t * kBM + r;
-            if (row < a.n) a.y[row] = y;
+            if (row < a.n) a.y[row] = a.base ? y + __ldg(a.base + row) : y;
         }
         // part[] is next written after two more barriers of the next tile
     }

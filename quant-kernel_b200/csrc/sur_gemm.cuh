@@ -46,13 +46,15 @@ struct GemmArgs {
     const float* b4;             // head bias [1]
     const float* target;         // [M] (training) or null (inference)
     float* y_out;                // [M]
+    const float* base;           // [M] added to y_out (inference), or null
     float* dy_out;               // [M] dL/dy (training)
     float loss_scale;            // dL/dy = loss_scale * (y - target)
     int* err;                    // error word (0 = ok)
 };
 
 // Fused MLP inference: y[i] = w4 . silu(W3 silu(W2 silu(W1 x_i + b1) + b2) + b3) + b4
-// for normalised bf16 rows x [n][64] (see sur_gemm.cu, mlp_infer_kernel).
+// (+ base[i] when base is not null) for normalised bf16 rows x [n][64] (see
+// sur_gemm.cu, mlp_infer_kernel).
 struct InferArgs {
     int64_t n;               // rows
     const float* b1;         // [256]
@@ -60,6 +62,7 @@ struct InferArgs {
     const float* b3;
     const float* w4;
     const float* b4;         // [1]
+    const float* base;       // [n] added to the network's output, or null
     float* y;                // [n]
     int* err;                // error word (0 = ok)
 };

@@ -55,7 +55,8 @@ void dfree(T*& p) {
 }
 
 // He-normal weights from the Philox/Box-Muller stream (seed, parameter index),
-// zero biases, zero layer-1 padding columns; the output layer uses 1/fan_in.
+// zero biases, zero layer-1 padding columns, and a zero output layer: the
+// untrained model is its base, and the first steps grow the residual from 0.
 __global__ void init_params_kernel(float* P, uint64_t seed) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= SurLayout::total) return;
@@ -67,8 +68,6 @@ __global__ void init_params_kernel(float* P, uint64_t seed) {
         v = col < kSurIn ? z[0] * sqrtf(2.0f / kSurIn) : 0.0f;
     } else if ((i >= SurLayout::W2 && i < SurLayout::b2) || (i >= SurLayout::W3 && i < SurLayout::b3)) {
         v = z[0] * sqrtf(2.0f / kSurHid);
-    } else if (i >= SurLayout::w4 && i < SurLayout::b4) {
-        v = z[0] * sqrtf(1.0f / kSurHid);
     }
     P[i] = v;
 }
@@ -86,6 +85,77 @@ __global__ void gather_kernel(const __nv_bfloat16* __restrict__ xall, const floa
     xb[static_cast<int64_t>(i) * kSurInPad + c] = v;
     xtb[static_cast<int64_t>(c) * B + i] = v;
     if (c == 0) tb[i] = tall[src];
+}
+
+// The residual's base: the Black-Scholes call / S at the Heston model's mean
+// variance over [0, T],
+//   vbar = theta + (v0 - theta) (1 - exp(-kappa T)) / (kappa T)
+// (the expectation of (1/T) int_0^T v_t dt), from f = (S/K, T, r, q, v0,
+// kappa, theta, ...).  The host and the device evaluate the same FP64
+// expression with their own exp/log/erfc; rounded to FP32 the two agree.
+__host__ __device__ inline double sur_base(const double* f) {
+    const double m = f[0], T = f[1], r = f[2], q = f[3], v0 = f[4], kappa = f[5], theta = f[6];
+    const double x = kappa * T;
+    const double w = (x > 1e-12) ? -expm1(-x) / x : 1.0;
+    double vbar = theta + (v0 - theta) * w;
+    if (!(vbar > 0.0)) vbar = 0.0;
+    const double sd = sqrt(vbar * T);
+    const double dq = exp(-q * T);
+    const double dk = exp(-r * T) / m;
+    if (!(sd > 1e-12)) {  // no variance left: the discounted forward payoff
+        const double fwd = dq - dk;
+        return fwd > 0.0 ? fwd : 0.0;
+    }
+    const double inv_sqrt2 = 0.70710678118654752440;
+    const double d1 = (log(m) + (r - q) * T) / sd + 0.5 * sd;
+    return dq * (0.5 * erfc(-d1 * inv_sqrt2)) - dk * (0.5 * erfc(-(d1 - sd) * inv_sqrt2));
+}
+
+// The normalised coordinate of feature value x in [lo, hi], as bf16 bits.
+__host__ __device__ inline unsigned short sur_norm_bits(double x, double lo, double hi) {
+    const double u = hi > lo ? 2.0 * (x - lo) / (hi - lo) - 1.0 : 0.0;
+    return __bfloat16_as_ushort(__float2bfloat16_rn(static_cast<float>(u)));
+}
+
+// Device features: one thread per row computes its nine normalised values
+// and base; the block then writes its 256 rows of 128 bytes as consecutive
+// 16-byte chunks (columns 9..63 are zero).
+constexpr int kFeatRows = 256;
+__global__ void __launch_bounds__(kFeatRows)
+features_kernel(const double* __restrict__ f, int64_t n, SurBox box, int32_t kind,
+                __nv_bfloat16* __restrict__ rows, float* __restrict__ base) {
+    __shared__ uint4 stage[kFeatRows][2];
+    const int t = threadIdx.x;
+    const int64_t row0 = static_cast<int64_t>(blockIdx.x) * kFeatRows;
+    const int64_t i = row0 + t;
+    unsigned short b[16] = {};
+    if (i < n) {
+        double x[kSurIn];
+#pragma unroll
+        for (int c = 0; c < kSurIn; ++c) x[c] = f[i * kSurIn + c];
+#pragma unroll
+        for (int c = 0; c < kSurIn; ++c) b[c] = sur_norm_bits(x[c], box.lo[c], box.hi[c]);
+        if (base) base[i] = kind == kSurBaseBsmMeanVar ? static_cast<float>(sur_base(x)) : 0.0f;
+    }
+    uint4 c0, c1;
+    c0.x = b[0] | (static_cast<uint32_t>(b[1]) << 16);
+    c0.y = b[2] | (static_cast<uint32_t>(b[3]) << 16);
+    c0.z = b[4] | (static_cast<uint32_t>(b[5]) << 16);
+    c0.w = b[6] | (static_cast<uint32_t>(b[7]) << 16);
+    c1.x = b[8];
+    c1.y = c1.z = c1.w = 0u;
+    stage[t][0] = c0;
+    stage[t][1] = c1;
+    __syncthreads();
+    uint4* out = reinterpret_cast<uint4*>(rows);
+    const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {  // 256 rows x 8 chunks, 8 per thread
+        const int idx = k * kFeatRows + t;
+        const int r = idx >> 3, c = idx & 7;
+        const int64_t row = row0 + r;
+        if (row < n) out[row * 8 + c] = c < 2 ? stage[r][c] : zero;
+    }
 }
 
 // out[r] = sum_j X[r][j] * (w ? w[j] : 1), one warp per row, fixed order.
@@ -216,7 +286,7 @@ SurModel::~SurModel() {
     if (device_ < 0) return;
     DeviceGuard g(device_);
     if (step_graph_) cudaGraphExecDestroy(step_graph_);
-    float* fl[] = {P_, M_, V_, G_, Tall_, Tb_, y_, dy_, dW1p_, dW2p_, dW3p_, db1_, db2_, db3_, dw4_, db4_, loss_hist_, Py_};
+    float* fl[] = {P_, M_, V_, G_, Tall_, Tb_, y_, dy_, dW1p_, dW2p_, dW3p_, db1_, db2_, db3_, dw4_, db4_, loss_hist_, Py_, Pbase_};
     for (float* p : fl)
         if (p) cudaFree(p);
     __nv_bfloat16* bl[] = {W1b_, W2b_, W3b_, W2Tb_, W3Tb_, Xall_, Xb_, XTb_, Z1_, H1_, H1T_, Z2_, H2_, H2T_,
@@ -262,13 +332,27 @@ void SurModel::normalise(const double* f, int64_t n, __nv_bfloat16* out) const {
     for (int64_t i = 0; i < n; ++i) {
         __nv_bfloat16* row = out + i * kSurInPad;
         for (int c = 0; c < kSurInPad; ++c) row[c] = __float2bfloat16_rn(0.0f);
-        for (int c = 0; c < kSurIn; ++c) {
-            const double lo = box_.lo[c], hi = box_.hi[c];
-            const double x = f[i * kSurIn + c];
-            const double u = hi > lo ? 2.0 * (x - lo) / (hi - lo) - 1.0 : 0.0;
-            row[c] = __float2bfloat16_rn(static_cast<float>(u));
-        }
+        for (int c = 0; c < kSurIn; ++c)
+            row[c] = __ushort_as_bfloat16(sur_norm_bits(f[i * kSurIn + c], box_.lo[c], box_.hi[c]));
     }
+}
+
+void SurModel::base_host(const double* f, int64_t n, float* out) const {
+    for (int64_t i = 0; i < n; ++i)
+        out[i] = base_kind_ == kSurBaseBsmMeanVar ? static_cast<float>(sur_base(f + i * kSurIn)) : 0.0f;
+}
+
+cudaError_t SurModel::features_device(const double* f, int64_t n, __nv_bfloat16* rows, float* base,
+                                      cudaStream_t st) {
+    DeviceGuard g(device_);
+    if (n <= 0 || (reinterpret_cast<uintptr_t>(rows) & 15u) != 0 ||
+        (reinterpret_cast<uintptr_t>(f) & 7u) != 0 || (reinterpret_cast<uintptr_t>(base) & 3u) != 0)
+        return cudaErrorInvalidValue;
+    const int64_t blocks = (n + kFeatRows - 1) / kFeatRows;
+    if (blocks > 0x7fffffff) return cudaErrorInvalidValue;
+    features_kernel<<<static_cast<unsigned>(blocks), kFeatRows, 0, st ? st : stream_>>>(
+        f, n, box_, base_kind_, rows, base);
+    return cudaGetLastError();
 }
 
 bool SurModel::in_box(const double* f) const {
@@ -306,8 +390,12 @@ cudaError_t SurModel::set_dataset(const double* features, const double* target, 
     }
     std::vector<__nv_bfloat16> rows(static_cast<size_t>(n) * kSurInPad);
     normalise(features, n, rows.data());
+    // the network learns target - base
     std::vector<float> t(static_cast<size_t>(n));
-    for (int64_t i = 0; i < n; ++i) t[i] = static_cast<float>(target[i]);
+    for (int64_t i = 0; i < n; ++i) {
+        const double b = base_kind_ == kSurBaseBsmMeanVar ? sur_base(features + i * kSurIn) : 0.0;
+        t[i] = static_cast<float>(target[i] - b);
+    }
     QK_TRY(dalloc(&Xall_, static_cast<size_t>(n) * kSurInPad));
     QK_TRY(dalloc(&Tall_, static_cast<size_t>(n)));
     QK_TRY(dalloc(&perm_, static_cast<size_t>(n)));
@@ -509,13 +597,15 @@ cudaError_t SurModel::ensure_predict_buffers(int64_t rows) {
     QK_TRY(dalloc(&PH1_, static_cast<size_t>(rows) * kSurHid));
     QK_TRY(dalloc(&PH2_, static_cast<size_t>(rows) * kSurHid));
     QK_TRY(dalloc(&Py_, static_cast<size_t>(rows)));
+    QK_TRY(dalloc(&Pbase_, static_cast<size_t>(rows)));
     pred_rows_ = rows;
     return cudaSuccess;
 }
 
-cudaError_t SurModel::predict_device(const __nv_bfloat16* x, int64_t n, float* y, cudaStream_t st,
-                                     bool layered) {
+cudaError_t SurModel::predict_device(const __nv_bfloat16* x, const float* base, int64_t n, float* y,
+                                     cudaStream_t st, bool layered) {
     DeviceGuard g(device_);
+    if (base_kind_ != kSurBaseNone && base == nullptr) return cudaErrorInvalidValue;
     if (!layered) {
         if (sm_count_ <= 0)
             QK_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
@@ -530,6 +620,7 @@ cudaError_t SurModel::predict_device(const __nv_bfloat16* x, int64_t n, float* y
         ia.b3 = P_ + SurLayout::b3;
         ia.w4 = P_ + SurLayout::w4;
         ia.b4 = P_ + SurLayout::b4;
+        ia.base = base_kind_ != kSurBaseNone ? base : nullptr;
         ia.y = y;
         ia.err = &state_->err;
         return launch_mlp_infer(tx, tw1, tw2, tw3, ia, sm_count_, st);
@@ -554,6 +645,7 @@ cudaError_t SurModel::predict_device(const __nv_bfloat16* x, int64_t n, float* y
         l.M = static_cast<int>(m); l.N = kSurHid; l.K = kSurHid; l.k_per_split = kSurHid;
         l.bias = P_ + SurLayout::b3; l.w4 = P_ + SurLayout::w4; l.b4 = P_ + SurLayout::b4;
         l.y_out = y + off;
+        l.base = base_kind_ != kSurBaseNone ? base + off : nullptr;
         QK_TRY(launch_umma_gemm(kEpiLast, 256, th2, tw3, l, 1, st));
     }
     return cudaSuccess;
@@ -564,15 +656,19 @@ cudaError_t SurModel::predict(const double* features, int64_t n, double* out) {
     const int64_t chunk = std::min<int64_t>(n, kPredChunk);
     QK_TRY(ensure_predict_buffers(chunk));
     std::vector<__nv_bfloat16> rows(static_cast<size_t>(chunk) * kSurInPad);
-    std::vector<float> y(static_cast<size_t>(chunk));
+    std::vector<float> y(static_cast<size_t>(chunk)), b(static_cast<size_t>(chunk));
     __nv_bfloat16* xin = PX_;  // the chunk's inputs; predict_device uses PH1_/PH2_
     cudaError_t e = cudaSuccess;
     for (int64_t off = 0; off < n && e == cudaSuccess; off += chunk) {
         const int64_t m = std::min<int64_t>(chunk, n - off);
         normalise(features + off * kSurIn, m, rows.data());
+        base_host(features + off * kSurIn, m, b.data());
         e = cudaMemcpyAsync(xin, rows.data(), static_cast<size_t>(m) * kSurInPad * sizeof(__nv_bfloat16),
                             cudaMemcpyHostToDevice, stream_);
-        if (e == cudaSuccess) e = predict_device(xin, m, Py_, stream_);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(Pbase_, b.data(), static_cast<size_t>(m) * sizeof(float), cudaMemcpyHostToDevice,
+                                stream_);
+        if (e == cudaSuccess) e = predict_device(xin, Pbase_, m, Py_, stream_);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(y.data(), Py_, static_cast<size_t>(m) * sizeof(float), cudaMemcpyDeviceToHost, stream_);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
@@ -644,7 +740,8 @@ int SurModel::device_error() {
     return s.err;
 }
 
-// Checkpoint: "QKSURv01", layout size, the box, the state, P, M, V (FP32).
+// Checkpoint: "QKSURv02", layout size, base kind, the box, the state, P, M, V
+// (FP32).  "QKSURv01" files (no base kind: a network without a base) load too.
 cudaError_t SurModel::save(const char* path) {
     DeviceGuard g(device_);
     SurState s{};
@@ -655,9 +752,10 @@ cudaError_t SurModel::save(const char* path) {
     QK_TRY(cudaMemcpy(buf.data() + 2 * SurLayout::total, V_, SurLayout::total * sizeof(float), cudaMemcpyDeviceToHost));
     FILE* f = std::fopen(path, "wb");
     if (!f) return cudaErrorInvalidValue;
-    const char magic[8] = {'Q', 'K', 'S', 'U', 'R', 'v', '0', '1'};
+    const char magic[8] = {'Q', 'K', 'S', 'U', 'R', 'v', '0', '2'};
     const int32_t total = SurLayout::total;
     bool ok = std::fwrite(magic, 1, 8, f) == 8 && std::fwrite(&total, sizeof total, 1, f) == 1 &&
+              std::fwrite(&base_kind_, sizeof base_kind_, 1, f) == 1 &&
               std::fwrite(&box_, sizeof box_, 1, f) == 1 && std::fwrite(&s, sizeof s, 1, f) == 1 &&
               std::fwrite(buf.data(), sizeof(float), buf.size(), f) == buf.size();
     ok = (std::fclose(f) == 0) && ok;
@@ -669,15 +767,22 @@ cudaError_t SurModel::load(const char* path) {
     FILE* f = std::fopen(path, "rb");
     if (!f) return cudaErrorInvalidValue;
     char magic[8];
-    int32_t total = 0;
+    int32_t total = 0, kind = kSurBaseNone;
+    SurBox box{};
     SurState s{};
     std::vector<float> buf(static_cast<size_t>(SurLayout::total) * 3);
-    bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "QKSURv01", 8) == 0 &&
-              std::fread(&total, sizeof total, 1, f) == 1 && total == SurLayout::total &&
-              std::fread(&box_, sizeof box_, 1, f) == 1 && std::fread(&s, sizeof s, 1, f) == 1 &&
-              std::fread(buf.data(), sizeof(float), buf.size(), f) == buf.size();
+    bool ok = std::fread(magic, 1, 8, f) == 8;
+    const bool v2 = ok && std::memcmp(magic, "QKSURv02", 8) == 0;
+    ok = ok && (v2 || std::memcmp(magic, "QKSURv01", 8) == 0) &&
+         std::fread(&total, sizeof total, 1, f) == 1 && total == SurLayout::total &&
+         (!v2 || std::fread(&kind, sizeof kind, 1, f) == 1) &&
+         (kind == kSurBaseNone || kind == kSurBaseBsmMeanVar) &&
+         std::fread(&box, sizeof box, 1, f) == 1 && std::fread(&s, sizeof s, 1, f) == 1 &&
+         std::fread(buf.data(), sizeof(float), buf.size(), f) == buf.size();
     std::fclose(f);
     if (!ok) return cudaErrorInvalidValue;
+    box_ = box;
+    base_kind_ = kind;
     s.err = 0;
     QK_TRY(cudaMemcpy(state_, &s, sizeof s, cudaMemcpyHostToDevice));
     QK_TRY(cudaMemcpy(P_, buf.data(), SurLayout::total * sizeof(float), cudaMemcpyHostToDevice));

@@ -1,6 +1,11 @@
 // sur_mlp.h -- the Heston price surrogate: MLP 9 -> 256 -> 256 -> 256 -> 1,
 // SiLU, BF16 weights/activations, FP32 accumulation, FP32 master weights and
 // Adam moments, trained and evaluated on the GPU with the tcgen05 GEMM.
+//
+// The network learns a residual: price / S = base(f) + MLP(normalised f),
+// with base the Black-Scholes call / S at the Heston model's mean variance
+// over [0, T] (see sur_base).  The base carries the bulk of the price
+// surface, so the network's absolute error shrinks with the residual's scale.
 #pragma once
 
 #include <cstdint>
@@ -12,6 +17,9 @@ namespace qkb {
 constexpr int kSurIn = 9;        // S/K, T, r, q, v0, kappa, theta, sigma, rho
 constexpr int kSurInPad = 64;    // layer-1 K, zero-padded for the 64-wide k-block
 constexpr int kSurHid = 256;
+// Base of the residual (stored in checkpoints).
+enum : int32_t { kSurBaseNone = 0, kSurBaseBsmMeanVar = 1 };
+
 constexpr int kSurParams = kSurHid * kSurIn + kSurHid + 2 * (kSurHid * kSurHid + kSurHid) +
                            kSurHid + 1;  // 134,401 trainable values
 
@@ -56,6 +64,14 @@ public:
     cudaError_t init(uint64_t seed, const SurBox& box);
     // Raw features (n x 9, the order of kSurIn) -> normalised bf16 rows.
     void normalise(const double* features, int64_t n, __nv_bfloat16* out_rows) const;
+    // The residual's base (price / S, FP64 rounded to FP32) for each row; 0
+    // for a model without one.
+    void base_host(const double* features, int64_t n, float* out_base) const;
+    // Device features (n x 9 FP64, DEVICE) -> normalised rows and base (DEVICE),
+    // the same values as normalise and base_host, asynchronous on st.
+    cudaError_t features_device(const double* features, int64_t n, __nv_bfloat16* rows,
+                                float* base, cudaStream_t st);
+    int32_t base_kind() const { return base_kind_; }
     bool in_box(const double* f) const;
 
     cudaError_t set_dataset(const double* features, const double* target, int64_t n);
@@ -63,11 +79,12 @@ public:
                       float* out_epoch_loss);
     // price / spot of calls for raw features, host in and out.
     cudaError_t predict(const double* features, int64_t n, double* out);
-    // Device-resident inference on normalised bf16 rows [n][64]: the fused
-    // kernel (all three layers per 128-row tile in one persistent launch), or
-    // with layered = true the layer-by-layer GEMMs it is tested against.
-    cudaError_t predict_device(const __nv_bfloat16* x_rows, int64_t n, float* y, cudaStream_t st,
-                               bool layered = false);
+    // Device-resident inference on normalised bf16 rows [n][64] plus the
+    // rows' base (required when base_kind() != kSurBaseNone): the fused kernel
+    // (all three layers per 128-row tile in one persistent launch), or with
+    // layered = true the layer-by-layer GEMMs it is tested against.
+    cudaError_t predict_device(const __nv_bfloat16* x_rows, const float* base, int64_t n, float* y,
+                               cudaStream_t st, bool layered = false);
     // One forward + backward without an update: loss and the 134,401 gradients.
     cudaError_t gradients(const double* features, const double* target, int n, double* grads,
                           double* loss);
@@ -89,6 +106,7 @@ private:
     int device_ = -1;
     cudaStream_t stream_ = nullptr;
     SurBox box_{};
+    int32_t base_kind_ = kSurBaseBsmMeanVar;
     // parameters, Adam moments, gradient
     float* P_ = nullptr;
     float* M_ = nullptr;
@@ -120,6 +138,7 @@ private:
     int sm_count_ = 0;
     __nv_bfloat16 *PX_ = nullptr, *PH1_ = nullptr, *PH2_ = nullptr;
     float* Py_ = nullptr;
+    float* Pbase_ = nullptr;
 };
 
 }  // namespace qkb

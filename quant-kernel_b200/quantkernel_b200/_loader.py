@@ -107,9 +107,10 @@ FUNCTION_SIGNATURES = [
     ("qk_sur_heston_set_dataset", I32, [VP, PD, PD, I64]),
     ("qk_sur_heston_train", I32, [VP, I32, I32, D, U64, PD]),
     ("qk_sur_heston_predict", I32, [VP, PD, I64, PD]),
-    ("qk_sur_heston_predict_device", I32, [VP, VP, I64, VP, VP]),
-    ("qk_sur_heston_predict_device_layered", I32, [VP, VP, I64, VP, VP]),
-    ("qk_sur_heston_features", I32, [VP, PD, I64, VP]),
+    ("qk_sur_heston_predict_device", I32, [VP, VP, VP, I64, VP, VP]),
+    ("qk_sur_heston_predict_device_layered", I32, [VP, VP, VP, I64, VP, VP]),
+    ("qk_sur_heston_features", I32, [VP, PD, I64, VP, VP]),
+    ("qk_sur_heston_features_device", I32, [VP, VP, I64, VP, VP, VP]),
     ("qk_sur_heston_gradients", I32, [VP, PD, PD, I32, PD, PD]),
     ("qk_sur_heston_parameters", I32, [VP, PD]),
     ("qk_sur_heston_set_parameters", I32, [VP, PD]),

@@ -2,9 +2,12 @@
 
 Features, in this order: S/K, T, r, q, v0, kappa, theta, sigma (vol of vol),
 rho.  Target: call price / S (prices are homogeneous of degree one in S and
-K, so the network works at S = 1).  Inputs are normalised to [-1, 1] over the
-training box; `price_batch` prices options inside the box with the network
-and the others with the plain GPU Monte Carlo.  Training and inference run on
+K, so the network works at S = 1).  The network learns the residual over a
+base, the Black-Scholes call / S at the Heston mean variance over [0, T]
+(theta + (v0 - theta)(1 - exp(-kappa T))/(kappa T)), which the library
+computes in FP64 and adds to the network's output.  Inputs are normalised to
+[-1, 1] over the training box; `price_batch` prices options inside the box
+with the network and the others with the plain GPU Monte Carlo.  Training and inference run on
 libqk_b200.so's tcgen05 BF16 GEMMs (FP32 accumulation, FP32 master weights)
 and Adam kernels.
 """
@@ -86,21 +89,36 @@ class HestonSurrogate:
         self._check(self.lib.qk_sur_heston_predict(self._h, _pd(f), f.shape[0], _pd(out)), "predict")
         return out
 
-    def predict_device(self, x_rows_ptr, n, y_ptr, stream=0, layered=False):
-        """Device rows in, device price/S out.  The fused kernel by default;
-        layered=True runs the layer-by-layer GEMMs it is tested against."""
+    def predict_device(self, x_rows_ptr, base_ptr, n, y_ptr, stream=0, layered=False):
+        """Device rows and base in, device price/S out.  The fused kernel by
+        default; layered=True runs the layer-by-layer GEMMs it is tested
+        against."""
         fn = (self.lib.qk_sur_heston_predict_device_layered if layered
               else self.lib.qk_sur_heston_predict_device)
-        self._check(fn(self._h, ct.c_void_p(x_rows_ptr), int(n), ct.c_void_p(y_ptr),
-                       ct.c_void_p(stream) if stream else None), "predict_device")
+        self._check(fn(self._h, ct.c_void_p(x_rows_ptr), ct.c_void_p(base_ptr) if base_ptr else None,
+                       int(n), ct.c_void_p(y_ptr), ct.c_void_p(stream) if stream else None),
+                    "predict_device")
+
+    def features_device(self, f_ptr, n, rows_ptr, base_ptr, stream=0):
+        """Device features (n x 9 float64) -> device rows [n][64] bf16 and base
+        (float32), one launch on `stream`."""
+        self._check(self.lib.qk_sur_heston_features_device(
+            self._h, ct.c_void_p(f_ptr), int(n), ct.c_void_p(rows_ptr), ct.c_void_p(base_ptr),
+            ct.c_void_p(stream) if stream else None), "features_device")
+
+    def features(self, features):
+        """Normalised bf16 rows [n][64] as uint16 and the rows' base (float32), host."""
+        f = np.ascontiguousarray(features, np.float64)
+        out = np.empty((f.shape[0], 64), np.uint16)
+        base = np.empty(f.shape[0], np.float32)
+        self._check(self.lib.qk_sur_heston_features(self._h, _pd(f), f.shape[0],
+                                                    out.ctypes.data_as(ct.c_void_p),
+                                                    base.ctypes.data_as(ct.c_void_p)), "features")
+        return out, base
 
     def feature_rows(self, features):
         """Normalised bf16 rows [n][64] as uint16 (host)."""
-        f = np.ascontiguousarray(features, np.float64)
-        out = np.empty((f.shape[0], 64), np.uint16)
-        self._check(self.lib.qk_sur_heston_features(self._h, _pd(f), f.shape[0],
-                                                    out.ctypes.data_as(ct.c_void_p)), "features")
-        return out
+        return self.features(features)[0]
 
     def gradients(self, features, target):
         f = np.ascontiguousarray(features, np.float64)
