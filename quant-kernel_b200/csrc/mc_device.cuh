@@ -78,13 +78,28 @@ __device__ __forceinline__ U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c
     return U4{c0, c1, c2, c3};
 }
 
+// Uniforms without an integer-to-float conversion: OR-ing k <= 23 bits b into
+// the mantissa of 1.0f gives y = 1 + b 2^-k exactly in [1, 2), and the affine
+// maps below are exact (Sterbenz, or a result with few enough fraction bits),
+// so they equal (b + 1/2) 2^-23 and (b + 1/2) 2^-(k-1) - 1 bit for bit while
+// staying off the conversion pipe.
+__device__ __forceinline__ float unit_from_bits(uint32_t b23) {  // (b + 1/2) 2^-23
+    return __uint_as_float(0x3F800000u | b23) - 0x1.fffffep-1f;   // y - (1 - 2^-24)
+}
+template <int K>  // K-bit b, K <= 22:  (b + 1/2) 2^-(K-1) - 1 = 2y - (3 - 2^-K)
+__device__ __forceinline__ float sym_from_bits(uint32_t b) {
+    const float y = __uint_as_float(0x3F800000u | (b << (23 - K)));
+    return fma_rn(y, 2.0f, -(3.0f - 1.0f / (float)(1u << K)));
+}
+
 // Box-Muller on two 32-bit words (the layout the FP64 replay in the oracle
 // mirrors):  u = ((xa >> 9) + 1/2) 2^-23 in (0,1), g = ((xb >> 9) + 1/2) 2^-22 - 1
 // in (-1,1);  za = sqrt(-2 ln u) cos(pi g),  zb = sqrt(-2 ln u) sin(pi g).
-// ln u = log2(u) * ln 2, and sqrt(w) = sqrt.approx(w).
+// ln u = log2(u) * ln 2, and sqrt(w) = sqrt.approx(w).  For the 23-bit angle,
+// y = 2 + b 2^-22 (exponent of 2.0f) and g = (y - 3) + 2^-23, both exact.
 __device__ __forceinline__ void box_muller(uint32_t xa, uint32_t xb, float& za, float& zb) {
-    const float u = fma_rn(__uint2float_rn(xa >> 9), 0x1p-23f, 0x1p-24f);
-    const float g = fma_rn(__uint2float_rn(xb >> 9), 0x1p-22f, 0x1p-23f - 1.0f);
+    const float u = unit_from_bits(xa >> 9);
+    const float g = (__uint_as_float(0x40000000u | (xb >> 9)) - 3.0f) + 0x1p-23f;
     const float w = -1.38629436111989061883f * ptx_lg2(u);  // -2 ln u
     const float rad = ptx_sqrt(w);
     const float ang = 3.14159265358979323846f * g;
@@ -99,13 +114,12 @@ __device__ __forceinline__ void normals4(uint32_t unit, uint32_t block, uint32_t
     box_muller(x.z, x.w, z[2], z[3]);
 }
 
-// Box-Muller from a 23-bit radius word and an n-bit angle word:
-//   u = (ub + 1/2) 2^-23,  g = (gb + 1/2) 2^-(n-1) - 1  (gscale = 2^-(n-1),
-//   goff = 2^-n - 1, both exact in FP32 for n <= 23).
-__device__ __forceinline__ void box_muller_bits(uint32_t ub, uint32_t gb, float gscale, float goff,
-                                                float& za, float& zb) {
-    const float u = fma_rn(__uint2float_rn(ub), 0x1p-23f, 0x1p-24f);
-    const float g = fma_rn(__uint2float_rn(gb), gscale, goff);
+// Box-Muller from a 23-bit radius word and a K-bit angle word:
+//   u = (ub + 1/2) 2^-23,  g = (gb + 1/2) 2^-(K-1) - 1.
+template <int K>
+__device__ __forceinline__ void box_muller_bits(uint32_t ub, uint32_t gb, float& za, float& zb) {
+    const float u = unit_from_bits(ub);
+    const float g = sym_from_bits<K>(gb);
     const float w = -1.38629436111989061883f * ptx_lg2(u);  // -2 ln u
     const float rad = ptx_sqrt(w);
     const float ang = 3.14159265358979323846f * g;
@@ -122,12 +136,11 @@ struct Philox6 {
     U4 x;
     __device__ __forceinline__ void pair(int p, float& za, float& zb) const {
         if (p == 0)
-            box_muller_bits(x.x >> 9, x.w & 0xFFFFu, 0x1p-15f, 0x1p-16f - 1.0f, za, zb);
+            box_muller_bits<16>(x.x >> 9, x.w & 0xFFFFu, za, zb);
         else if (p == 1)
-            box_muller_bits(x.y >> 9, x.w >> 16, 0x1p-15f, 0x1p-16f - 1.0f, za, zb);
+            box_muller_bits<16>(x.y >> 9, x.w >> 16, za, zb);
         else
-            box_muller_bits(x.z >> 9, (x.x & 0x1FFu) | ((x.y & 0x1FFu) << 9), 0x1p-17f,
-                            0x1p-18f - 1.0f, za, zb);
+            box_muller_bits<18>(x.z >> 9, (x.x & 0x1FFu) | ((x.y & 0x1FFu) << 9), za, zb);
     }
 };
 
