@@ -231,12 +231,17 @@ QK_EXPORT int32_t qk_get_device(int32_t* device);
 #define QK_PLAN_GRAPH         0x2 /* replay execute() from a captured CUDA graph */
 #define QK_PLAN_NO_ANTITHETIC 0x4 /* stepwise models: independent paths, not pairs */
 #define QK_PLAN_TIMING        0x8 /* record CUDA events around the simulate kernel */
-#define QK_PLAN_AUTOTUNE      0x10 /* choose block size / units per thread by timing; for
-                                      * batches of several model families also the mode:
-                                      * one persistent kernel or one grid per family (the
-                                      * latter not when QK_PLAN_PERSISTENT is given) */
+#define QK_PLAN_AUTOTUNE      0x10 /* choose block size / units per thread / step
+                                      * unrolling by timing; for batches of several model
+                                      * families also the mode: one persistent kernel or
+                                      * one grid per family (the latter not when
+                                      * QK_PLAN_PERSISTENT is given) */
 #define QK_PLAN_FAMILY_GRIDS  0x20 /* several model families: one grid per family group,
                                       * back to back, instead of the persistent kernel */
+#define QK_PLAN_STEP_UNROLL2  0x40 /* stepwise single-family plans at 1 or 2 units per
+                                      * thread: two Philox step blocks per loop iteration
+                                      * (same results bit for bit; the autotuner also
+                                      * tries it) */
 
 /* Price + standard error batches.  Same inputs as the Part 1 batch calls;
  * out_stderr[i] is the standard error of out_prices[i] (NaN where no
@@ -362,6 +367,9 @@ QK_EXPORT int32_t qk_mcm_plan_stats(qk_mc_plan* plan, double* simulate_ms, int32
  * group); CTAs of the persistent kernel. */
 QK_EXPORT int32_t qk_mcm_plan_config(qk_mc_plan* plan, int32_t* block, int32_t* units_per_thread,
                                      int32_t* ctas);
+/* Step blocks per loop iteration of the plan's simulate kernel (1 or 2; 1 for
+ * terminal, variance-reduction and multi-family plans). */
+QK_EXPORT int32_t qk_mcm_plan_step_unroll(qk_mc_plan* plan, int32_t* step_unroll);
 QK_EXPORT int32_t qk_mcm_plan_destroy(qk_mc_plan* plan);
 
 /* ======================================================================= *

@@ -143,9 +143,12 @@ __device__ __forceinline__ void sim_terminal(const McOption& o, uint32_t unit0, 
 //   s' = max(s + s * inc, 1e-12/spot),  inc = (r-q)dt + vol sqrt(dt) z
 //   [Milstein: + c (z^2 - 1), c = vol^2 dt / 2]
 // evaluated as one fused s + s * inc.  One Philox call feeds six steps
-// (Philox6: three Box-Muller pairs).
+// (Philox6: three Box-Muller pairs).  SU step blocks run per loop iteration
+// (their Philox calls first): the same normals and arithmetic for every SU,
+// more independent work per iteration for larger SU (the autotuner's step
+// unrolling).
 // ----------------------------------------------------------------------------
-template <int UPT, bool ANTI, bool MIL>
+template <int UPT, bool ANTI, bool MIL, int SU>
 __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, uint32_t stride,
                                              uint32_t k0, uint32_t k1, Acc& acc) {
     const float m0 = o.p[0], b = o.p[1], fl = o.p[2], c = o.p[3];
@@ -159,29 +162,38 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
         sd[k] = 1.0f;
     }
     uint32_t blk = 0;  // step block j / 6
-    for (int32_t j = 0; j < steps; j += 6, ++blk) {
-        Philox6 r[UPT];
+    for (int32_t j0 = 0; j0 < steps; j0 += 6 * SU, blk += SU) {
+        Philox6 rb[SU][UPT];
 #pragma unroll
-        for (int k = 0; k < UPT; ++k)
-            r[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk, 0u, c3, k0, k1);
-        const int32_t m = (steps - j) < 6 ? (steps - j) : 6;
-        float zp[UPT][2];
+        for (int sb = 0; sb < SU; ++sb)
 #pragma unroll
-        for (int s = 0; s < 6; ++s) {
-            if (s < m) {
+            for (int k = 0; k < UPT; ++k)
+                rb[sb][k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk + (uint32_t)sb, 0u, c3,
+                                            k0, k1);
 #pragma unroll
-                for (int k = 0; k < UPT; ++k) {
-                    if ((s & 1) == 0) r[k].pair(s >> 1, zp[k][0], zp[k][1]);
-                    const float zz = zp[k][s & 1];                    float iu, id;
-                    if (MIL) {
-                        iu = fma_rn(fma_rn(c, zz, b), zz, m0);
-                        id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
-                    } else {
-                        iu = fma_rn(b, zz, m0);
-                        id = fma_rn(-b, zz, m0);
+        for (int sb = 0; sb < SU; ++sb) {
+            const int32_t j = j0 + 6 * sb;
+            const Philox6 (&r)[UPT] = rb[sb];
+            const int32_t m = (steps - j) < 6 ? (steps - j) : 6;
+            float zp[UPT][2];
+#pragma unroll
+            for (int s = 0; s < 6; ++s) {
+                if (s < m) {
+#pragma unroll
+                    for (int k = 0; k < UPT; ++k) {
+                        if ((s & 1) == 0) r[k].pair(s >> 1, zp[k][0], zp[k][1]);
+                        const float zz = zp[k][s & 1];
+                        float iu, id;
+                        if (MIL) {
+                            iu = fma_rn(fma_rn(c, zz, b), zz, m0);
+                            id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
+                        } else {
+                            iu = fma_rn(b, zz, m0);
+                            id = fma_rn(-b, zz, m0);
+                        }
+                        su[k] = fmaxf(fma_rn(su[k], iu, su[k]), fl);
+                        if (ANTI) sd[k] = fmaxf(fma_rn(sd[k], id, sd[k]), fl);
                     }
-                    su[k] = fmaxf(fma_rn(su[k], iu, su[k]), fl);
-                    if (ANTI) sd[k] = fmaxf(fma_rn(sd[k], id, sd[k]), fl);
                 }
             }
         }
@@ -210,14 +222,15 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 //            + sigma sqrt(dt) sqrt(v) (rho z1 + sqrt(1-rho^2) z2), 0)
 // v >= 0 after every step (and v0 >= 0 is validated), so the reference's
 // v_pos = max(v, 0) is v itself.  One Philox call feeds three steps of a unit
-// (six normals: Philox6).
+// (six normals: Philox6); SU step blocks per loop iteration as in
+// sim_stepwise.
 // ----------------------------------------------------------------------------
 //
 // LR = true: the likelihood-ratio delta of heston_lr_delta.cpp:37-132.  Each
 // path's payoff is weighted by the score of its first spot step,
 // w = clamp(z1_0 / (sqrt(v0) sqrt(dt) S0), -clip, clip); the antithetic path's
 // score is -w.
-template <int UPT, bool ANTI, bool LR>
+template <int UPT, bool ANTI, bool LR, int SU>
 __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, uint32_t stride,
                                            uint32_t k0, uint32_t k1, Acc& acc) {
     const float cmu = o.p[0], hdt = o.p[1], sqdt = o.p[2], kdt = o.p[3], kth = o.p[4];
@@ -238,33 +251,41 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         zfirst[k] = 0.0f;
     }
     uint32_t blk = 0;  // step block j / 3
-    for (int32_t j = 0; j < steps; j += 3, ++blk) {
-        Philox6 r[UPT];
+    for (int32_t j0 = 0; j0 < steps; j0 += 3 * SU, blk += SU) {
+        Philox6 rb[SU][UPT];
 #pragma unroll
-        for (int k = 0; k < UPT; ++k)
-            r[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk, 0u, c3, k0, k1);
-        const int32_t m = (steps - j) < 3 ? (steps - j) : 3;
+        for (int sb = 0; sb < SU; ++sb)
 #pragma unroll
-        for (int s = 0; s < 3; ++s) {
-            if (s < m) {
+            for (int k = 0; k < UPT; ++k)
+                rb[sb][k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk + (uint32_t)sb, 0u, c3,
+                                            k0, k1);
 #pragma unroll
-                for (int k = 0; k < UPT; ++k) {
-                    float z1, z2;
-                    r[k].pair(s, z1, z2);
-                    if (LR && j == 0 && s == 0) zfirst[k] = z1;
-                    const float sz1 = sqdt * z1;
-                    const float xw = fma_rn(xr, z1, xc * z2);
-                    {
-                        const float sv = ptx_sqrt(vu[k]);
-                        const float inc = fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu));
-                        xu[k] = ptx_max_nan(xu[k] + inc, xfl);
-                        vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
-                    }
-                    if (ANTI) {
-                        const float sv = ptx_sqrt(vd[k]);
-                        const float inc = fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu));
-                        xd[k] = ptx_max_nan(xd[k] + inc, xfl);
-                        vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
+        for (int sb = 0; sb < SU; ++sb) {
+            const int32_t j = j0 + 3 * sb;
+            const Philox6 (&r)[UPT] = rb[sb];
+            const int32_t m = (steps - j) < 3 ? (steps - j) : 3;
+#pragma unroll
+            for (int s = 0; s < 3; ++s) {
+                if (s < m) {
+#pragma unroll
+                    for (int k = 0; k < UPT; ++k) {
+                        float z1, z2;
+                        r[k].pair(s, z1, z2);
+                        if (LR && j == 0 && s == 0) zfirst[k] = z1;
+                        const float sz1 = sqdt * z1;
+                        const float xw = fma_rn(xr, z1, xc * z2);
+                        {
+                            const float sv = ptx_sqrt(vu[k]);
+                            const float inc = fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu));
+                            xu[k] = ptx_max_nan(xu[k] + inc, xfl);
+                            vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
+                        }
+                        if (ANTI) {
+                            const float sv = ptx_sqrt(vd[k]);
+                            const float inc = fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu));
+                            xd[k] = ptx_max_nan(xd[k] + inc, xfl);
+                            vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
+                        }
                     }
                 }
             }
@@ -458,19 +479,19 @@ __device__ __forceinline__ int32_t find_option(const int64_t* __restrict__ tile_
     return lo;
 }
 
-template <int FAMILY, int UPT, bool ANTI>
+template <int FAMILY, int UPT, bool ANTI, int SU>
 __device__ __forceinline__ void sim_family(const McOption& o, uint32_t unit0, uint32_t stride,
                                            uint32_t k0, uint32_t k1, Acc& acc) {
     if (FAMILY == kFamTerminal) sim_terminal<UPT, ANTI>(o, unit0, stride, k0, k1, acc);
-    if (FAMILY == kFamEuler) sim_stepwise<UPT, ANTI, false>(o, unit0, stride, k0, k1, acc);
-    if (FAMILY == kFamMilstein) sim_stepwise<UPT, ANTI, true>(o, unit0, stride, k0, k1, acc);
-    if (FAMILY == kFamHeston) sim_heston<UPT, ANTI, false>(o, unit0, stride, k0, k1, acc);
-    if (FAMILY == kFamHestonLr) sim_heston<UPT, ANTI, true>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamEuler) sim_stepwise<UPT, ANTI, false, SU>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamMilstein) sim_stepwise<UPT, ANTI, true, SU>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamHeston) sim_heston<UPT, ANTI, false, SU>(o, unit0, stride, k0, k1, acc);
+    if (FAMILY == kFamHestonLr) sim_heston<UPT, ANTI, true, SU>(o, unit0, stride, k0, k1, acc);
     if (FAMILY == kFamVr) sim_vr<UPT>(o, unit0, stride, k0, k1, acc);
 }
 
 // One tile: all UPT * unit_iters units of every thread, then the reduction.
-template <int FAMILY, int BLOCK, int UPT, bool ANTI>
+template <int FAMILY, int BLOCK, int UPT, bool ANTI, int SU = 1>
 __device__ __forceinline__ void run_tile(const McOption& o, int64_t tile, TilePartial* partials,
                                          DD* smem) {
     const uint32_t k0 = (uint32_t)o.seed, k1 = (uint32_t)(o.seed >> 32);
@@ -481,7 +502,7 @@ __device__ __forceinline__ void run_tile(const McOption& o, int64_t tile, TilePa
     for (int32_t it = 0; it < o.unit_iters; ++it) {
         const uint32_t base = first + (uint32_t)it * per_iter;
         if (base >= (uint32_t)o.units) break;
-        sim_family<FAMILY, UPT, ANTI>(o, base + threadIdx.x, (uint32_t)BLOCK, k0, k1, acc);
+        sim_family<FAMILY, UPT, ANTI, SU>(o, base + threadIdx.x, (uint32_t)BLOCK, k0, k1, acc);
     }
     reduce_tile<BLOCK, FAMILY == kFamVr>(acc, partials + tile, smem);
 }
@@ -504,7 +525,7 @@ __device__ __noinline__ void run_tile_call(const McOption& o, int64_t tile, Tile
 // No register cap: the kernel is issue- and special-function-bound, and
 // forcing 64 registers (4 CTAs of 256 per SM) added instructions and ran
 // slower on B200 than the compiler's 70 (3 CTAs).
-template <int FAMILY, int BLOCK, int UPT, bool ANTI>
+template <int FAMILY, int BLOCK, int UPT, bool ANTI, int SU>
 __global__ void __launch_bounds__(BLOCK)
     mc_simulate_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
                        int32_t n, int64_t tile0, int64_t n_tiles, TilePartial* __restrict__ partials) {
@@ -513,7 +534,7 @@ __global__ void __launch_bounds__(BLOCK)
         const int64_t tile = tile0 + t;  // tile_begin holds absolute tile indices
         const int32_t oi = find_option(tile_begin, n, tile);
         const McOption o = opts[oi];
-        run_tile<FAMILY, BLOCK, UPT, ANTI>(o, tile, partials, smem);
+        run_tile<FAMILY, BLOCK, UPT, ANTI, SU>(o, tile, partials, smem);
     }
 }
 
@@ -681,38 +702,56 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-template <int FAMILY, int BLOCK, int UPT, bool ANTI>
+template <int FAMILY, int BLOCK, int UPT, bool ANTI, int SU>
 cudaError_t launch_one(const SimArgs& a, cudaStream_t st) {
     const int64_t cap = (int64_t)a.max_ctas;
     const unsigned grid = (unsigned)(a.n_tiles < cap ? a.n_tiles : cap);
-    mc_simulate_kernel<FAMILY, BLOCK, UPT, ANTI>
+    mc_simulate_kernel<FAMILY, BLOCK, UPT, ANTI, SU>
         <<<grid, BLOCK, 0, st>>>(a.opts, a.tile_begin, a.n, a.tile0, a.n_tiles, a.partials);
     return cudaGetLastError();
 }
 
+constexpr bool is_stepwise(int family) {
+    return family == kFamEuler || family == kFamMilstein || family == kFamHeston ||
+           family == kFamHestonLr;
+}
+
+// Step unrolling 2 is compiled for the stepwise families at 1 and 2 units per
+// thread (4 units x 2 blocks of Philox words would exceed the register file
+// share that keeps 4+ CTAs resident).
 template <int FAMILY, int BLOCK, bool ANTI>
-cudaError_t launch_upt(int upt, const SimArgs& a, cudaStream_t st) {
+cudaError_t launch_upt(int upt, int su, const SimArgs& a, cudaStream_t st) {
+    if constexpr (is_stepwise(FAMILY)) {
+        if (su == 2) {
+            switch (upt) {
+                case 1: return launch_one<FAMILY, BLOCK, 1, ANTI, 2>(a, st);
+                case 2: return launch_one<FAMILY, BLOCK, 2, ANTI, 2>(a, st);
+                default: return cudaErrorInvalidValue;
+            }
+        }
+    }
+    if (su != 1) return cudaErrorInvalidValue;
     switch (upt) {
-        case 1: return launch_one<FAMILY, BLOCK, 1, ANTI>(a, st);
-        case 2: return launch_one<FAMILY, BLOCK, 2, ANTI>(a, st);
-        case 4: return launch_one<FAMILY, BLOCK, 4, ANTI>(a, st);
+        case 1: return launch_one<FAMILY, BLOCK, 1, ANTI, 1>(a, st);
+        case 2: return launch_one<FAMILY, BLOCK, 2, ANTI, 1>(a, st);
+        case 4: return launch_one<FAMILY, BLOCK, 4, ANTI, 1>(a, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <int FAMILY, bool ANTI>
-cudaError_t launch_block(int block, int upt, const SimArgs& a, cudaStream_t st) {
+cudaError_t launch_block(int block, int upt, int su, const SimArgs& a, cudaStream_t st) {
     switch (block) {
-        case 128: return launch_upt<FAMILY, 128, ANTI>(upt, a, st);
-        case 256: return launch_upt<FAMILY, 256, ANTI>(upt, a, st);
+        case 128: return launch_upt<FAMILY, 128, ANTI>(upt, su, a, st);
+        case 256: return launch_upt<FAMILY, 256, ANTI>(upt, su, a, st);
         default: return cudaErrorInvalidValue;
     }
 }
 
 template <int FAMILY>
-cudaError_t launch_anti(bool anti, int block, int upt, const SimArgs& a, cudaStream_t st) {
-    return anti ? launch_block<FAMILY, true>(block, upt, a, st)
-                : launch_block<FAMILY, false>(block, upt, a, st);
+cudaError_t launch_anti(bool anti, int block, int upt, int su, const SimArgs& a, cudaStream_t st) {
+    return anti ? launch_block<FAMILY, true>(block, upt, su, a, st)
+                : launch_block<FAMILY, false>(block, upt, su, a, st);
 }
 
 }  // namespace
@@ -735,16 +774,16 @@ int family_of(int32_t model) {
     }
 }
 
-cudaError_t launch_simulate(int family, bool anti, int block, int upt, const SimArgs& a,
+cudaError_t launch_simulate(int family, bool anti, int block, int upt, int su, const SimArgs& a,
                             cudaStream_t st) {
     if (a.n_tiles <= 0) return cudaSuccess;
     switch (family) {
-        case kFamTerminal: return launch_anti<kFamTerminal>(anti, block, upt, a, st);
-        case kFamEuler: return launch_anti<kFamEuler>(anti, block, upt, a, st);
-        case kFamMilstein: return launch_anti<kFamMilstein>(anti, block, upt, a, st);
-        case kFamHeston: return launch_anti<kFamHeston>(anti, block, upt, a, st);
-        case kFamHestonLr: return launch_anti<kFamHestonLr>(anti, block, upt, a, st);
-        case kFamVr: return launch_block<kFamVr, false>(block, upt, a, st);
+        case kFamTerminal: return launch_anti<kFamTerminal>(anti, block, upt, su, a, st);
+        case kFamEuler: return launch_anti<kFamEuler>(anti, block, upt, su, a, st);
+        case kFamMilstein: return launch_anti<kFamMilstein>(anti, block, upt, su, a, st);
+        case kFamHeston: return launch_anti<kFamHeston>(anti, block, upt, su, a, st);
+        case kFamHestonLr: return launch_anti<kFamHestonLr>(anti, block, upt, su, a, st);
+        case kFamVr: return launch_block<kFamVr, false>(block, upt, su, a, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -787,13 +826,13 @@ int max_resident_ctas(int family_or_persistent, int block, int upt, int device) 
     } else {
         // Occupancy of the Heston variant bounds the others (most registers).
         if (block == 128) {
-            e = upt == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 1, true>, 128, 0)
-              : upt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 2, true>, 128, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 4, true>, 128, 0);
+            e = upt == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 1, true, 1>, 128, 0)
+              : upt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 2, true, 1>, 128, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 128, 4, true, 1>, 128, 0);
         } else {
-            e = upt == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 1, true>, 256, 0)
-              : upt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 2, true>, 256, 0)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 4, true>, 256, 0);
+            e = upt == 1 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 1, true, 1>, 256, 0)
+              : upt == 2 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 2, true, 1>, 256, 0)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mc_simulate_kernel<kFamHeston, 256, 4, true, 1>, 256, 0);
         }
     }
     if (e != cudaSuccess || per_sm <= 0) return 0;

@@ -26,6 +26,11 @@ constexpr int kUptStepwise = 2;
 constexpr int kUptHeston = 2;
 constexpr int kUptVr = 1;
 
+inline bool family_is_stepwise(int family) {
+    return family == kFamEuler || family == kFamMilstein || family == kFamHeston ||
+           family == kFamHestonLr;
+}
+
 struct SimArgs {
     const McOption* opts;      // device, n records
     const int64_t* tile_begin; // device, n + 1 entries
@@ -38,7 +43,9 @@ struct SimArgs {
 
 int family_of(int32_t model);
 
-cudaError_t launch_simulate(int family, bool anti, int block, int upt, const SimArgs& a,
+// su: step blocks per loop iteration of the stepwise families (1 or 2; 2 only
+// with upt 1 or 2); other families take 1.
+cudaError_t launch_simulate(int family, bool anti, int block, int upt, int su, const SimArgs& a,
                             cudaStream_t st);
 cudaError_t launch_persistent(int block, const SimArgs& a, unsigned long long* work_counter,
                               cudaStream_t st);

@@ -131,7 +131,7 @@ NoAllocStatus noalloc_heston_batch(const BatchInput& in, double* out_prices, dou
         a.n_tiles = running;
         a.partials = d_part;
         a.max_ctas = 0x7fffffff;
-        e = launch_simulate(kFamHeston, true, kBlock, kUpt, a, 0);
+        e = launch_simulate(kFamHeston, true, kBlock, kUpt, 1, a, 0);
     }
     if (e == cudaSuccess) e = launch_finalize(d_rec, in.n, d_part, d_price, d_se, nullptr, nullptr, 0);
     if (e == cudaSuccess)

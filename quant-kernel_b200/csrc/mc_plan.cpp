@@ -360,13 +360,15 @@ void load_tune_file_locked() {
     if (!path) return;
     FILE* f = std::fopen(path, "r");
     if (!f) return;
-    char key[512];
-    int block = 0, upt = 0;
-    // one entry per line: <key> <block> <upt>
-    while (std::fscanf(f, "%511s %d %d", key, &block, &upt) == 3) {
+    char line[600], key[512];
+    // one entry per line: <key> <block> <upt> [<step unroll>]
+    while (std::fgets(line, sizeof line, f)) {
+        int block = 0, upt = 0, su = 1;
+        if (std::sscanf(line, "%511s %d %d %d", key, &block, &upt, &su) < 3) continue;
         if ((block == 128 || block == 256) &&
-            (upt == 1 || upt == 2 || upt == 4 || upt == kUptPersistent || upt == kUptFamilyGrids))
-            tune_map()[key] = LaunchConfig{block, upt};
+            (upt == 1 || upt == 2 || upt == 4 || upt == kUptPersistent || upt == kUptFamilyGrids) &&
+            (su == 1 || (su == 2 && (upt == 1 || upt == 2))))
+            tune_map()[key] = LaunchConfig{block, upt, su};
     }
     std::fclose(f);
 }
@@ -390,7 +392,8 @@ void store_tuned_config(const std::string& key, const LaunchConfig& cfg) {
     FILE* f = std::fopen(path, "w");
     if (!f) return;
     for (const auto& kv : tune_map())
-        std::fprintf(f, "%s %d %d\n", kv.first.c_str(), kv.second.block, kv.second.upt);
+        std::fprintf(f, "%s %d %d %d\n", kv.first.c_str(), kv.second.block, kv.second.upt,
+                     kv.second.su);
     std::fclose(f);
 }
 
@@ -492,7 +495,12 @@ cudaError_t Plan::build(const BatchInput& in, int32_t flags, std::string* err) {
         if (!persistent_ || (tuned.upt <= 0 && !(flags & (kFlagPersistent | kFlagFamilyGrids))))
             cfg_.upt = tuned.upt;
         if (persistent_ && cfg_.upt > 0) cfg_.upt = kUptPersistent;
+        cfg_.su = (!persistent_ && family_is_stepwise(family_)) ? tuned.su : 1;
     }
+    // QK_PLAN_STEP_UNROLL2: two step blocks per loop iteration where compiled
+    if ((flags & kFlagStepUnroll2) && !persistent_ && family_is_stepwise(family_) &&
+        (cfg_.upt == 1 || cfg_.upt == 2))
+        cfg_.su = 2;
     e = layout_tiles(cfg_);
     if (e != cudaSuccess) return e;
     if ((flags & kFlagAutotune) && n_tiles_ > 0) {
@@ -634,11 +642,11 @@ cudaError_t Plan::launch_all(cudaStream_t st, bool timing) {
                 ga.tile0 = g.tile_lo;
                 ga.n_tiles = g.tile_hi - g.tile_lo;
                 e = launch_simulate(g.family, g.anti, cfg_.block,
-                                    upt_for(g.family, true, cfg_), ga, st);
+                                    upt_for(g.family, true, cfg_), 1, ga, st);
                 if (e != cudaSuccess) return e;
             }
         } else {
-            e = launch_simulate(family_, anti_, cfg_.block, cfg_.upt, a, st);
+            e = launch_simulate(family_, anti_, cfg_.block, cfg_.upt, cfg_.su, a, st);
         }
         if (e != cudaSuccess) return e;
     }
@@ -739,8 +747,13 @@ cudaError_t Plan::autotune() {
             cands.push_back(LaunchConfig{256, kUptFamilyGrids});
         }
     } else {
+        // block size x units per thread, and for the stepwise families the
+        // step unrolling (one or two Philox step blocks per loop iteration)
         for (int b : {128, 256})
-            for (int u : {1, 2, 4}) cands.push_back(LaunchConfig{b, u});
+            for (int u : {1, 2, 4}) {
+                cands.push_back(LaunchConfig{b, u, 1});
+                if (family_is_stepwise(family_) && u <= 2) cands.push_back(LaunchConfig{b, u, 2});
+            }
     }
     LaunchConfig best = cfg_;
     float best_ms = std::numeric_limits<float>::max();

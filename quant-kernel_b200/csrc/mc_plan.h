@@ -35,6 +35,7 @@ enum : int32_t {
     kFlagTiming = 0x8,
     kFlagAutotune = 0x10,
     kFlagFamilyGrids = 0x20,
+    kFlagStepUnroll2 = 0x40,
 };
 
 // Grow-only device / pinned host allocations.
@@ -61,6 +62,7 @@ constexpr int kUptFamilyGrids = -1;
 struct LaunchConfig {
     int block = 256;
     int upt = 2;
+    int su = 1;  // step blocks per loop iteration (stepwise single-family grids)
 };
 
 class Plan {
@@ -89,6 +91,7 @@ public:
     }
     int block() const { return cfg_.block; }
     int upt() const { return cfg_.upt; }
+    int step_unroll() const { return cfg_.upt > 0 ? cfg_.su : 1; }
     int ctas() const { return max_ctas_; }
     bool persistent() const { return persistent_; }
     double* d_price() const { return static_cast<double*>(d_price_.p); }

@@ -766,6 +766,13 @@ int32_t qk_mcm_plan_config(qk_mc_plan* plan, int32_t* block, int32_t* units_per_
     return QK_OK;
 }
 
+int32_t qk_mcm_plan_step_unroll(qk_mc_plan* plan, int32_t* step_unroll) {
+    if (!plan) return fail_null("plan");
+    if (!step_unroll) return fail_null("step_unroll");
+    *step_unroll = plan->plan.step_unroll();
+    return QK_OK;
+}
+
 int32_t qk_mcm_plan_destroy(qk_mc_plan* plan) {
     if (!plan) return QK_OK;
     delete plan;

@@ -35,3 +35,4 @@ QK_PLAN_NO_ANTITHETIC = 0x4
 QK_PLAN_TIMING = 0x8
 QK_PLAN_AUTOTUNE = 0x10
 QK_PLAN_FAMILY_GRIDS = 0x20
+QK_PLAN_STEP_UNROLL2 = 0x40

@@ -100,6 +100,7 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_plan_device_results", I32, [VP, ct.POINTER(VP), ct.POINTER(VP)]),
     ("qk_mcm_plan_stats", I32, [VP, PD, PI32, PI64]),
     ("qk_mcm_plan_config", I32, [VP, PI32, PI32, PI32]),
+    ("qk_mcm_plan_step_unroll", I32, [VP, PI32]),
     ("qk_mcm_plan_destroy", I32, [VP]),
     ("qk_sur_gemm_bf16", I32, [VP, VP, VP, I32, I32, I32, I32, VP]),
     ("qk_sur_heston_create", I32, [PD, PD, U64, ct.POINTER(VP)]),

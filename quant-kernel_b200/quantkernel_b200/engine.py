@@ -651,7 +651,10 @@ class McPlan:
     def config(self):
         b, u, c = ct.c_int32(0), ct.c_int32(0), ct.c_int32(0)
         self._lib.qk_mcm_plan_config(self._h, ct.byref(b), ct.byref(u), ct.byref(c))
-        return {"block": b.value, "units_per_thread": u.value, "ctas": c.value}
+        su = ct.c_int32(1)
+        self._lib.qk_mcm_plan_step_unroll(self._h, ct.byref(su))
+        return {"block": b.value, "units_per_thread": u.value, "ctas": c.value,
+                "step_unroll": su.value}
 
     def close(self) -> None:
         if self._h:

@@ -8,9 +8,11 @@ geometry is the same)."""
 import numpy as np
 import pytest
 
-from quantkernel_b200 import (QK_MC_EULER, QK_MC_HESTON, QK_MC_LOCAL_VOL, QK_MC_MILSTEIN,
-                              QK_PLAN_AUTOTUNE, QK_PLAN_FAMILY_GRIDS, QK_PLAN_GRAPH,
-                              QK_PLAN_PERSISTENT, QK_PLAN_TIMING, workloads)
+from quantkernel_b200 import (QK_MC_EULER, QK_MC_HESTON, QK_MC_HESTON_LR_DELTA, QK_MC_LOCAL_VOL,
+                              QK_MC_MILSTEIN, QK_MC_STANDARD, QK_PLAN_AUTOTUNE,
+                              QK_PLAN_FAMILY_GRIDS, QK_PLAN_GRAPH, QK_PLAN_NO_ANTITHETIC,
+                              QK_PLAN_PERSISTENT, QK_PLAN_STEP_UNROLL2, QK_PLAN_TIMING,
+                              workloads)
 
 pytestmark = pytest.mark.gpu
 
@@ -110,3 +112,60 @@ def test_timing_stats_and_device_results(qk):
     dp, ds = plan.device_results()
     assert dp and ds
     plan.close()
+
+
+@pytest.mark.parametrize("model", [QK_MC_EULER, QK_MC_MILSTEIN, QK_MC_LOCAL_VOL, QK_MC_HESTON,
+                                   QK_MC_HESTON_LR_DELTA])
+@pytest.mark.parametrize("anti", [True, False])
+def test_step_unrolling_gives_the_same_bits(qk, model, anti):
+    """Two Philox step blocks per loop iteration (the autotuner's step
+    unrolling) draw the same normals and do the same arithmetic: prices and
+    standard errors equal the default kernel's bit for bit, for step counts
+    that end inside a block, on a block boundary and at one step."""
+    n = 24
+    rng = np.random.default_rng(int(model) * 7 + int(anti))
+    h = workloads.heston(n, paths=2048, steps=8, seed=int(model))
+    h["steps"] = rng.choice([1, 2, 3, 5, 6, 7, 12, 13, 37, 200], n).astype(np.int32)
+    h["paths"] = rng.choice([2, 3, 1001, 2048, 4097], n).astype(np.int32)
+    h["vol"] = rng.uniform(0.1, 0.5, n)
+    if model == QK_MC_HESTON_LR_DELTA:
+        h["vol"] = np.full(n, 6.0)  # the mixed call's weight-clip column
+    extra = 0 if anti else QK_PLAN_NO_ANTITHETIC
+    base = qk.plan(model=np.full(n, model, np.int32), **h, flags=extra)
+    base.execute()
+    p0, s0 = base.results()
+    for upt_flag in (0, QK_PLAN_GRAPH):
+        plan = qk.plan(model=np.full(n, model, np.int32), **h,
+                       flags=extra | upt_flag | QK_PLAN_STEP_UNROLL2)
+        assert plan.config()["step_unroll"] == 2
+        plan.execute()
+        p, s = plan.results()
+        np.testing.assert_array_equal(p, p0)
+        np.testing.assert_array_equal(s, s0)
+        plan.close()
+    assert base.config()["step_unroll"] == 1
+    base.close()
+
+
+def test_autotuner_chooses_step_unrolling(qk):
+    """The autotuner times block size x units per thread x step unrolling for
+    a stepwise plan (and only block x units for a terminal one); whatever it
+    picks, the prices stay those of the default shape to the last bits."""
+    h = workloads.heston(64, paths=16384, steps=48, seed=21)
+    model = np.full(64, QK_MC_HESTON, np.int32)
+    base = qk.plan(model=model, **h)
+    base.execute()
+    p0, _ = base.results()
+    tuned = qk.plan(model=model, **h, flags=QK_PLAN_AUTOTUNE)
+    cfg = tuned.config()
+    assert cfg["step_unroll"] in (1, 2) and cfg["units_per_thread"] in (1, 2, 4)
+    assert cfg["step_unroll"] == 1 or cfg["units_per_thread"] <= 2
+    tuned.execute()
+    p, _ = tuned.results()
+    np.testing.assert_allclose(p, p0, rtol=1e-13, atol=0)
+    b = workloads.bsm_terminal(16, paths=65536, seed=2)
+    term = qk.plan(model=np.full(16, QK_MC_STANDARD, np.int32), steps=np.ones(16, np.int32), **b,
+                   flags=QK_PLAN_AUTOTUNE | QK_PLAN_STEP_UNROLL2)
+    assert term.config()["step_unroll"] == 1
+    for pl in (base, tuned, term):
+        pl.close()
