@@ -141,9 +141,11 @@ __global__ void __launch_bounds__(128)
     const double phi_abs2 = phi_mi.re * phi_mi.re + phi_mi.im * phi_mi.im;
     const double a = 1e-8, width = (o.limit - a) / static_cast<double>(o.panels);
     double s1 = 0.0, s2 = 0.0;
-    const int32_t nodes = o.panels * 64;
-    for (int32_t k = threadIdx.x; k < nodes; k += blockDim.x) {
-        const int32_t p = k >> 6, j = (k >> 1) & 31, side = k & 1;
+    // 64-bit node counter: panels * 64 and the strided index can pass INT32_MAX
+    const int64_t nodes = static_cast<int64_t>(o.panels) * 64;
+    for (int64_t k = threadIdx.x; k < nodes; k += blockDim.x) {
+        const int32_t p = static_cast<int32_t>(k >> 6), j = static_cast<int32_t>((k >> 1) & 31),
+                      side = static_cast<int32_t>(k & 1);
         const double pa = a + static_cast<double>(p) * width;
         const double pb = pa + width;
         const double mid = 0.5 * (pa + pb), half = 0.5 * (pb - pa);
@@ -253,7 +255,7 @@ __global__ void __launch_bounds__(128)
         const double interval = b - a;
         const double inv = 1.0 / interval;
         const double exp_d = exp(dd), exp_c = exp(c);
-        for (int32_t k = threadIdx.x; k < o.panels; k += blockDim.x) {
+        for (int64_t k = threadIdx.x; k < o.panels; k += blockDim.x) {  // 64-bit: no wrap
             const double u = static_cast<double>(k) * kPi * inv;
             double chi, psi;
             if (k == 0) {
@@ -360,7 +362,8 @@ CfOption pack_cf_option(double spot, double strike, double t, double r, double q
     o.rho = rho;
     o.limit = limit;
     o.option_type = ot;
-    o.panels = (steps + 63) / 64 > 1 ? (steps + 63) / 64 : 1;
+    const int64_t panels = (static_cast<int64_t>(steps) + 63) / 64;  // no int32 overflow
+    o.panels = static_cast<int32_t>(panels > 1 ? panels : 1);
     return o;
 }
 

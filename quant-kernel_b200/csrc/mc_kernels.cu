@@ -161,6 +161,7 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
         su[k] = 1.0f;
         sd[k] = 1.0f;
     }
+    // steps <= kMaxSteps (checked when packing), so j0 + 12 never wraps
     uint32_t blk = 0;  // step block j / 6
     for (int32_t j0 = 0; j0 < steps; j0 += 6 * SU, blk += SU) {
         Philox6 rb[SU][UPT];
@@ -250,6 +251,7 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         vd[k] = v0;
         zfirst[k] = 0.0f;
     }
+    // steps <= kMaxSteps (checked when packing), so j0 + 6 never wraps
     uint32_t blk = 0;  // step block j / 3
     for (int32_t j0 = 0; j0 < steps; j0 += 3 * SU, blk += SU) {
         Philox6 rb[SU][UPT];

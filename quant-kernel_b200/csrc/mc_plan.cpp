@@ -158,7 +158,8 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
         const double vol = in.vol[i], r = in.r[i], q = in.q[i];
         const int32_t steps = geti(in.steps, i, 0);
         o.steps = steps;
-        if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) || !(paths > 1 && steps > 0)) {
+        if (!valid_common_inputs(spot, strike, t, vol, r, q, ot) ||
+            !(paths > 1 && steps > 0 && steps <= kMaxSteps)) {
             set_const(o, nan_value());
             return o;
         }
@@ -192,7 +193,7 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
         const double clip = (m == kHestonLrDelta) ? (in.weight_clip ? in.weight_clip[i] : in.vol[i]) : 1.0;
         if (!valid_option_type(ot) || spot <= 0.0 || strike <= 0.0 || t < 0.0 || v0 < 0.0 ||
             kappa < 0.0 || theta < 0.0 || sigma < 0.0 || rho < -1.0 || rho > 1.0 ||
-            !(paths > 1 && steps > 0) || !(clip > 0.0)) {
+            !(paths > 1 && steps > 0 && steps <= kMaxSteps) || !(clip > 0.0)) {
             set_const(o, nan_value());
             return o;
         }

@@ -5,6 +5,11 @@
 
 namespace qkb {
 
+// Largest step count a stepwise option may have: the kernels count steps in
+// int32 blocks of up to 12, so the last block's index must not wrap.  Larger
+// counts (over 2.1e9 steps per path) are rejected as invalid input (NaN).
+constexpr int32_t kMaxSteps = 0x7FFFFFFF - 64;
+
 // ---------------------------------------------------------------------------
 // Model codes (same values as QK_MC_* in include/qk_api.h).
 // ---------------------------------------------------------------------------

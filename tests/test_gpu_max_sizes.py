@@ -72,3 +72,22 @@ def test_tile_cap_for_long_options(qk):
                                                                   "steps", "seed")))
     assert one == p[1]
     assert math.isfinite(one)
+
+
+def test_step_counts_past_the_cap_are_invalid(qk):
+    """Step counts within 64 of INT32_MAX (over 2.1e9 steps per path) would
+    wrap the kernels' int32 step-block index; they price as invalid input
+    (NaN), like a non-positive count, without launching a simulation."""
+    for steps in (MAX_PATHS, MAX_PATHS - 63):
+        a = _one(paths=np.array([1000], np.int32), steps=np.array([steps], np.int32),
+                 seed=np.array([1], np.uint64))
+        p, se = qk.euler_maruyama_price_se_batch(**a)
+        assert np.isnan(p[0]) and np.isnan(se[0])
+        h = dict(spot=np.array([100.0]), strike=np.array([100.0]), t=np.array([1.0]),
+                 r=np.array([0.03]), q=np.array([0.0]), v0=np.array([0.04]),
+                 kappa=np.array([2.0]), theta=np.array([0.04]), sigma=np.array([0.3]),
+                 rho=np.array([-0.7]), option_type=np.array([0], np.int32),
+                 paths=np.array([1000], np.int32), steps=np.array([steps], np.int32),
+                 seed=np.array([1], np.uint64))
+        p, se = qk.heston_monte_carlo_price_se_batch(**h)
+        assert np.isnan(p[0]) and np.isnan(se[0])
