@@ -149,16 +149,24 @@ __device__ __forceinline__ void load_bf16x32(const __nv_bfloat16* src, float (&v
     }
 }
 
+// Eight epilogue warps: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its tile
+// rows) and the column half w / 4 of the tile (chunks of 32 columns
+// [c_lo, c_hi)); every element's arithmetic is the same as with one warp per
+// lane quarter, so the split changes no bits.
 template <int BN, int EPI>
-__device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m0, int n0) {
+__device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m0, int n0,
+                                         float (*part_s)[kBM]) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = m0 + warp * 32 + lane;
+    const int q = warp & 3, half = warp >> 2;
+    const int row = m0 + q * 32 + lane;
     const bool live = row < a.M;
-    const uint32_t tbase = tmem + (static_cast<uint32_t>(warp * 32) << 16);
+    const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16);
+    constexpr int kChunks = BN / 32;
+    const int c_lo = half * (kChunks / 2), c_hi = c_lo + kChunks / 2;
     float v[32];
     if (EPI == kEpiF32) {
 #pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
+        for (int c = c_lo; c < c_hi; ++c) {
             tmem_ld32(tbase + c * 32, v);
             if (live) {
                 float4* dst = reinterpret_cast<float4*>(
@@ -169,7 +177,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
         }
     } else if (EPI == kEpiFwd) {
 #pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
+        for (int c = c_lo; c < c_hi; ++c) {
             tmem_ld32(tbase + c * 32, v);
             const int col0 = n0 + c * 32;
             float z[32];
@@ -190,7 +198,7 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
         }
     } else if (EPI == kEpiBwd) {
 #pragma unroll 1
-        for (int c = 0; c < BN / 32; ++c) {
+        for (int c = c_lo; c < c_hi; ++c) {
             tmem_ld32(tbase + c * 32, v);
             const int col0 = n0 + c * 32;
             if (live) {
@@ -208,11 +216,12 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
             }
         }
     } else {  // kEpiLast: BN == N (the whole hidden row is in this CTA)
-        // head dot product as four partial sums over columns 64g .. 64g + 63,
-        // combined in order -- the summation the fused inference kernel uses
-        float part[4];
+        // head dot product as four partial sums over columns 64g .. 64g + 63
+        // (this warp's half: groups 2 half, 2 half + 1), combined in order --
+        // the summation the fused inference kernel uses
 #pragma unroll
-        for (int g = 0; g < 4; ++g) {
+        for (int gg = 0; gg < 2; ++gg) {
+            const int g = 2 * half + gg;
             float p = 0.0f;  // one fmaf chain over the group's 64 columns
 #pragma unroll 1
             for (int cc = 0; cc < 2; ++cc) {
@@ -224,16 +233,18 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
                     p = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), p);
                 }
             }
-            part[g] = p;
+            part_s[g][q * 32 + lane] = p;
         }
-        float y = ((part[0] + part[1]) + part[2]) + part[3];
+        __syncthreads();  // all eight warps run the epilogue
+        const int r = q * 32 + lane;
+        float y = ((part_s[0][r] + part_s[1][r]) + part_s[2][r]) + part_s[3][r];
         y += __ldg(a.b4);
-        if (live) a.y_out[row] = a.base ? y + __ldg(a.base + row) : y;
+        if (live && half == 0) a.y_out[row] = a.base ? y + __ldg(a.base + row) : y;
         if (a.target != nullptr) {
             const float dy = live ? a.loss_scale * (y - a.target[row]) : 0.0f;
-            if (live) a.dy_out[row] = dy;
+            if (live && half == 0) a.dy_out[row] = dy;
 #pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
+            for (int c = c_lo; c < c_hi; ++c) {
                 tmem_ld32(tbase + c * 32, v);
                 const int col0 = c * 32;
                 float h[32];
@@ -257,8 +268,10 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
     }
 }
 
+constexpr int kGemmThreads = 256;  // warp 0: TMA, warp 1: MMA; all 8 warps: epilogue
+
 template <int BN, int EPI>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(kGemmThreads, 1)
     umma_gemm_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
                      const GemmArgs a) {
     constexpr uint32_t kBBytes = BN * kBK * 2;
@@ -271,6 +284,7 @@ __global__ void __launch_bounds__(128, 1)
     __shared__ __align__(8) uint64_t acc_bar;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
+    __shared__ float part_s[4][kBM];  // head partial sums (kEpiLast)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * BN;
@@ -354,7 +368,7 @@ __global__ void __launch_bounds__(128, 1)
         abort_flag = 1;
     }
     __syncthreads();
-    if (!abort_flag && nkb > 0) epilogue<BN, EPI>(a, tmem, m0, n0);
+    if (!abort_flag && nkb > 0) epilogue<BN, EPI>(a, tmem, m0, n0, part_s);
 
     // Teardown: the producer drains its own loads (bounded), then TMEM is freed.
     if (warp == 0 && lane == 0 && abort_flag) {
@@ -630,7 +644,7 @@ cudaError_t launch_t(const CUtensorMap& ta, const CUtensorMap& tb, const GemmArg
     });
     if (attr_err != cudaSuccess) return attr_err;
     dim3 grid((a.M + kBM - 1) / kBM, a.N / BN, splits);
-    umma_gemm_kernel<BN, EPI><<<grid, 128, smem, st>>>(ta, tb, a);
+    umma_gemm_kernel<BN, EPI><<<grid, kGemmThreads, smem, st>>>(ta, tb, a);
     return cudaGetLastError();
 }
 
