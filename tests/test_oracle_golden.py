@@ -194,6 +194,19 @@ def test_philox_matches_python_restatement(oracle):
     assert oracle.philox([0, 0, 0, 0], [0, 0]) == _philox_py([0, 0, 0, 0], [0, 0])
 
 
+def test_philox_published_known_answers(oracle):
+    """Philox4x32-10 known-answer vectors published with the algorithm
+    (Salmon et al., SC'11; the Random123 distribution's kat_vectors): zero
+    counter and key, all-ones, and the digits of pi."""
+    kat = [([0, 0, 0, 0], [0, 0], [0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8]),
+           ([0xFFFFFFFF] * 4, [0xFFFFFFFF] * 2, [0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD]),
+           ([0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344], [0xA4093822, 0x299F31D0],
+            [0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1])]
+    for ctr, key, want in kat:
+        assert list(oracle.philox(ctr, key)) == want
+        assert list(_philox_py(ctr, key)) == want
+
+
 def test_philox_box_muller_layout(oracle):
     seed = 0x123456789ABCDEF
     key = [seed & 0xFFFFFFFF, seed >> 32]
