@@ -398,9 +398,11 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 //
 // Ring schedule (loads are numbered wl = 9 t + i within the CTA): a load is
 // issued only when the previous user of its slot (load wl - 4) belongs to a
-// layer whose accumulator is already complete -- loads 0-3 at the start of a
-// tile (previous users: the last tile's W3), load 4 after layer 1, loads 5-8
-// after layer 2 -- so the producer never waits on work issued later.
+// layer whose accumulator is already complete -- loads 0-3 of a tile when the
+// previous tile's layer 3 completes (previous users: that tile's W3; the
+// first tile issues them at the start), load 4 after layer 1, loads 5-8 after
+// layer 2 -- so the producer never waits on work issued later, and every
+// load flies during an epilogue.
 // The arithmetic and summation order are those of the layer-by-layer GEMMs
 // (kEpiFwd, kEpiLast), so the results are the same bits.
 // ----------------------------------------------------------------------------
@@ -555,9 +557,10 @@ __global__ void __launch_bounds__(kInferThreads, 1)
 
     int it = 0;
     for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
-        // layer 1: H = silu(X W1^T + b1)
-        if (tid == 0) {
-            if (it == 0) load_x(t);
+        // layer 1: H = silu(X W1^T + b1).  The tile's first four weight loads
+        // were issued when the previous tile's layer-3 accumulator completed.
+        if (tid == 0 && it == 0) {
+            load_x(t);
             if (!(load_w(&tw1, 0) && load_w(&tw2, 0) && load_w(&tw2, 64) && load_w(&tw2, 128)))
                 fail(11);
         } else if (tid == 32) {
@@ -585,6 +588,12 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             if (!mma_layer(hbuf, 4)) fail(12);
         }
         if (!acc_ready()) break;
+        // the next tile's W1 and W2[0..2]: their slots' previous users (this
+        // tile's W3 k-blocks) are complete with the accumulator, so the loads
+        // fly while the head epilogue runs instead of after it
+        if (tid == 0 && t + gridDim.x < n_tiles &&
+            !(load_w(&tw1, 0) && load_w(&tw2, 0) && load_w(&tw2, 64) && load_w(&tw2, 128)))
+            fail(11);
         {
             float v[32];
             float p = 0.0f;  // one fmaf chain over this group's 64 columns
