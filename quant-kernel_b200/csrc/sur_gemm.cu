@@ -113,6 +113,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // sigmoid(z) = (1 + tanh(z / 2)) / 2 with the MUFU tanh (one special-function
 // op; |error| ~ 2^-11, below the bf16 rounding every activation gets next).
 __device__ __forceinline__ float tanh_approx(float x) {
@@ -216,25 +218,28 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
             }
         }
     } else {  // kEpiLast: BN == N (the whole hidden row is in this CTA)
-        // head dot product as four partial sums over columns 64g .. 64g + 63
-        // (this warp's half: groups 2 half, 2 half + 1), combined in order --
-        // the summation the fused inference kernel uses
-#pragma unroll
-        for (int gg = 0; gg < 2; ++gg) {
-            const int g = 2 * half + gg;
-            float p = 0.0f;  // one fmaf chain over the group's 64 columns
+        // head dot product as four partial sums, group g over the columns
+        // 64 kb + 16 g + j (kb = 0..3, j = 0..15, in that order), combined in
+        // order -- the summation of the fused inference kernel, whose warp g
+        // owns those columns.  This warp's half takes groups 2 half, 2 half + 1.
+        float p0 = 0.0f, p1 = 0.0f;
 #pragma unroll 1
-            for (int cc = 0; cc < 2; ++cc) {
-                const int col0 = (2 * g + cc) * 32;
-                tmem_ld32(tbase + col0, v);
+        for (int kb = 0; kb < 4; ++kb) {
+            const int col0 = kb * 64 + half * 32;  // groups 2 half (16 cols), 2 half + 1 (16)
+            tmem_ld32(tbase + col0, v);
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const float z = v[j] + __ldg(a.bias + col0 + j);
-                    p = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), p);
-                }
+            for (int j = 0; j < 16; ++j) {
+                const float z = v[j] + __ldg(a.bias + col0 + j);
+                p0 = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), p0);
             }
-            part_s[g][q * 32 + lane] = p;
+#pragma unroll
+            for (int j = 16; j < 32; ++j) {
+                const float z = v[j] + __ldg(a.bias + col0 + j);
+                p1 = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), p1);
+            }
         }
+        part_s[2 * half][q * 32 + lane] = p0;
+        part_s[2 * half + 1][q * 32 + lane] = p1;
         __syncthreads();  // all eight warps run the epilogue
         const int r = q * 32 + lane;
         float y = ((part_s[0][r] + part_s[1][r]) + part_s[2][r]) + part_s[3][r];
@@ -387,22 +392,33 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
 
 // ----------------------------------------------------------------------------
-// Fused MLP inference.  One persistent CTA per SM (512 threads) walks 128-row
-// tiles: layer 1 (K = 64), layer 2 and layer 3 (K = 256) run back to back on
-// one TMEM accumulator (128 x 256 fp32); each hidden activation tile goes
-// from TMEM through the bias + SiLU epilogue into shared memory, written in
-// the 128-byte-swizzled K-major layout the next layer's MMA reads as its A
-// operand, so activations never leave the SM.  Weights stream from L2 through
-// a 4-slot ring of 32 KiB k-blocks (W1, W2[0..3], W3[0..3] per tile: nine
-// loads); the next tile's input rows are prefetched during layer 2.
-//
-// Ring schedule (loads are numbered wl = 9 t + i within the CTA): a load is
-// issued only when the previous user of its slot (load wl - 4) belongs to a
-// layer whose accumulator is already complete -- loads 0-3 of a tile when the
-// previous tile's layer 3 completes (previous users: that tile's W3; the
-// first tile issues them at the start), load 4 after layer 1, loads 5-8 after
-// layer 2 -- so the producer never waits on work issued later, and every
-// load flies during an epilogue.
+// Fused MLP inference.  One persistent CTA per SM walks 128-row tiles with
+// three warp roles:
+//   warp 16 (one lane)  TMA producer: per tile the input rows X and the nine
+//                       32 KiB weight k-blocks W1, W2[0..3], W3[0..3] through
+//                       a 4-slot ring (a slot is reloaded once the MMA that
+//                       read it has completed);
+//   warp 17 (one lane)  MMA issuer: layer 1 (K = 64), then layers 2 and 3 k-block
+//                       by k-block, each k-block as soon as the epilogue has
+//                       written that 64-column block of the previous layer's
+//                       activations;
+//   warps 0-15          epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
+//                       (its tile rows) and, in each 64-column block kb,
+//                       columns 64 kb + 16 (w / 4) .. + 15; bias + SiLU, BF16
+//                       into shared memory in the 128-byte-swizzled K-major
+//                       layout the next layer's MMA reads as its A operand.
+// Two TMEM accumulators (2 x 256 columns) alternate between consecutive
+// layers, so layer l + 1's MMAs run while layer l's epilogue is still
+// reading: all 16 epilogue warps finish block kb of the activations before
+// any starts block kb + 1, and the MMA issuer takes the blocks in that order.
+// Every hand-off is an mbarrier with a bounded wait (no CTA-wide barrier
+// inside the loop), so a timeout anywhere ends every role with an error code.
+// Hazards, each closed by the order of the chain: a layer's accumulator is
+// rewritten two layers later, after every epilogue warp has reported the
+// intervening layer's activations (or, for the head, the next tile's first
+// layer); the activation buffer is rewritten only after the accumulator
+// commit of the layer that read it; the input rows are reloaded after the
+// commit of the layer-1 MMAs.
 // The arithmetic and summation order are those of the layer-by-layer GEMMs
 // (kEpiFwd, kEpiLast), so the results are the same bits.
 // ----------------------------------------------------------------------------
@@ -410,16 +426,34 @@ constexpr int kIWSlots = 4;
 constexpr uint32_t kWBlock = 256 * kBK * 2;        // 32 KiB: 256 rows x 64 bf16
 constexpr uint32_t kHBytes = 4 * kABytes;          // 64 KiB: 128 rows x 256 bf16
 constexpr size_t kInferSmem = kHBytes + kABytes + kIWSlots * kWBlock + 1024;
-constexpr int kInferThreads = 512;                 // 16 warps: 4 per TMEM lane quarter
+constexpr int kInferEpiWarps = 16;                 // 4 per TMEM lane quarter
+constexpr int kInferThreads = (kInferEpiWarps + 2) * 32;
+constexpr int kProducerWarp = kInferEpiWarps, kMmaWarp = kInferEpiWarps + 1;
 
-// 32 activations (columns col0 .. col0 + 31 of tile row r) into the layout a
-// 128-byte-swizzle TMA load would produce: k-block col / 64, row r at 128 r,
-// 16-byte chunk c at (c ^ (r & 7)) * 16.
-__device__ __forceinline__ void store_h_sw128(uint8_t* hbuf, int r, int col0, const float (&v)[32]) {
+// 16 consecutive fp32 columns of this thread's TMEM lane (no wait).
+__device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// 16 activations (columns col0 .. col0 + 15 of tile row r, col0 % 16 == 0)
+// into the layout a 128-byte-swizzle TMA load would produce: k-block
+// col / 64, row r at 128 r, 16-byte chunk c at (c ^ (r & 7)) * 16.
+__device__ __forceinline__ void store_h16_sw128(uint8_t* hbuf, int r, int col0, const float (&v)[16]) {
     uint8_t* row = hbuf + (col0 >> 6) * kABytes + r * 128;
     const int c0 = (col0 & 63) >> 3;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < 2; ++q) {
         __nv_bfloat162 p[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) p[j] = __floats2bfloat162_rn(v[q * 8 + 2 * j], v[q * 8 + 2 * j + 1]);
@@ -437,7 +471,9 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     uint8_t* hbuf = smem;
     uint8_t* xbuf = smem + kHBytes;
     uint8_t* wbuf = xbuf + kABytes;
-    __shared__ __align__(8) uint64_t xfull, accbar, drain;
+    __shared__ __align__(8) uint64_t xfull, xempty, drain, pready;
+    __shared__ __align__(8) uint64_t accfull[2];
+    __shared__ __align__(8) uint64_t hfull[4];
     __shared__ __align__(8) uint64_t wfull[kIWSlots];
     __shared__ __align__(8) uint64_t wempty[kIWSlots];
     __shared__ float sb1[kSurHidden], sb2[kSurHidden], sb3[kSurHidden], sw4[kSurHidden];
@@ -446,10 +482,6 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     __shared__ volatile int abort_flag;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // epilogue mapping: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its tile
-    // rows) and columns 64 (w / 4) .. + 63 (its column group)
-    const int q = warp & 3, grp = warp >> 2;
-    const int r = q * 32 + lane;
     const int64_t n_tiles = (a.n + kBM - 1) / kBM;
 
     if (tid < kSurHidden) {
@@ -460,8 +492,11 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     }
     if (tid == 0) {
         mbar_init(smem_u32(&xfull), 1);
-        mbar_init(smem_u32(&accbar), 1);
+        mbar_init(smem_u32(&xempty), 1);
         mbar_init(smem_u32(&drain), 1);
+        mbar_init(smem_u32(&pready), kInferEpiWarps);
+        for (int i = 0; i < 2; ++i) mbar_init(smem_u32(&accfull[i]), 1);
+        for (int kb = 0; kb < 4; ++kb) mbar_init(smem_u32(&hfull[kb]), kInferEpiWarps);
         for (int s = 0; s < kIWSlots; ++s) {
             mbar_init(smem_u32(&wfull[s]), 1);
             mbar_init(smem_u32(&wempty[s]), 1);
@@ -469,10 +504,10 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (warp == 0) {  // two accumulators of 256 fp32 columns
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_slot)),
-                     "r"(256u)
+                     "r"(512u)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -480,154 +515,193 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     __syncthreads();
     fence_after();
     const uint32_t tmem = tmem_slot;
-    const uint32_t tbase = tmem + (static_cast<uint32_t>(q * 32) << 16);
-    const float b4 = __ldg(a.b4);
-    constexpr uint32_t idesc = idesc_bf16<256>();
-
-    // producer state (thread 0) and MMA state (thread 32)
-    uint32_t wl = 0, wc = 0, ap = 0, xl = 0;
-    int last_round[kIWSlots] = {-1, -1, -1, -1};
-    bool x_pending = false;        // an input-row load not yet consumed
-    uint32_t x_pending_parity = 0;
-
-    auto load_w = [&](const CUtensorMap* m, int kx) -> bool {
-        const uint32_t s = wl % kIWSlots, round = wl / kIWSlots;
-        if (round > 0 && !mbar_wait(smem_u32(&wempty[s]), (round - 1) & 1)) return false;
-        mbar_expect_tx(smem_u32(&wfull[s]), kWBlock);
-        tma_load_2d(smem_u32(wbuf + s * kWBlock), m, kx, 0, smem_u32(&wfull[s]));
-        last_round[s] = static_cast<int>(round);
-        ++wl;
-        return true;
-    };
-    auto load_x = [&](int64_t tile) {  // load number xl; tile iteration xl waits on it
-        mbar_expect_tx(smem_u32(&xfull), kABytes);
-        tma_load_2d(smem_u32(xbuf), &tx, 0, static_cast<int>(tile * kBM), smem_u32(&xfull));
-        x_pending = true;
-        x_pending_parity = xl & 1;
-        ++xl;
-    };
-    auto mma_layer = [&](const uint8_t* abase, int nkb) -> bool {
-        for (int kb = 0; kb < nkb; ++kb) {
-            const uint32_t s = wc % kIWSlots;
-            if (!mbar_wait(smem_u32(&wfull[s]), (wc / kIWSlots) & 1)) return false;
-            fence_after();
-            const uint32_t sa = smem_u32(abase + kb * kABytes), sb = smem_u32(wbuf + s * kWBlock);
-#pragma unroll
-            for (int kk = 0; kk < kBK / 16; ++kk)
-                umma_bf16(tmem, desc_sw128(sa + kk * 32), desc_sw128(sb + kk * 32), idesc,
-                          (kb | kk) != 0 ? 1u : 0u);
-            umma_commit(smem_u32(&wempty[s]));
-            ++wc;
-        }
-        umma_commit(smem_u32(&accbar));
-        return true;
-    };
     auto fail = [&](int code) {
         abort_flag = 1;
         atomicExch(a.err, code);
     };
-    // all threads: the layer's accumulator is complete
-    auto acc_ready = [&]() -> bool {
-        __syncwarp();
-        const bool ok = mbar_wait(smem_u32(&accbar), ap & 1);
-        ++ap;
-        __syncwarp();
-        fence_after();
-        if (!ok && lane == 0) fail(13);
-        __syncthreads();
-        return abort_flag == 0;
-    };
-    auto epi_hidden = [&](const float* bias) {
-        float v[32];
-#pragma unroll 1
-        for (int cc = 0; cc < 2; ++cc) {
-            const int col0 = (2 * grp + cc) * 32;
-            tmem_ld32(tbase + col0, v);
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const float z = v[j] + bias[col0 + j];
-                v[j] = z * sigmoidf_(z);
-            }
-            store_h_sw128(hbuf, r, col0, v);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        fence_before();
-        __syncthreads();
-    };
 
-    int it = 0;
-    for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
-        // layer 1: H = silu(X W1^T + b1).  The tile's first four weight loads
-        // were issued when the previous tile's layer-3 accumulator completed.
-        if (tid == 0 && it == 0) {
-            load_x(t);
-            if (!(load_w(&tw1, 0) && load_w(&tw2, 0) && load_w(&tw2, 64) && load_w(&tw2, 128)))
-                fail(11);
-        } else if (tid == 32) {
-            if (!mbar_wait(smem_u32(&xfull), it & 1) || !mma_layer(xbuf, 1)) fail(12);
-        }
-        if (!acc_ready()) break;
-        if (tid == 0) x_pending = false;  // consumed by layer 1
-        epi_hidden(sb1);
-        // layer 2: H = silu(H W2^T + b2); the next tile's rows load meanwhile
-        if (tid == 0) {
-            if (t + gridDim.x < n_tiles) load_x(t + gridDim.x);
-            if (!load_w(&tw2, 192)) fail(11);
-        } else if (tid == 32) {
-            fence_after();
-            if (!mma_layer(hbuf, 4)) fail(12);
-        }
-        if (!acc_ready()) break;
-        epi_hidden(sb2);
-        // layer 3 and the head: y = silu(H W3^T + b3) . w4 + b4
-        if (tid == 0) {
-            if (!(load_w(&tw3, 0) && load_w(&tw3, 64) && load_w(&tw3, 128) && load_w(&tw3, 192)))
-                fail(11);
-        } else if (tid == 32) {
-            fence_after();
-            if (!mma_layer(hbuf, 4)) fail(12);
-        }
-        if (!acc_ready()) break;
-        // the next tile's W1 and W2[0..2]: their slots' previous users (this
-        // tile's W3 k-blocks) are complete with the accumulator, so the loads
-        // fly while the head epilogue runs instead of after it
-        if (tid == 0 && t + gridDim.x < n_tiles &&
-            !(load_w(&tw1, 0) && load_w(&tw2, 0) && load_w(&tw2, 64) && load_w(&tw2, 128)))
-            fail(11);
-        {
-            float v[32];
-            float p = 0.0f;  // one fmaf chain over this group's 64 columns
-#pragma unroll 1
-            for (int cc = 0; cc < 2; ++cc) {
-                const int col0 = (2 * grp + cc) * 32;
-                tmem_ld32(tbase + col0, v);
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const float z = v[j] + sb3[col0 + j];
-                    p = fmaf(z * sigmoidf_(z), sw4[col0 + j], p);
+    // producer bookkeeping for the teardown drain
+    int last_round[kIWSlots] = {-1, -1, -1, -1};
+    int x_loads = 0;
+
+    if (warp == kProducerWarp) {
+        if (lane == 0) {
+            uint32_t wl = 0;
+            int it = 0;
+            auto load_w = [&](const CUtensorMap* m, int kx) -> bool {
+                const uint32_t s = wl % kIWSlots, round = wl / kIWSlots;
+                if (round > 0 && !mbar_wait(smem_u32(&wempty[s]), (round - 1) & 1)) return false;
+                mbar_expect_tx(smem_u32(&wfull[s]), kWBlock);
+                tma_load_2d(smem_u32(wbuf + s * kWBlock), m, kx, 0, smem_u32(&wfull[s]));
+                last_round[s] = static_cast<int>(round);
+                ++wl;
+                return true;
+            };
+            for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+                if (abort_flag) break;
+                if (it > 0 && !mbar_wait(smem_u32(&xempty), (it - 1) & 1)) {
+                    fail(21);
+                    break;
+                }
+                mbar_expect_tx(smem_u32(&xfull), kABytes);
+                tma_load_2d(smem_u32(xbuf), &tx, 0, static_cast<int>(t * kBM), smem_u32(&xfull));
+                ++x_loads;
+                bool ok = load_w(&tw1, 0);
+                for (int kb = 0; ok && kb < 4; ++kb) ok = load_w(&tw2, kb * kBK);
+                for (int kb = 0; ok && kb < 4; ++kb) ok = load_w(&tw3, kb * kBK);
+                if (!ok) {
+                    fail(22);
+                    break;
                 }
             }
-            part[grp][r] = p;
         }
-        fence_before();
-        __syncthreads();
-        if (grp == 0) {
-            const float y = (((part[0][r] + part[1][r]) + part[2][r]) + part[3][r]) + b4;
-            const int64_t row = t * kBM + r;
-            if (row < a.n) a.y[row] = a.base ? y + __ldg(a.base + row) : y;
+    } else if (warp == kMmaWarp) {
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16<256>();
+            uint32_t wc = 0, L = 0, hp = 0;
+            int it = 0;
+            // one k-block of W from the ring into accumulator acc
+            auto mma_kblock = [&](uint32_t acc, uint32_t sa, bool first) -> bool {
+                const uint32_t s = wc % kIWSlots;
+                if (!mbar_wait(smem_u32(&wfull[s]), (wc / kIWSlots) & 1)) return false;
+                fence_after();
+                const uint32_t sb = smem_u32(wbuf + s * kWBlock);
+#pragma unroll
+                for (int kk = 0; kk < kBK / 16; ++kk)
+                    umma_bf16(acc, desc_sw128(sa + kk * 32), desc_sw128(sb + kk * 32), idesc,
+                              (first && kk == 0) ? 0u : 1u);
+                umma_commit(smem_u32(&wempty[s]));
+                ++wc;
+                return true;
+            };
+            for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+                if (abort_flag) break;
+                if (!mbar_wait(smem_u32(&xfull), it & 1)) {
+                    fail(23);
+                    break;
+                }
+                // layer 1 (K = 64)
+                uint32_t acc = tmem + (L & 1) * 256;
+                if (!mma_kblock(acc, smem_u32(xbuf), true)) {
+                    fail(24);
+                    break;
+                }
+                umma_commit(smem_u32(&xempty));
+                umma_commit(smem_u32(&accfull[L & 1]));
+                ++L;
+                // layers 2 and 3, k-block by k-block behind the epilogue
+                bool ok = true;
+                for (int l = 1; ok && l <= 2; ++l) {
+                    acc = tmem + (L & 1) * 256;
+                    for (int kb = 0; ok && kb < 4; ++kb) {
+                        ok = mbar_wait(smem_u32(&hfull[kb]), hp & 1);
+                        if (ok) ok = mma_kblock(acc, smem_u32(hbuf + kb * kABytes), kb == 0);
+                    }
+                    ++hp;
+                    if (ok) umma_commit(smem_u32(&accfull[L & 1]));
+                    ++L;
+                }
+                if (!ok) {
+                    fail(25);
+                    break;
+                }
+            }
         }
-        // part[] is next written after two more barriers of the next tile
+    } else {
+        // epilogue warps; lane 0 polls each barrier and broadcasts the
+        // outcome, so a warp's lanes always take the same path; then every
+        // lane observes the completed phase itself (its own acquire: the
+        // phase cannot advance again before this warp's next arrival)
+        auto warp_wait = [&](uint32_t bar, uint32_t parity) -> bool {
+            bool done = false;
+            if (lane == 0) done = mbar_wait(bar, parity);
+            done = __shfl_sync(0xFFFFFFFFu, done ? 1 : 0, 0) != 0;
+            if (done) done = __all_sync(0xFFFFFFFFu, mbar_try(bar, parity)) != 0;
+            return done;
+        };
+        const int q = warp & 3, g = warp >> 2;
+        const int r = q * 32 + lane;
+        const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
+        const float b4 = __ldg(a.b4);
+        uint32_t L = 0;
+        int it = 0;
+        bool ok = true;
+        for (int64_t t = blockIdx.x; ok && t < n_tiles; t += gridDim.x, ++it) {
+            for (int l = 0; ok && l < 3; ++l, ++L) {
+                const uint32_t acc = tmem + (L & 1) * 256 + lane_off;
+                ok = warp_wait(smem_u32(&accfull[L & 1]), (L >> 1) & 1);
+                fence_after();
+                if (!ok) {
+                    if (lane == 0) fail(26);
+                    break;
+                }
+                if (l < 2) {
+                    const float* bias = l == 0 ? sb1 : sb2;
+#pragma unroll 1
+                    for (int kb = 0; kb < 4; ++kb) {
+                        const int col0 = kb * 64 + g * 16;
+                        uint32_t u[16];
+                        tmem_ld16_async(acc + col0, u);
+                        tmem_wait_ld();
+                        float v[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const float z = __uint_as_float(u[j]) + bias[col0 + j];
+                            v[j] = z * sigmoidf_(z);
+                        }
+                        store_h16_sw128(hbuf, r, col0, v);
+                        // the shared stores to the tensor core's (async) proxy,
+                        // the TMEM reads before the hand-off
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(smem_u32(&hfull[kb]));
+                    }
+                } else {
+                    // head: this warp's chain over columns 64 kb + 16 g + j
+                    float p = 0.0f;
+#pragma unroll 1
+                    for (int kb = 0; kb < 4; ++kb) {
+                        const int col0 = kb * 64 + g * 16;
+                        uint32_t u[16];
+                        tmem_ld16_async(acc + col0, u);
+                        tmem_wait_ld();
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const float z = __uint_as_float(u[j]) + sb3[col0 + j];
+                            p = fmaf(z * sigmoidf_(z), sw4[col0 + j], p);
+                        }
+                    }
+                    part[g][r] = p;
+                    fence_before();
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&pready));
+                    if (g == 0) {
+                        ok = warp_wait(smem_u32(&pready), it & 1);
+                        if (!ok) {
+                            if (lane == 0) fail(27);
+                            break;
+                        }
+                        const float y = (((part[0][r] + part[1][r]) + part[2][r]) + part[3][r]) + b4;
+                        const int64_t row = t * kBM + r;
+                        if (row < a.n) a.y[row] = a.base ? y + __ldg(a.base + row) : y;
+                    }
+                }
+            }
+        }
     }
 
     // Teardown.  After an abort: the producer waits (bounded) for the loads
-    // it issued, the MMA thread for its MMAs (a commit on `drain`), then the
-    // accumulator is freed.
+    // it issued, the MMA issuer for its MMAs (a commit on `drain`), then the
+    // accumulators are freed.
+    fence_before();
+    __syncthreads();
     if (abort_flag) {
-        if (tid == 0) {
+        if (warp == kProducerWarp && lane == 0) {
             for (int s = 0; s < kIWSlots; ++s)
                 if (last_round[s] >= 0) mbar_wait(smem_u32(&wfull[s]), last_round[s] & 1);
-            if (x_pending) mbar_wait(smem_u32(&xfull), x_pending_parity);
-        } else if (tid == 32) {
+            if (x_loads > 0) mbar_wait(smem_u32(&xfull), (x_loads - 1) & 1);
+        } else if (warp == kMmaWarp && lane == 0) {
             umma_commit(smem_u32(&drain));
             mbar_wait(smem_u32(&drain), 0);
         }
@@ -636,7 +710,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     __syncthreads();
     if (warp == 0) {
         fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(256u)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512u)
                      : "memory");
     }
 }
