@@ -92,11 +92,47 @@ def _cpu_sample_batch(n_opt, paths):
     return {k: v[:n_opt] for k, v in h.items()}
 
 
+HESTON_KEYS = ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho",
+               "option_type", "paths", "steps", "seed")
+CPU_TIMER = ROOT / "oracle" / "_ref" / "cpu_timer"
+
+
+def _time_cpu_cxx(b):
+    """The compiled reference's qk_mcm_heston_monte_carlo_price_batch timed by
+    the C++ harness (oracle/cpu_timer.cpp, std::chrono around the call)."""
+    import tempfile
+
+    from oracle import oracle as orc
+
+    n = len(b["spot"])
+    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
+        f.write(np.int32(n).tobytes())
+        for k in HESTON_KEYS[:10]:
+            f.write(np.ascontiguousarray(b[k], np.float64).tobytes())
+        for k in ("option_type", "paths", "steps"):
+            f.write(np.ascontiguousarray(b[k], np.int32).tobytes())
+        f.write(np.ascontiguousarray(b["seed"], np.uint64).tobytes())
+        path = f.name
+    try:
+        r = subprocess.run([str(CPU_TIMER), str(orc.REF_SO), "qk_mcm_heston_monte_carlo_price_batch",
+                            path, "1"], capture_output=True, text=True, timeout=1800)
+    finally:
+        os.unlink(path)
+    if r.returncode != 0:
+        raise RuntimeError(f"cpu_timer failed: {r.stderr[-1000:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])["seconds"][0]
+
+
 def _time_cpu(impl, n_opt, paths, threads):
-    """One bounded sample of the CPU path; returns (seconds, path_steps)."""
+    """One bounded sample of the CPU path; returns (seconds, path_steps).  The
+    reference is timed from C++ (std::chrono around its batch call); the
+    oracle port, used only where the reference could not be built, from
+    Python around its C call."""
     from oracle import oracle as orc
 
     b = _cpu_sample_batch(n_opt, paths)
+    if impl == "reference" and CPU_TIMER.exists():
+        return _time_cpu_cxx(b), int(n_opt) * int(paths) * STEPS
     t0 = time.perf_counter()
     if impl == "reference":
         orc.Reference().heston_batch(**b)
@@ -207,6 +243,12 @@ def cpu_kind():
     return "reference" if orc.reference_available() else "port"
 
 
+def cpu_timer_name():
+    return ("C++ std::chrono::steady_clock around the batch call (oracle/cpu_timer.cpp)"
+            if cpu_kind() == "reference" and CPU_TIMER.exists() else
+            "Python time.perf_counter around the batch call")
+
+
 def cpu_model():
     """The host CPU's model name (/proc/cpuinfo), for the baseline record."""
     try:
@@ -247,7 +289,7 @@ def reference_arm(args):
         "config": {"workload": WORKLOAD, "options": N_OPT, "paths": PATHS, "steps": STEPS,
                    "cpu_sample": sample},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
-                         "cpu_model": cpu_model(), "sample": sample},
+                         "cpu_model": cpu_model(), "timer": cpu_timer_name(), "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "prices_per_sec": value / (PATHS * STEPS),
     }
@@ -448,7 +490,7 @@ def main_gpu(args):
         cs = cres["samples"][0]
         cpu_value = cs["path_steps"] / cs["seconds"]
         cpu = {"value": cpu_value, "unit": UNIT, "cores": threads, "kind": cpu_kind(),
-               "cpu_model": cpu_model(),
+               "cpu_model": cpu_model(), "timer": cpu_timer_name(),
                "sample": f"64 options x {cres['paths']} paths x {STEPS} steps of the workload"}
         c1 = run_cpu(cpu_kind(), 1, seconds=4.0)["samples"][0]
         cpu["value_1_core"] = c1["path_steps"] / c1["seconds"]

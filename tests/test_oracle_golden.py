@@ -265,3 +265,38 @@ def test_philox_replay_estimator_is_statistically_the_reference(oracle):
         b, sb = oracle.price(model, paths=20000, steps=steps, seed=11, **base)
         z = (a - b) / math.hypot(sa, sb)
         assert abs(z) < 4.0, (model, a, b, z)
+
+
+def test_cpu_timer_calls_the_reference_batch(ref, tmp_path):
+    """The C++ timing harness behind the benchmark's CPU baseline calls the
+    reference's Heston batch entry point with the benchmark's inputs: its
+    prices sum to the Python binding's, bit for bit."""
+    import subprocess
+
+    from oracle import oracle as orc
+
+    timer = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "cpu_timer"
+    if not timer.exists():
+        pytest.skip("cpu_timer not built")
+    rng = np.random.default_rng(3)
+    n = 6
+    b = dict(spot=np.full(n, 100.0), strike=rng.uniform(80, 120, n), t=rng.uniform(0.2, 2, n),
+             r=rng.uniform(0, 0.05, n), q=np.zeros(n), v0=rng.uniform(0.01, 0.09, n),
+             kappa=rng.uniform(0.5, 5, n), theta=rng.uniform(0.01, 0.09, n),
+             sigma=rng.uniform(0.1, 1, n), rho=rng.uniform(-0.9, 0, n),
+             option_type=(np.arange(n) % 2).astype(np.int32), paths=np.full(n, 500, np.int32),
+             steps=np.full(n, 20, np.int32), seed=np.arange(n, dtype=np.uint64) + 7)
+    f = tmp_path / "in.bin"
+    with open(f, "wb") as fh:
+        fh.write(np.int32(n).tobytes())
+        for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho"):
+            fh.write(b[k].astype(np.float64).tobytes())
+        for k in ("option_type", "paths", "steps"):
+            fh.write(b[k].astype(np.int32).tobytes())
+        fh.write(b["seed"].astype(np.uint64).tobytes())
+    r = subprocess.run([str(timer), str(orc.REF_SO), "qk_mcm_heston_monte_carlo_price_batch",
+                        str(f), "2"], capture_output=True, text=True, check=True)
+    out = json.loads(r.stdout)
+    assert len(out["seconds"]) == 2 and all(s > 0 for s in out["seconds"])
+    want = float(np.sum(ref.heston_batch(**b)))
+    assert out["price_sum"] == want
