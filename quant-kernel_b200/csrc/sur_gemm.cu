@@ -637,7 +637,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 }
                 if (l < 2) {
                     const float* bias = l == 0 ? sb1 : sb2;
-#pragma unroll 1
+#pragma unroll
                     for (int kb = 0; kb < 4; ++kb) {
                         const int col0 = kb * 64 + g * 16;
                         uint32_t u[16];
@@ -660,7 +660,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 } else {
                     // head: this warp's chain over columns 64 kb + 16 g + j
                     float p = 0.0f;
-#pragma unroll 1
+#pragma unroll
                     for (int kb = 0; kb < 4; ++kb) {
                         const int col0 = kb * 64 + g * 16;
                         uint32_t u[16];
