@@ -486,6 +486,8 @@ def main_gpu(args):
 
     threads = host_threads()
     try:
+        if world > 1:  # measured once, at N = 1; all N GPUs stay held meanwhile
+            raise RuntimeError("measured in the 1-GPU run only")
         cres = run_cpu(cpu_kind(), threads, seconds=10.0)
         cs = cres["samples"][0]
         cpu_value = cs["path_steps"] / cs["seconds"]
@@ -496,10 +498,12 @@ def main_gpu(args):
         cpu["value_1_core"] = c1["path_steps"] / c1["seconds"]
     except Exception as exc:  # the CPU baseline never blocks the GPU line
         cpu = {"value": None, "unit": UNIT, "cores": threads, "kind": cpu_kind(),
-               "sample": f"failed: {exc}"[:200]}
+               "sample": (f"skipped: {exc}" if world > 1 else f"failed: {exc}")[:200]}
 
     extras = {}
     try:
+        if world > 1:  # the secondary 1-GPU workloads run in the N = 1 line only
+            raise RuntimeError("secondary legs run in the 1-GPU run only")
         extras["mixed"] = mixed_leg(qk)
         extras["bsm_terminal"] = bsm_terminal_leg(qk)
         extras["heston_cf"] = heston_cf_leg(qk)
@@ -508,7 +512,10 @@ def main_gpu(args):
             extras["surrogate"] = surrogate_infer_leg(qk, args.sur_checkpoint,
                                                       mc_prices_per_s=value / (PATHS * STEPS))
     except Exception as exc:  # secondary workloads never block the headline line
-        extras["secondary_error"] = f"{type(exc).__name__}: {exc}"[:300]
+        if world > 1:
+            extras["secondary"] = f"skipped: {exc}"
+        else:
+            extras["secondary_error"] = f"{type(exc).__name__}: {exc}"[:300]
 
     h2d = n_opt * 128 + (n_opt + 1) * 8  # packed option records + tile offsets
     line = {
