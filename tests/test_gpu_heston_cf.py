@@ -129,3 +129,38 @@ def test_large_batch_deterministic(qk):
     a = qk.heston_price_cf_batch(*(cols[k] for k in KEYS))
     b = qk.heston_price_cf_batch(*(cols[k] for k in KEYS))
     assert np.array_equal(a, b) and np.all(np.isfinite(a))
+
+
+def test_batch_speed_regression(qk):
+    """Port of the reference's Heston batch speed guard
+    (test_perf_regression.py:135-175: batch < 1.10 x a scalar loop on 1000
+    options at 512 steps, limit 80).  On the GPU one batch launch replaces a
+    thousand synchronous calls, so the bar here is 10x, not 1.1x."""
+    import statistics
+    import time
+
+    rng = np.random.default_rng(17)
+    n = 1000
+    a = dict(spot=rng.uniform(90.0, 110.0, n), strike=rng.uniform(90.0, 110.0, n),
+             t=rng.uniform(0.25, 1.0, n), r=rng.uniform(0.01, 0.05, n), q=rng.uniform(0.0, 0.02, n),
+             v0=rng.uniform(0.02, 0.08, n), kappa=rng.uniform(1.0, 3.0, n),
+             theta=rng.uniform(0.02, 0.08, n), sigma=rng.uniform(0.2, 0.5, n),
+             rho=rng.uniform(-0.8, -0.3, n),
+             option_type=np.where(np.arange(n) % 2 == 0, 0, 1).astype(np.int32),
+             integration_steps=np.full(n, 512, np.int32), integration_limit=np.full(n, 80.0))
+    keys = list(a)
+    qk.heston_price_cf_batch(*(a[k][:10] for k in keys))
+
+    def median_ms(fn, repeats=3):
+        samples = []
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            fn()
+            samples.append((time.perf_counter() - t0) * 1e3)
+        return statistics.median(samples)
+
+    scalar_ms = median_ms(lambda: [qk.heston_price_cf(*(a[k][i].item() for k in keys))
+                                   for i in range(n)])
+    batch_ms = median_ms(lambda: qk.heston_price_cf_batch(*(a[k] for k in keys)))
+    print(f"\nHeston CF, 1000 options: batch {batch_ms:.2f} ms, scalar loop {scalar_ms:.1f} ms")
+    assert batch_ms * 10 < scalar_ms
