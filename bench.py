@@ -142,19 +142,36 @@ def _time_cpu(impl, n_opt, paths, threads):
     return dt, int(n_opt) * int(paths) * STEPS
 
 
+def _cos_batch(n=65536):
+    """The CF workload's options for the COS pricer at the reference's
+    defaults (256 terms, truncation width 10)."""
+    from quantkernel_b200 import workloads
+
+    b = workloads.heston_cf(n)
+    out = {k: b[k] for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma",
+                             "rho", "option_type")}
+    out["n_terms"] = np.full(n, 256, np.int32)
+    out["truncation_width"] = np.full(n, 10.0)
+    return out
+
+
 def _cf_cpu_leg(s):
-    """Reference (or oracle) Heston CF batch on a bounded sample of the CF workload."""
+    """Reference (or oracle) Heston CF or COS batch on a bounded sample of the
+    Fourier workload."""
     from oracle import oracle as orc
     from quantkernel_b200 import workloads
 
-    b = workloads.heston_cf()
+    cos = s.get("method") == "cos"
+    b = _cos_batch() if cos else workloads.heston_cf()
     cap = len(b["spot"])
-    fn = (orc.Reference() if s["impl"] == "reference" else orc.Oracle()).heston_cf
+    port = orc.Oracle()
+    fn = port.heston_cos if cos else port.heston_cf
     n = 16
     while True:
         t0 = time.perf_counter()
         if s["impl"] == "reference":
-            orc.Reference().heston_cf_batch(**{k: v[:n] for k, v in b.items()})
+            ref = orc.Reference()
+            (ref.heston_cos_batch if cos else ref.heston_cf_batch)(**{k: v[:n] for k, v in b.items()})
         else:
             for i in range(n):
                 fn(*(b[k][i].item() for k in b))
@@ -226,10 +243,10 @@ def cpu_leg(spec):
     print(json.dumps({"samples": out, "n_opt": 64, "paths": paths}))
 
 
-def run_cpu(impl, threads, seconds, reps=1, kind="heston_mc"):
+def run_cpu(impl, threads, seconds, reps=1, kind="heston_mc", **extra):
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     spec = json.dumps({"impl": impl, "threads": threads, "seconds": seconds, "reps": reps,
-                       "kind": kind})
+                       "kind": kind, **extra})
     r = subprocess.run([sys.executable, str(Path(__file__).resolve()), "--cpu-leg", spec],
                        env=env, capture_output=True, text=True, timeout=1800)
     if r.returncode != 0:
@@ -921,6 +938,27 @@ def heston_cf_leg(qk, reps=5, n=65536, cpu=True):
                                "sample": f"first {c['options']} options of the workload"}
     except Exception as exc:
         res["cpu_baseline"] = {"value": None, "sample": f"failed: {exc}"[:200]}
+    # the COS pricer on the same options at the reference's defaults
+    cb = _cos_batch(n)
+    for _ in range(2):
+        qk.cos_method_fang_oosterlee_heston_price_batch(**cb)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        out = qk.cos_method_fang_oosterlee_heston_price_batch(**cb)
+    e2e = (time.perf_counter() - t0) / reps
+    assert np.all(np.isfinite(out))
+    cos = {"workload": f"{n} Heston calls/puts, COS with 256 terms, width 10",
+           "e2e_ms": 1e3 * e2e, "e2e_options_per_s": n / e2e,
+           "h2d_bytes": n * 128, "d2h_bytes": n * 8}
+    try:
+        threads = host_threads()
+        c = run_cpu(cpu_kind(), threads, seconds=5.0, kind="heston_cf", method="cos")
+        cos["cpu_baseline"] = {"value": c["options"] / c["seconds"], "unit": "options/s",
+                               "cores": threads, "kind": cpu_kind(),
+                               "sample": f"first {c['options']} options of the workload"}
+    except Exception as exc:
+        cos["cpu_baseline"] = {"value": None, "sample": f"failed: {exc}"[:200]}
+    res["cos"] = cos
     return res
 
 

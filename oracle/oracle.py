@@ -225,6 +225,7 @@ class Reference:
             "qk_cf_heston_price_cf": (D, [D] * 10 + [I32, I32, D]),
             "qk_cf_heston_price_cf_batch": (I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
             "qk_ftm_cos_fang_oosterlee_heston_price": (D, [D] * 10 + [I32, I32, D]),
+            "qk_ftm_cos_fang_oosterlee_heston_price_batch": (I32, [PD] * 10 + [PI32, PI32, PD, I32, PD]),
             "qk_mcm_control_variates_price": (D, term),
             "qk_mcm_stratified_sampling_price": (D, term),
             "qk_mcm_importance_sampling_price": (D, [D] * 6 + [I32, I32, D, U64]),
@@ -340,6 +341,22 @@ class Reference:
         out = np.empty(n)
         rc = self.lib.qk_cf_heston_price_cf_batch(
             *[_pd(x) for x in a], ot.ctypes.data_as(PI32), st.ctypes.data_as(PI32), _pd(lim), n,
+            _pd(out))
+        if rc != 0:
+            raise RuntimeError(f"reference batch rc={rc}")
+        return out
+
+    def heston_cos_batch(self, spot, strike, t, r, q, v0, kappa, theta, sigma, rho, option_type,
+                         n_terms, truncation_width):
+        """qk_ftm_cos_fang_oosterlee_heston_price_batch."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (spot, strike, t, r, q, v0, kappa, theta, sigma, rho)]
+        ot = np.ascontiguousarray(option_type, np.int32)
+        nt = np.ascontiguousarray(n_terms, np.int32)
+        w = np.ascontiguousarray(truncation_width, np.float64)
+        n = a[0].shape[0]
+        out = np.empty(n)
+        rc = self.lib.qk_ftm_cos_fang_oosterlee_heston_price_batch(
+            *[_pd(x) for x in a], ot.ctypes.data_as(PI32), nt.ctypes.data_as(PI32), _pd(w), n,
             _pd(out))
         if rc != 0:
             raise RuntimeError(f"reference batch rc={rc}")
