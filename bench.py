@@ -913,51 +913,42 @@ def vr_leg(qk, reps=5, cpu=True):
 def heston_cf_leg(qk, reps=5, n=65536, cpu=True):
     """65536 Heston calls/puts by the characteristic-function pricer (1024
     Gauss-Legendre nodes on [1e-8, 120], 2048 FP64 characteristic-function
-    evaluations per option) through qk_cf_heston_price_cf_batch with host
-    buffers; beside it the reference's OpenMP CPU batch on a bounded sample."""
+    evaluations per option) through qk_cf_heston_price_cf_batch, and by the
+    COS pricer (256 terms, width 10) through
+    qk_ftm_cos_fang_oosterlee_heston_price_batch, with host buffers; beside
+    each the reference's OpenMP CPU batch on a bounded sample."""
     from quantkernel_b200 import workloads
 
-    b = workloads.heston_cf(n)
-    for _ in range(2):
-        qk.heston_price_cf_batch(**b)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        out = qk.heston_price_cf_batch(**b)
-    e2e = (time.perf_counter() - t0) / reps
-    assert np.all(np.isfinite(out))
+    def e2e_time(fn, batch):
+        for _ in range(2):
+            fn(**batch)
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            out = fn(**batch)
+        dt = (time.perf_counter() - t0) / reps
+        assert np.all(np.isfinite(out))
+        return dt
+
+    def cpu_rate(**extra):
+        try:
+            threads = host_threads()
+            c = run_cpu(cpu_kind(), threads, seconds=5.0, kind="heston_cf", **extra)
+            return {"value": c["options"] / c["seconds"], "unit": "options/s", "cores": threads,
+                    "kind": cpu_kind(), "sample": f"first {c['options']} options of the workload"}
+        except Exception as exc:
+            return {"value": None, "sample": f"failed: {exc}"[:200]}
+
+    e2e = e2e_time(qk.heston_price_cf_batch, workloads.heston_cf(n))
     res = {"workload": f"{n} Heston calls/puts, CF with 1024 steps, limit 120",
            "e2e_ms": 1e3 * e2e, "e2e_options_per_s": n / e2e,
            "h2d_bytes": n * 112, "d2h_bytes": n * 8}
-    if not cpu:
-        return res
-    try:
-        threads = host_threads()
-        c = run_cpu(cpu_kind(), threads, seconds=5.0, kind="heston_cf")
-        res["cpu_baseline"] = {"value": c["options"] / c["seconds"], "unit": "options/s",
-                               "cores": threads, "kind": cpu_kind(),
-                               "sample": f"first {c['options']} options of the workload"}
-    except Exception as exc:
-        res["cpu_baseline"] = {"value": None, "sample": f"failed: {exc}"[:200]}
-    # the COS pricer on the same options at the reference's defaults
-    cb = _cos_batch(n)
-    for _ in range(2):
-        qk.cos_method_fang_oosterlee_heston_price_batch(**cb)
-    t0 = time.perf_counter()
-    for _ in range(reps):
-        out = qk.cos_method_fang_oosterlee_heston_price_batch(**cb)
-    e2e = (time.perf_counter() - t0) / reps
-    assert np.all(np.isfinite(out))
+    e2e = e2e_time(qk.cos_method_fang_oosterlee_heston_price_batch, _cos_batch(n))
     cos = {"workload": f"{n} Heston calls/puts, COS with 256 terms, width 10",
            "e2e_ms": 1e3 * e2e, "e2e_options_per_s": n / e2e,
            "h2d_bytes": n * 128, "d2h_bytes": n * 8}
-    try:
-        threads = host_threads()
-        c = run_cpu(cpu_kind(), threads, seconds=5.0, kind="heston_cf", method="cos")
-        cos["cpu_baseline"] = {"value": c["options"] / c["seconds"], "unit": "options/s",
-                               "cores": threads, "kind": cpu_kind(),
-                               "sample": f"first {c['options']} options of the workload"}
-    except Exception as exc:
-        cos["cpu_baseline"] = {"value": None, "sample": f"failed: {exc}"[:200]}
+    if cpu:
+        res["cpu_baseline"] = cpu_rate()
+        cos["cpu_baseline"] = cpu_rate(method="cos")
     res["cos"] = cos
     return res
 
