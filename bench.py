@@ -941,7 +941,7 @@ def heston_cf_leg(qk, reps=5, n=65536, cpu=True):
     e2e = e2e_time(qk.heston_price_cf_batch, workloads.heston_cf(n))
     res = {"workload": f"{n} Heston calls/puts, CF with 1024 steps, limit 120",
            "e2e_ms": 1e3 * e2e, "e2e_options_per_s": n / e2e,
-           "h2d_bytes": n * 112, "d2h_bytes": n * 8}
+           "h2d_bytes": n * 128, "d2h_bytes": n * 8}
     e2e = e2e_time(qk.cos_method_fang_oosterlee_heston_price_batch, _cos_batch(n))
     cos = {"workload": f"{n} Heston calls/puts, COS with 256 terms, width 10",
            "e2e_ms": 1e3 * e2e, "e2e_options_per_s": n / e2e,
