@@ -736,8 +736,8 @@ cudaError_t Plan::sync_stats() {
     return e;
 }
 
-// Times every candidate launch shape on this plan (one warm-up and one timed
-// run each) and keeps the fastest.  Tile geometry follows the shape, so the
+// Times every candidate launch shape on this plan (one warm-up and the best
+// of three timed runs each) and keeps the fastest.  Tile geometry follows the shape, so the
 // plan is re-laid-out per candidate; per-path results do not change.
 cudaError_t Plan::autotune() {
     std::vector<LaunchConfig> cands;
@@ -761,12 +761,15 @@ cudaError_t Plan::autotune() {
     cudaError_t e;
     for (const LaunchConfig& c : cands) {
         if ((e = layout_tiles(c)) != cudaSuccess) return e;
-        for (int rep = 0; rep < 2; ++rep) {
+        if ((e = launch_all(stream_, false)) != cudaSuccess) return e;  // warm-up
+        float ms = std::numeric_limits<float>::max();
+        for (int rep = 0; rep < 3; ++rep) {  // best of three: shapes differ by ~1%
             if ((e = launch_all(stream_, true)) != cudaSuccess) return e;
+            if ((e = cudaEventSynchronize(ev1_)) != cudaSuccess) return e;
+            float t = 0.0f;
+            if ((e = cudaEventElapsedTime(&t, ev0_, ev1_)) != cudaSuccess) return e;
+            ms = std::min(ms, t);
         }
-        if ((e = cudaEventSynchronize(ev1_)) != cudaSuccess) return e;
-        float ms = 0.0f;
-        if ((e = cudaEventElapsedTime(&ms, ev0_, ev1_)) != cudaSuccess) return e;
         if (ms < best_ms) {
             best_ms = ms;
             best = c;
