@@ -393,8 +393,9 @@ def main_gpu(args):
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
     # the autotuner picks block size, paths per thread and step unrolling by
-    # timing each candidate once (before the timed region); --profile keeps
-    # the default shape so that an ncu capture sees the launch it names
+    # timing each candidate (best of three, before the timed region);
+    # --profile keeps the default shape so that an ncu capture sees the
+    # launch it names
     plan = qk.plan(model=np.full(n_opt, QK_MC_HESTON, np.int32),
                    flags=QK_PLAN_TIMING | (0 if args.profile else QK_PLAN_AUTOTUNE), **h)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
