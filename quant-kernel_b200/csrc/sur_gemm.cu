@@ -124,6 +124,16 @@ __device__ __forceinline__ float tanh_approx(float x) {
 }
 __device__ __forceinline__ float sigmoidf_(float z) { return fmaf(0.5f, tanh_approx(0.5f * z), 0.5f); }
 
+// SiLU straight from the accumulator: hz = z / 2 = fma(acc, 1/2, bias / 2) is
+// exact (halving commutes with the rounding of acc + bias), so tanh(hz) is the
+// sigmoid's tanh(z / 2), and silu(z) = z sigma(z) = hz + hz tanh(hz): two FMAs
+// around one MUFU op.  Returns silu; hz and t = tanh(hz) for the caller.
+__device__ __forceinline__ float silu_from_acc(float acc, float half_bias, float& hz, float& t) {
+    hz = fmaf(acc, 0.5f, half_bias);
+    t = tanh_approx(hz);
+    return fmaf(hz, t, hz);
+}
+
 // 32 bf16 values to 64 contiguous bytes.
 __device__ __forceinline__ void store_bf16x32(__nv_bfloat16* dst, const float (&v)[32]) {
     uint4* d = reinterpret_cast<uint4*>(dst);
@@ -185,8 +195,9 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
             float z[32];
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                z[j] = v[j] + __ldg(a.bias + col0 + j);
-                v[j] = z[j] * sigmoidf_(z[j]);
+                float hz, t;
+                v[j] = silu_from_acc(v[j], 0.5f * __ldg(a.bias + col0 + j), hz, t);
+                z[j] = 2.0f * hz;  // exact: the pre-activation acc + bias
             }
             if (live) {
                 if (a.z_out) store_bf16x32(a.z_out + static_cast<size_t>(row) * a.N + col0, z);
@@ -229,13 +240,15 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
             tmem_ld32(tbase + col0, v);
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
-                const float z = v[j] + __ldg(a.bias + col0 + j);
-                p0 = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), p0);
+                float hz, t;
+                const float h = silu_from_acc(v[j], 0.5f * __ldg(a.bias + col0 + j), hz, t);
+                p0 = fmaf(h, __ldg(a.w4 + col0 + j), p0);
             }
 #pragma unroll
             for (int j = 16; j < 32; ++j) {
-                const float z = v[j] + __ldg(a.bias + col0 + j);
-                p1 = fmaf(z * sigmoidf_(z), __ldg(a.w4 + col0 + j), p1);
+                float hz, t;
+                const float h = silu_from_acc(v[j], 0.5f * __ldg(a.bias + col0 + j), hz, t);
+                p1 = fmaf(h, __ldg(a.w4 + col0 + j), p1);
             }
         }
         part_s[2 * half][q * 32 + lane] = p0;
@@ -255,9 +268,9 @@ __device__ __forceinline__ void epilogue(const GemmArgs& a, uint32_t tmem, int m
                 float h[32];
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const float z = v[j] + __ldg(a.bias + col0 + j);
-                    const float s = sigmoidf_(z);
-                    h[j] = z * s;
+                    float hz, t;
+                    h[j] = silu_from_acc(v[j], 0.5f * __ldg(a.bias + col0 + j), hz, t);
+                    const float z = 2.0f * hz, s = fmaf(0.5f, t, 0.5f);
                     v[j] = dy * __ldg(a.w4 + col0 + j) * s * (1.0f + z * (1.0f - s));
                 }
                 if (live) {
@@ -485,9 +498,9 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     const int64_t n_tiles = (a.n + kBM - 1) / kBM;
 
     if (tid < kSurHidden) {
-        sb1[tid] = a.b1[tid];
-        sb2[tid] = a.b2[tid];
-        sb3[tid] = a.b3[tid];
+        sb1[tid] = 0.5f * a.b1[tid];  // halved biases for silu_from_acc (exact)
+        sb2[tid] = 0.5f * a.b2[tid];
+        sb3[tid] = 0.5f * a.b3[tid];
         sw4[tid] = a.w4[tid];
     }
     if (tid == 0) {
@@ -646,8 +659,8 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                         float v[16];
 #pragma unroll
                         for (int j = 0; j < 16; ++j) {
-                            const float z = __uint_as_float(u[j]) + bias[col0 + j];
-                            v[j] = z * sigmoidf_(z);
+                            float hz, t;
+                            v[j] = silu_from_acc(__uint_as_float(u[j]), bias[col0 + j], hz, t);
                         }
                         store_h16_sw128(hbuf, r, col0, v);
                         // the shared stores to the tensor core's (async) proxy,
@@ -668,8 +681,9 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                         tmem_wait_ld();
 #pragma unroll
                         for (int j = 0; j < 16; ++j) {
-                            const float z = __uint_as_float(u[j]) + sb3[col0 + j];
-                            p = fmaf(z * sigmoidf_(z), sw4[col0 + j], p);
+                            float hz, t;
+                            const float h = silu_from_acc(__uint_as_float(u[j]), sb3[col0 + j], hz, t);
+                            p = fmaf(h, sw4[col0 + j], p);
                         }
                     }
                     part[g][r] = p;
