@@ -79,3 +79,22 @@ def test_accelerator_native_batch_map_covers_all_scalar_methods():
     assert not missing, f"scalar methods the accelerator does not route: {missing}"
     for scalar, batch in native.items():
         assert batch == scalar + "_batch" and hasattr(QuantKernel, batch), (scalar, batch)
+
+
+def test_python_constants_match_the_header():
+    """Every #define of include/qk_abi.h and include/qk_api.h that the Python
+    package mirrors (ABI version, option types, error codes, model codes,
+    plan flags) has the header's value."""
+    import quantkernel_b200._abi as abi
+
+    text = (ROOT / "include" / "qk_abi.h").read_text() + HEADER.read_text()
+    defines = dict(re.findall(r"#define\s+(QK_[A-Z0-9_]+)\s+\(?(-?(?:0x)?[0-9A-Fa-f]+)\)?", text))
+    checked = 0
+    for name, value in defines.items():
+        if hasattr(abi, name):
+            assert getattr(abi, name) == int(value, 0), name
+            checked += 1
+    assert checked >= 25, checked
+    for flag in ("QK_PLAN_PERSISTENT", "QK_PLAN_GRAPH", "QK_PLAN_NO_ANTITHETIC", "QK_PLAN_TIMING",
+                 "QK_PLAN_AUTOTUNE", "QK_PLAN_FAMILY_GRIDS", "QK_PLAN_STEP_UNROLL2"):
+        assert hasattr(abi, flag) and flag in defines, flag
