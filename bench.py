@@ -501,6 +501,12 @@ def main_gpu(args):
                         "xu_pipe_busy"):
                 if line.startswith(key + ":"):
                     roofline["measured"][key] = float(line.split(":")[1])
+    m = roofline["measured"]
+    if "thread_instructions_per_path_step" in m and "xu_per_path_step" in m:
+        # the same bound with this kernel's own (ncu-measured) instruction mix
+        own = min(issue_peak / m["thread_instructions_per_path_step"],
+                  xu_peak / m["xu_per_path_step"])
+        m["frac_of_own_mix_bound"] = achieved / own
 
     threads = host_threads()
     try:
