@@ -79,30 +79,26 @@ __device__ __forceinline__ U4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c
 }
 
 // Uniforms without an integer-to-float conversion: OR-ing k <= 23 bits b into
-// the mantissa of 1.0f gives y = 1 + b 2^-k exactly in [1, 2), and the affine
-// maps below are exact (Sterbenz, or a result with few enough fraction bits),
-// so they equal (b + 1/2) 2^-23 and (b + 1/2) 2^-(k-1) - 1 bit for bit while
-// staying off the conversion pipe.
+// the mantissa of 1.0f gives y = 1 + b 2^-k exactly in [1, 2), and y minus
+// (1 - 2^-24) is exact (Sterbenz), so it equals (b + 1/2) 2^-23 bit for bit
+// while staying off the conversion pipe.
 __device__ __forceinline__ float unit_from_bits(uint32_t b23) {  // (b + 1/2) 2^-23
     return __uint_as_float(0x3F800000u | b23) - 0x1.fffffep-1f;   // y - (1 - 2^-24)
-}
-template <int K>  // K-bit b, K <= 22:  (b + 1/2) 2^-(K-1) - 1 = 2y - (3 - 2^-K)
-__device__ __forceinline__ float sym_from_bits(uint32_t b) {
-    const float y = __uint_as_float(0x3F800000u | (b << (23 - K)));
-    return fma_rn(y, 2.0f, -(3.0f - 1.0f / (float)(1u << K)));
 }
 
 // Box-Muller on two 32-bit words (the layout the FP64 replay in the oracle
 // mirrors):  u = ((xa >> 9) + 1/2) 2^-23 in (0,1), g = ((xb >> 9) + 1/2) 2^-22 - 1
 // in (-1,1);  za = sqrt(-2 ln u) cos(pi g),  zb = sqrt(-2 ln u) sin(pi g).
 // ln u = log2(u) * ln 2, and sqrt(w) = sqrt.approx(w).  For the 23-bit angle,
-// y = 2 + b 2^-22 (exponent of 2.0f) and g = (y - 3) + 2^-23, both exact.
+// y = 2 + b 2^-22 (exponent of 2.0f) and pi g = pi y - pi (3 - 2^-23): one FMA.
 __device__ __forceinline__ void box_muller(uint32_t xa, uint32_t xb, float& za, float& zb) {
+    constexpr float kPi = 3.14159265358979323846f;
+    constexpr float kOff = (float)(3.14159265358979323846 * (3.0 - 0x1p-23));
     const float u = unit_from_bits(xa >> 9);
-    const float g = (__uint_as_float(0x40000000u | (xb >> 9)) - 3.0f) + 0x1p-23f;
+    const float y = __uint_as_float(0x40000000u | (xb >> 9));
     const float w = -1.38629436111989061883f * ptx_lg2(u);  // -2 ln u
     const float rad = ptx_sqrt(w);
-    const float ang = 3.14159265358979323846f * g;
+    const float ang = fma_rn(y, kPi, -kOff);
     za = rad * ptx_cos(ang);
     zb = rad * ptx_sin(ang);
 }
@@ -114,24 +110,50 @@ __device__ __forceinline__ void normals4(uint32_t unit, uint32_t block, uint32_t
     box_muller(x.z, x.w, z[2], z[3]);
 }
 
-// Box-Muller from a 23-bit radius word and a K-bit angle word:
-//   u = (ub + 1/2) 2^-23,  g = (gb + 1/2) 2^-(K-1) - 1.
+// sqrt(2 ln 2): sqrt(-2 ln u) = kBmRadius * sqrt(-log2 u).
+constexpr float kBmRadius = 1.17741002251547469101f;
+constexpr double kBmRadiusD = 1.17741002251547469101;
+constexpr float kBmRadius2 = 1.38629436111989061883f;  // kBmRadius^2 = 2 ln 2
+
+// Box-Muller from a 23-bit radius word and a K-bit angle word, in parts:
+//   u = (ub + 1/2) 2^-23,  g = (gb + 1/2) 2^-(K-1) - 1,
+//   w = -log2 u,  c = cos(pi g),  s = sin(pi g),
+// so that the normals are kBmRadius sqrt(w) c and kBmRadius sqrt(w) s.  With
+// y = 1 + gb 2^-K (gb OR-ed into the mantissa of 1.0f), pi g =
+// 2 pi y - pi (3 - 2^-K): one FMA from y to the angle.
+template <int K>
+__device__ __forceinline__ void box_muller_parts(uint32_t ub, uint32_t gb, float& w, float& c,
+                                                 float& s) {
+    constexpr float kTwoPi = 6.28318530717958647692f;
+    constexpr float kOff = (float)(3.14159265358979323846 * (3.0 - 1.0 / (double)(1u << K)));
+    const float u = unit_from_bits(ub);
+    const float y = __uint_as_float(0x3F800000u | (gb << (23 - K)));
+    w = -ptx_lg2(u);
+    const float ang = fma_rn(y, kTwoPi, -kOff);
+    c = ptx_cos(ang);
+    s = ptx_sin(ang);
+}
+
+// The normals of box_muller_parts divided by kBmRadius (the callers fold that
+// factor into their step constants, which saves a multiply per pair):
+//   za = sqrt(w) c,  zb = sqrt(w) s.
 template <int K>
 __device__ __forceinline__ void box_muller_bits(uint32_t ub, uint32_t gb, float& za, float& zb) {
-    const float u = unit_from_bits(ub);
-    const float g = sym_from_bits<K>(gb);
-    const float w = -1.38629436111989061883f * ptx_lg2(u);  // -2 ln u
+    float w, c, s;
+    box_muller_parts<K>(ub, gb, w, c, s);
     const float rad = ptx_sqrt(w);
-    const float ang = 3.14159265358979323846f * g;
-    za = rad * ptx_cos(ang);
-    zb = rad * ptx_sin(ang);
+    za = rad * c;
+    zb = rad * s;
 }
 
 // Six normals from one Philox call: three Box-Muller pairs, each with a
 // 23-bit radius (the top 23 bits of x, y, z) and an angle of 16, 16 and 18
 // bits (the low and high halves of w; the low 9 bits of x and of y).  Every
 // output bit of the call is used once.  pair(p) computes pair p on demand, so
-// only the four words stay live across the three steps they feed.
+// only the four words stay live across the three steps they feed.  pair()
+// gives the normals divided by kBmRadius (box_muller_bits); parts() gives
+// (w, c, s) of box_muller_parts, for a caller that folds sqrt(w) into a square
+// root of its own (sqrt(v) sqrt(w) = sqrt(v w)).
 struct Philox6 {
     U4 x;
     __device__ __forceinline__ void pair(int p, float& za, float& zb) const {
@@ -141,6 +163,14 @@ struct Philox6 {
             box_muller_bits<16>(x.y >> 9, x.w >> 16, za, zb);
         else
             box_muller_bits<18>(x.z >> 9, (x.x & 0x1FFu) | ((x.y & 0x1FFu) << 9), za, zb);
+    }
+    __device__ __forceinline__ void parts(int p, float& w, float& c, float& s) const {
+        if (p == 0)
+            box_muller_parts<16>(x.x >> 9, x.w & 0xFFFFu, w, c, s);
+        else if (p == 1)
+            box_muller_parts<16>(x.y >> 9, x.w >> 16, w, c, s);
+        else
+            box_muller_parts<18>(x.z >> 9, (x.x & 0x1FFu) | ((x.y & 0x1FFu) << 9), w, c, s);
     }
 };
 

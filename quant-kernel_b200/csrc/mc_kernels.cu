@@ -151,7 +151,9 @@ __device__ __forceinline__ void sim_terminal(const McOption& o, uint32_t unit0, 
 template <int UPT, bool ANTI, bool MIL, int SU>
 __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, uint32_t stride,
                                              uint32_t k0, uint32_t k1, Acc& acc) {
-    const float m0 = o.p[0], b = o.p[1], fl = o.p[2], c = o.p[3];
+    // Philox6 normals are z / kBmRadius: the vol and Milstein constants take
+    // the factor (b z = (b kBmRadius)(z / kBmRadius), likewise c z^2)
+    const float m0 = o.p[0], b = o.p[1] * kBmRadius, fl = o.p[2], c = o.p[3] * kBmRadius2;
     const int32_t steps = o.steps;
     const uint32_t units = (uint32_t)o.units;
     const uint32_t c3 = ANTI ? 0u : 1u;
@@ -224,7 +226,9 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 // v >= 0 after every step (and v0 >= 0 is validated), so the reference's
 // v_pos = max(v, 0) is v itself.  One Philox call feeds three steps of a unit
 // (six normals: Philox6); SU step blocks per loop iteration as in
-// sim_stepwise.
+// sim_stepwise.  With Box-Muller z1 = r cos a, z2 = r sin a, r = sqrt(-2 ln u),
+// the step needs sqrt(v) r = sqrt(v r^2) only: one square root per path and
+// step instead of one per path and step plus one per pair.
 // ----------------------------------------------------------------------------
 //
 // LR = true: the likelihood-ratio delta of heston_lr_delta.cpp:37-132.  Each
@@ -234,8 +238,10 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 template <int UPT, bool ANTI, bool LR, int SU>
 __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, uint32_t stride,
                                            uint32_t k0, uint32_t k1, Acc& acc) {
-    const float cmu = o.p[0], hdt = o.p[1], sqdt = o.p[2], kdt = o.p[3], kth = o.p[4];
-    const float xsq = o.p[5], rho = o.p[6], rhoc = o.p[7], v0 = o.p[8], xfl = o.p[9];
+    // the normals enter as kBmRadius sqrt(w) (c, s) (Philox6::parts): the two
+    // constants that multiply them take the factor kBmRadius
+    const float cmu = o.p[0], hdt = o.p[1], sqdt = o.p[2] * kBmRadius, kdt = o.p[3], kth = o.p[4];
+    const float xsq = o.p[5] * kBmRadius, rho = o.p[6], rhoc = o.p[7], v0 = o.p[8], xfl = o.p[9];
     const float omk = 1.0f - kdt;
     const float xr = xsq * rho, xc = xsq * rhoc;
     const int32_t steps = o.steps;
@@ -271,19 +277,22 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
                 if (s < m) {
 #pragma unroll
                     for (int k = 0; k < UPT; ++k) {
-                        float z1, z2;
-                        r[k].pair(s, z1, z2);
-                        if (LR && j == 0 && s == 0) zfirst[k] = z1;
-                        const float sz1 = sqdt * z1;
-                        const float xw = fma_rn(xr, z1, xc * z2);
+                        // z1 = kBmRadius sqrt(w) c, z2 = kBmRadius sqrt(w) s; the
+                        // step needs sqrt(v) z1 and sqrt(v) z2 only, so sqrt(w)
+                        // joins the variance's square root: sqrt(v w)
+                        float w, c1, s1;
+                        r[k].parts(s, w, c1, s1);
+                        if (LR && j == 0 && s == 0) zfirst[k] = ptx_sqrt(w) * c1;
+                        const float sz1 = sqdt * c1;
+                        const float xw = fma_rn(xr, c1, xc * s1);
                         {
-                            const float sv = ptx_sqrt(vu[k]);
+                            const float sv = ptx_sqrt(vu[k] * w);
                             const float inc = fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu));
                             xu[k] = ptx_max_nan(xu[k] + inc, xfl);
                             vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
                         }
                         if (ANTI) {
-                            const float sv = ptx_sqrt(vd[k]);
+                            const float sv = ptx_sqrt(vd[k] * w);
                             const float inc = fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu));
                             xd[k] = ptx_max_nan(xd[k] + inc, xfl);
                             vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
@@ -294,8 +303,9 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         }
     }
     const uint32_t n_pairs = (uint32_t)o.paths >> 1;
-    // score scale 1 / (sqrt(v0) sqrt(dt) S0); v0 = 0 is a constant-zero option
-    const double wscale = LR ? 1.0 / ((double)ptx_sqrt(v0) * (double)sqdt * o.spot) : 0.0;
+    // score scale 1 / (sqrt(v0) sqrt(dt) S0) for z1 = kBmRadius zfirst; v0 = 0
+    // is a constant-zero option
+    const double wscale = LR ? kBmRadiusD / ((double)ptx_sqrt(v0) * (double)o.p[2] * o.spot) : 0.0;
 #pragma unroll
     for (int k = 0; k < UPT; ++k) {
         const uint32_t unit = unit0 + (uint32_t)k * stride;
