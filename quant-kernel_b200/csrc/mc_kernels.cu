@@ -219,7 +219,8 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 }
 
 // ----------------------------------------------------------------------------
-// Heston full-truncation Euler.  State (x, v) with x = log(S/spot):
+// Heston full-truncation Euler.  State (x, v) with x = log(S/spot), kept as
+// y = x - j (r-q)dt after j steps (see xu below):
 //   x' = max_nan(x + (r-q)dt - v dt/2 + sqrt(v) sqrt(dt) z1, log(1e-12/spot))
 //   v' = max(v (1 - kappa dt) + kappa theta dt
 //            + sigma sqrt(dt) sqrt(v) (rho z1 + sqrt(1-rho^2) z2), 0)
@@ -247,7 +248,11 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
     const int32_t steps = o.steps;
     const uint32_t units = (uint32_t)o.units;
     const uint32_t c3 = ANTI ? 0u : 1u;
+    // xu, xd hold y = x - j (r-q)dt after j steps: the drift leaves the per-step
+    // update (one add fewer per path and step) and enters the floor instead,
+    // y_j >= log(1e-12/spot) - j (r-q)dt, the same map as x_j >= log(1e-12/spot)
     float xu[UPT], vu[UPT], xd[UPT], vd[UPT];
+    float fl = xfl;
     float zfirst[UPT];
 #pragma unroll
     for (int k = 0; k < UPT; ++k) {
@@ -275,6 +280,7 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
 #pragma unroll
             for (int s = 0; s < 3; ++s) {
                 if (s < m) {
+                    fl -= cmu;  // the floor of y after this step
 #pragma unroll
                     for (int k = 0; k < UPT; ++k) {
                         // z1 = kBmRadius sqrt(w) c, z2 = kBmRadius sqrt(w) s; the
@@ -287,14 +293,12 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
                         const float xw = fma_rn(xr, c1, xc * s1);
                         {
                             const float sv = ptx_sqrt(vu[k] * w);
-                            const float inc = fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu));
-                            xu[k] = ptx_max_nan(xu[k] + inc, xfl);
+                            xu[k] = ptx_max_nan(fma_rn(sv, sz1, fma_rn(-hdt, vu[k], xu[k])), fl);
                             vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
                         }
                         if (ANTI) {
                             const float sv = ptx_sqrt(vd[k] * w);
-                            const float inc = fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu));
-                            xd[k] = ptx_max_nan(xd[k] + inc, xfl);
+                            xd[k] = ptx_max_nan(fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], xd[k])), fl);
                             vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
                         }
                     }
@@ -303,6 +307,7 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         }
     }
     const uint32_t n_pairs = (uint32_t)o.paths >> 1;
+    const double drift = (double)steps * (double)cmu;  // x = y + steps (r-q)dt
     // score scale 1 / (sqrt(v0) sqrt(dt) S0) for z1 = kBmRadius zfirst; v0 = 0
     // is a constant-zero option
     const double wscale = LR ? kBmRadiusD / ((double)ptx_sqrt(v0) * (double)o.p[2] * o.spot) : 0.0;
@@ -312,10 +317,10 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         if (unit >= units) continue;
         double w = 1.0;
         if (LR) w = fmin(o.weight_clip, fmax(-o.weight_clip, (double)zfirst[k] * wscale));
-        const double pu = payoff(o.spot * exp((double)xu[k]), o.strike, o.option_type) * w;
+        const double pu = payoff(o.spot * exp((double)xu[k] + drift), o.strike, o.option_type) * w;
         if (ANTI) {
             if (unit < n_pairs)
-                acc.add_pair(pu, payoff(o.spot * exp((double)xd[k]), o.strike, o.option_type) * (LR ? -w : 1.0));
+                acc.add_pair(pu, payoff(o.spot * exp((double)xd[k] + drift), o.strike, o.option_type) * (LR ? -w : 1.0));
             else
                 acc.add_lone(pu);
         } else {
