@@ -483,8 +483,9 @@ def main_gpu(args):
         "kernel_ms": sim_ms,
         "measured": {"source": "ncu, profiles/heston_simulate_ncu.md"},
         "note": ("frac > 1: the reference formulas cost 6 XU + 50 ALU per path-step; this "
-                 "kernel needs 3 XU + ~25 (antithetic pairs share normals, log-space spot "
-                 "drops the per-step exp)"),
+                 "kernel needs 2.5 XU + ~23 (antithetic pairs share normals, log-space spot "
+                 "drops the per-step exp, sqrt(v) times the Box-Muller radius is one "
+                 "square root)"),
         "per_unit": {"xu": XU_PER_UNIT, "alu": ALU_PER_UNIT, "unit": "path-step"},
         "peak_source": ("nominal per-clock SM widths (148 SMs x 128 issue / 16 XU per clk) at "
                         "the SM clock sampled during the timed region; the driver's measured "
