@@ -236,9 +236,16 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 // path's payoff is weighted by the score of its first spot step,
 // w = clamp(z1_0 / (sqrt(v0) sqrt(dt) S0), -clip, clip); the antithetic path's
 // score is -w.
-template <int UPT, bool ANTI, bool LR, int SU>
-__device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, uint32_t stride,
-                                           uint32_t k0, uint32_t k1, Acc& acc) {
+//
+// DF (drift in floor) selects the state: y = x - j (r-q)dt (one add fewer per
+// path and step) or x itself.  y is used while |(r-q)dt| steps <= 1: then y
+// stays as small as x, so FP32 rounds it no worse, and the floor
+// log(1e-12/spot) - j (r-q)dt stays exact to FP32 rounding.  Larger or
+// non-finite drifts, which the reference accepts for Heston (no finiteness
+// check on r and q), keep x, whose floor is exact at any drift.
+template <int UPT, bool ANTI, bool LR, int SU, bool DF>
+__device__ __forceinline__ void sim_heston_form(const McOption& o, uint32_t unit0, uint32_t stride,
+                                                uint32_t k0, uint32_t k1, Acc& acc) {
     // the normals enter as kBmRadius sqrt(w) (c, s) (Philox6::parts): the two
     // constants that multiply them take the factor kBmRadius
     const float cmu = o.p[0], hdt = o.p[1], sqdt = o.p[2] * kBmRadius, kdt = o.p[3], kth = o.p[4];
@@ -248,9 +255,9 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
     const int32_t steps = o.steps;
     const uint32_t units = (uint32_t)o.units;
     const uint32_t c3 = ANTI ? 0u : 1u;
-    // xu, xd hold y = x - j (r-q)dt after j steps: the drift leaves the per-step
-    // update (one add fewer per path and step) and enters the floor instead,
-    // y_j >= log(1e-12/spot) - j (r-q)dt, the same map as x_j >= log(1e-12/spot)
+    // DF: xu, xd hold y = x - j (r-q)dt after j steps: the drift leaves the
+    // per-step update and enters the floor instead, y_j >= log(1e-12/spot) -
+    // j (r-q)dt, the same map as x_j >= log(1e-12/spot)
     float xu[UPT], vu[UPT], xd[UPT], vd[UPT];
     float fl = xfl;
     float zfirst[UPT];
@@ -280,7 +287,7 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
 #pragma unroll
             for (int s = 0; s < 3; ++s) {
                 if (s < m) {
-                    fl -= cmu;  // the floor of y after this step
+                    if (DF) fl -= cmu;  // the floor of y after this step
 #pragma unroll
                     for (int k = 0; k < UPT; ++k) {
                         // z1 = kBmRadius sqrt(w) c, z2 = kBmRadius sqrt(w) s; the
@@ -293,12 +300,18 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
                         const float xw = fma_rn(xr, c1, xc * s1);
                         {
                             const float sv = ptx_sqrt(vu[k] * w);
-                            xu[k] = ptx_max_nan(fma_rn(sv, sz1, fma_rn(-hdt, vu[k], xu[k])), fl);
+                            if (DF)
+                                xu[k] = ptx_max_nan(fma_rn(sv, sz1, fma_rn(-hdt, vu[k], xu[k])), fl);
+                            else
+                                xu[k] = ptx_max_nan(xu[k] + fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu)), xfl);
                             vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
                         }
                         if (ANTI) {
                             const float sv = ptx_sqrt(vd[k] * w);
-                            xd[k] = ptx_max_nan(fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], xd[k])), fl);
+                            if (DF)
+                                xd[k] = ptx_max_nan(fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], xd[k])), fl);
+                            else
+                                xd[k] = ptx_max_nan(xd[k] + fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu)), xfl);
                             vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
                         }
                     }
@@ -307,7 +320,7 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
         }
     }
     const uint32_t n_pairs = (uint32_t)o.paths >> 1;
-    const double drift = (double)steps * (double)cmu;  // x = y + steps (r-q)dt
+    const double drift = DF ? (double)steps * (double)cmu : 0.0;  // x = y + steps (r-q)dt
     // score scale 1 / (sqrt(v0) sqrt(dt) S0) for z1 = kBmRadius zfirst; v0 = 0
     // is a constant-zero option
     const double wscale = LR ? kBmRadiusD / ((double)ptx_sqrt(v0) * (double)o.p[2] * o.spot) : 0.0;
@@ -327,6 +340,16 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
             acc.add_plain(pu);
         }
     }
+}
+
+template <int UPT, bool ANTI, bool LR, int SU>
+__device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, uint32_t stride,
+                                           uint32_t k0, uint32_t k1, Acc& acc) {
+    // uniform per option (and so per CTA); a NaN drift takes the x state
+    if (fabsf(o.p[0]) * (float)o.steps <= 1.0f)
+        sim_heston_form<UPT, ANTI, LR, SU, true>(o, unit0, stride, k0, k1, acc);
+    else
+        sim_heston_form<UPT, ANTI, LR, SU, false>(o, unit0, stride, k0, k1, acc);
 }
 
 // ----------------------------------------------------------------------------

@@ -69,3 +69,51 @@ def test_gpu_equals_fp64_replay_of_same_stream(qk, oracle, model, anti):
         else:  # fewer than two samples
             assert not math.isfinite(se[i]), (c, se[i])
     print(f"model {model} anti={anti}: worst |diff|/tol = {worst:.3f}")
+
+
+def test_heston_large_and_non_finite_drift(qk, oracle):
+    """The Heston kernel keeps y = log(S/spot) - j (r-q)dt as its state while
+    |(r-q) t| <= 1 and log(S/spot) itself beyond, where y would outgrow FP32
+    and its moving floor would lose log(1e-12/spot).  The reference accepts
+    any r and q for Heston (heston_monte_carlo.cpp:18-24 checks neither), so
+    both sides of that switch are held to the FP64 replay of the same stream,
+    and drifts that pin every path to the 1e-12 floor, or send it to +inf, to
+    the values the reference's step gives them."""
+    base = dict(spot=100.0, strike=95.0, t=1.5, vol=0.0, v0=0.04, kappa=1.5, theta=0.05,
+                sigma=0.6, rho=-0.6, paths=20001, steps=40, seed=77)
+    keys = ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho",
+            "option_type", "paths", "steps", "seed")
+
+    def run(cases):
+        cols = {k: np.array([c[k] for c in cases]) for k in keys}
+        for k in ("option_type", "paths", "steps"):
+            cols[k] = cols[k].astype(np.int32)
+        cols["seed"] = cols["seed"].astype(np.uint64)
+        return qk.heston_monte_carlo_price_se_batch(**cols)
+
+    # |(r-q) t| = 0.9 (y state) and 1.05, 1.35, 2.25 (log-spot state)
+    cases = [dict(base, r=r, q=q, option_type=ot)
+             for r, q in ((0.6, 0.0), (0.7, 0.0), (0.0, 0.9), (2.0, 0.5)) for ot in (0, 1)]
+    price, se = run(cases)
+    for i, c in enumerate(cases):
+        want, want_se = oracle.philox_price(6, antithetic=True, **c)
+        tol = 5e-5 * c["spot"] + 0.02 * want_se
+        assert abs(price[i] - want) <= tol, (c, price[i], want)
+        assert abs(se[i] - want_se) <= 0.02 * want_se + 1e-12, (c, se[i], want_se)
+
+    # every step's exp(-inf) (or exp of -1e4 (r-q) dt) sends S to the 1e-12 floor
+    inf = math.inf
+    floor_put = 95.0 - 1e-12
+    cases = [dict(base, r=0.03, q=q, option_type=ot) for q in (inf, 1e4) for ot in (0, 1)]
+    cases += [dict(base, r=-inf, q=0.0, option_type=ot) for ot in (0, 1)]
+    cases += [dict(base, r=inf, q=0.0, option_type=ot) for ot in (0, 1)]
+    price, se = run(cases)
+    disc = math.exp(-0.03 * 1.5)
+    for i in range(4):
+        want = 0.0 if cases[i]["option_type"] == 0 else disc * floor_put
+        assert abs(price[i] - want) <= 1e-12 * max(1.0, want), (cases[i], price[i], want)
+        assert 0.0 <= se[i] <= 1e-9 * max(1.0, want), (cases[i], se[i])
+    # r = -inf: exp(-r t) = inf times the floor payoff (inf for the put; inf * 0 for the call)
+    assert math.isnan(price[4]) and price[5] == inf, price[4:6]
+    # r = +inf: S = +inf at every step, exp(-r t) = 0 (0 * inf for the call; 0 for the put)
+    assert math.isnan(price[6]) and price[7] == 0.0, price[6:8]
