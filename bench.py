@@ -365,6 +365,23 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------------------- GPU arm
+NCU_FIGURES = ("dram_bytes_per_launch_full", "thread_instructions_per_path_step",
+               "xu_per_path_step", "issue_busy", "xu_pipe_busy")
+
+
+def ncu_figures(path=None):
+    """The `<key>: <number>` lines of the committed ncu summary of the Heston
+    simulate kernel (the figures the roofline block reports), as floats."""
+    path = Path(path) if path else ROOT / "profiles" / "heston_simulate_ncu.md"
+    out = {}
+    if path.exists():
+        for line in path.read_text().splitlines():
+            key, sep, val = line.partition(":")
+            if sep and key in NCU_FIGURES:
+                out[key] = float(val)
+    return out
+
+
 def main_gpu(args):
     import torch
     import torch.distributed as dist
@@ -493,15 +510,10 @@ def main_gpu(args):
     }
     # DRAM bytes per full launch, from the committed ncu summary (a small case
     # of the same kernel scaled by the option count; see that file)
-    prof = ROOT / "profiles" / "heston_simulate_ncu.md"
-    if prof.exists():
-        for line in prof.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch_full:"):
-                roofline["traffic"] = int(line.split(":")[1]) * n_opt // N_OPT
-            for key in ("thread_instructions_per_path_step", "xu_per_path_step", "issue_busy",
-                        "xu_pipe_busy"):
-                if line.startswith(key + ":"):
-                    roofline["measured"][key] = float(line.split(":")[1])
+    figs = ncu_figures()
+    if "dram_bytes_per_launch_full" in figs:
+        roofline["traffic"] = int(figs.pop("dram_bytes_per_launch_full")) * n_opt // N_OPT
+    roofline["measured"].update(figs)
     m = roofline["measured"]
     if "thread_instructions_per_path_step" in m and "xu_per_path_step" in m:
         # the same bound with this kernel's own (ncu-measured) instruction mix
