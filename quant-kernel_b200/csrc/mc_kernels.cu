@@ -22,7 +22,8 @@
 //              stratified_sampling.cpp:11-35, quasi_monte_carlo.cpp:10-56
 // Heston keeps log(S/spot) instead of S: the reference's s * exp(a) step with
 // the std::max(s, 1e-12) floor is the same map as x + a floored at
-// log(1e-12/spot), and it removes the per-step exp.
+// log(1e-12/spot), and it removes the per-step exp; sqrt(v) times the
+// Box-Muller radius is taken as one square root.
 #include "mc_device.cuh"
 #include "mc_launch.h"
 
@@ -219,8 +220,8 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
 }
 
 // ----------------------------------------------------------------------------
-// Heston full-truncation Euler.  State (x, v) with x = log(S/spot), kept as
-// y = x - j (r-q)dt after j steps (see xu below):
+// Heston full-truncation Euler.  State (x, v) with x = log(S/spot), or y =
+// x - j (r-q)dt after j steps where the drift is small (DF below):
 //   x' = max_nan(x + (r-q)dt - v dt/2 + sqrt(v) sqrt(dt) z1, log(1e-12/spot))
 //   v' = max(v (1 - kappa dt) + kappa theta dt
 //            + sigma sqrt(dt) sqrt(v) (rho z1 + sqrt(1-rho^2) z2), 0)
