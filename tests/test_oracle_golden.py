@@ -60,6 +60,22 @@ def test_oracle_bitwise_equals_reference_live(oracle, ref):
             assert _same(got, want), (model, a, got, want)
 
 
+def test_oracle_heston_extreme_drift_equals_reference_live(oracle, ref):
+    """Heston accepts any r and q (heston_monte_carlo.cpp:18-24 checks neither):
+    drifts that pin every path to the 1e-12 floor, send it to +inf, or are
+    NaN give the same prices in the oracle as in the reference."""
+    inf = math.inf
+    base = dict(spot=100.0, strike=95.0, t=1.5, vol=0.0, v0=0.04, kappa=1.5, theta=0.05,
+                sigma=0.6, rho=-0.6, paths=501, steps=17, seed=77)
+    for r, q in ((0.03, inf), (0.03, 1e4), (-inf, 0.0), (inf, 0.0), (0.03, -inf), (-1e4, 0.0),
+                 (math.nan, 0.0), (0.03, math.nan), (0.7, 0.0), (0.0, 0.9)):
+        for ot in (0, 1):
+            a = dict(base, r=r, q=q, option_type=ot)
+            got, _ = oracle.price(HESTON, **a)
+            want = ref.price(HESTON, **a)
+            assert _same(got, want), (a, got, want)
+
+
 @pytest.mark.parametrize("i", range(len(GOLDEN["heston_cf"])))
 def test_heston_cf_matches_reference(oracle, i):
     case = GOLDEN["heston_cf"][i]
