@@ -311,8 +311,11 @@ QK_EXPORT int32_t qk_mcm_quasi_monte_carlo_halton_price_se_batch(
  * of 262,144 paths); larger batches return QK_ERR_BAD_SIZE before any GPU
  * work.  The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current, so make it before any
- * stream capture.  Calls share the array; this entry point serialises them
- * and is synchronous, so its calls never overlap on the GPU. */
+ * stream capture.  Calls share the array, which keeps the last call's
+ * contents (every call overwrites what it reads, so nothing needs clearing);
+ * two calls running on the GPU at once would race on it, so this entry point
+ * serialises its calls with a lock and returns only after the results are
+ * copied back. */
 QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_batch_noalloc(
     const double* spot, const double* strike, const double* t, const double* r, const double* q,
     const double* v0, const double* kappa, const double* theta, const double* sigma,
