@@ -42,9 +42,6 @@ struct Cx {
 __device__ __forceinline__ Cx cx(double r, double i) { return Cx{r, i}; }
 __device__ __forceinline__ Cx operator+(Cx a, Cx b) { return cx(a.re + b.re, a.im + b.im); }
 __device__ __forceinline__ Cx operator-(Cx a, Cx b) { return cx(a.re - b.re, a.im - b.im); }
-__device__ __forceinline__ Cx operator*(Cx a, Cx b) {
-    return cx(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re);
-}
 __device__ __forceinline__ Cx operator*(double s, Cx a) { return cx(s * a.re, s * a.im); }
 __device__ __forceinline__ Cx operator/(Cx a, Cx b) {
     // Smith's algorithm (scaled division)
