@@ -323,12 +323,15 @@ class ClockSampler:
     def __init__(self, index):
         self.index = index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{index}.csv"
+        self.path = None
 
     def start(self):
+        import tempfile
+
         try:
-            self.path.parent.mkdir(exist_ok=True)
-            self.fh = open(self.path, "w")
+            fd, name = tempfile.mkstemp(prefix=f"qk_clocks_gpu{self.index}_", suffix=".csv")
+            self.path = Path(name)
+            self.fh = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
                  "-lms", "200", "-i", str(self.index)], stdout=self.fh, stderr=subprocess.DEVNULL)
@@ -346,7 +349,9 @@ class ClockSampler:
         self.fh.close()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.path.read_text().splitlines():
+        text = self.path.read_text()
+        self.path.unlink(missing_ok=True)
+        for line in text.splitlines():
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue

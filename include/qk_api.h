@@ -307,15 +307,18 @@ QK_EXPORT int32_t qk_mcm_quasi_monte_carlo_halton_price_se_batch(
  * arrays; out_stderr may be NULL) and the same kernels and results; every
  * device buffer lives in one fixed 16.6 MiB array per GPU, held until the
  * process exits.  Limits: n <= 4096 options and at most 262,144 tiles in
- * total (a tile is 512 antithetic path pairs of one option, e.g. 1024 options
- * of 262,144 paths); larger batches return QK_ERR_BAD_SIZE before any GPU
- * work.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current, so make it before any
- * stream capture.  Calls share the array, which keeps the last call's
- * contents (every call overwrites what it reads, so nothing needs clearing);
- * two calls running on the GPU at once would race on it, so this entry point
- * serialises its calls with a lock and returns only after the results are
- * copied back. */
+ * total, where an option of P paths takes min(4096, ceil(ceil(P/2) / 512))
+ * tiles (1024 options of 262,144 paths fill the limit; past 2^22 paths an
+ * option's tiles grow instead of multiplying); larger batches return
+ * QK_ERR_BAD_SIZE before any GPU work.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress) and creates the
+ * library's non-blocking stream for this entry point, with that device
+ * current, so make it before any stream capture; later calls use only that
+ * stream (never the legacy default stream).  Calls share the array, which
+ * keeps the last call's contents (every call overwrites what it reads, so
+ * nothing needs clearing); two calls running on the GPU at once would race on
+ * it, so this entry point serialises its calls with a lock and returns only
+ * after the results are copied back. */
 QK_EXPORT int32_t qk_mcm_heston_monte_carlo_price_batch_noalloc(
     const double* spot, const double* strike, const double* t, const double* r, const double* q,
     const double* v0, const double* kappa, const double* theta, const double* sigma,

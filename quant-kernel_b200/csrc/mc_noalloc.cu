@@ -12,9 +12,12 @@
 // array of fixed size.  The array exists once per GPU that loads the library
 // and is held until the process exits.
 //
-// Limits: at most kMaxOptions options and kMaxTiles tiles per call (a tile is
-// 512 antithetic pairs of one option: 1024 options of 262144 paths fill it).
-// Larger calls are rejected before any GPU work.
+// Limits: at most kMaxOptions options and kMaxTiles tiles per call.  An
+// option of P paths has ceil(P/2) antithetic pairs and takes
+// min(4096, ceil(pairs / 512)) tiles: a tile holds 512 pairs until an option
+// would need more than 4096 tiles (over 2^22 paths), after which each tile
+// holds 512 * ceil(pairs / 2^21) pairs.  1024 options of 262144 paths fill the
+// array.  Larger calls are rejected before any GPU work.
 //
 // Every call shares the array and it keeps the last call's contents.  Nothing
 // in it has to start at zero: each call overwrites every record, tile slot and
@@ -22,6 +25,11 @@
 // only after their results are copied back, so calls through this entry point
 // never overlap on the GPU; any other work that touched the same array while a
 // call runs would race with it.
+//
+// The copies and launches go to a non-blocking stream of the library's own,
+// created once per device at set-up: the legacy default stream would join
+// (and so break) a global-mode stream capture that another thread of the
+// process has in progress.
 #include "mc_noalloc.h"
 
 #include <cstring>
@@ -29,6 +37,7 @@
 
 #include "mc_launch.h"
 #include "mc_plan.h"
+#include "qk_fault.h"
 
 namespace qkb {
 
@@ -51,23 +60,32 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;                               // serialises calls (and set-up)
 unsigned char* g_scratch_dev[kMaxDevices] = {};  // per-device address, set once
+cudaStream_t g_stream_dev[kMaxDevices] = {};     // per-device stream, set once
 
-// Fixed launch shape: 256 threads x 2 pairs = 512 antithetic pairs per tile,
-// the unit the tile limit is stated in.  The regular entry uses 128-thread
-// CTAs; the same paths summed in other tile groups agree to ~1e-15 relative
-// (double-double sums), not always bit for bit.
+// Fixed launch shape: 256 threads x 2 pairs = 512 antithetic pairs per tile
+// pass.  The regular entry uses 128-thread CTAs; the same paths summed in
+// other tile groups agree to ~1e-15 relative (double-double sums), not always
+// bit for bit.
 constexpr int kBlock = 256;
 constexpr int kUpt = 2;
 
-// Device address of the scratch array on `dev` (the current device).
-cudaError_t scratch_address(int dev, unsigned char** out) {
+// Set-up on `dev` (the current device), once: the scratch array's device
+// address and the library's stream for this entry point.
+cudaError_t device_setup(int dev, unsigned char** base, cudaStream_t* stream) {
     if (g_scratch_dev[dev] == nullptr) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_scratch_dev[dev] = static_cast<unsigned char*>(p);
     }
-    *out = g_scratch_dev[dev];
+    if (g_stream_dev[dev] == nullptr) {
+        cudaStream_t s = nullptr;
+        cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+        g_stream_dev[dev] = s;
+    }
+    *base = g_scratch_dev[dev];
+    *stream = g_stream_dev[dev];
     return cudaSuccess;
 }
 
@@ -93,7 +111,8 @@ NoAllocStatus noalloc_heston_batch(const BatchInput& in, double* out_prices, dou
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess && (dev < 0 || dev >= kMaxDevices)) e = cudaErrorInvalidDevice;
     unsigned char* base = nullptr;
-    if (e == cudaSuccess) e = scratch_address(dev, &base);
+    cudaStream_t st = nullptr;
+    if (e == cudaSuccess) e = device_setup(dev, &base, &st);
     if (e != cudaSuccess) {
         *cuda_err = e;
         return NoAllocStatus::kCudaError;
@@ -104,8 +123,9 @@ NoAllocStatus noalloc_heston_batch(const BatchInput& in, double* out_prices, dou
     double* d_price = reinterpret_cast<double*>(base + kOffPrices);
     double* d_se = reinterpret_cast<double*>(base + kOffStderr);
 
-    // Pass 2: pack in fixed stack chunks and copy each (synchronous copies
-    // from pageable memory: no staging buffer of ours).
+    // Pass 2: pack in fixed stack chunks and copy each (copies from pageable
+    // memory, which return once the source has been read: no staging buffer
+    // of ours).
     constexpr int kChunk = 64;
     McOption rec[kChunk];
     int64_t tb[kChunk];
@@ -118,10 +138,14 @@ NoAllocStatus noalloc_heston_batch(const BatchInput& in, double* out_prices, dou
             running += tile_option(rec[j], kBlock, kUpt);
             tb[j] = rec[j].tile_begin;
         }
-        e = cudaMemcpy(d_rec + i0, rec, sizeof(McOption) * m, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(d_tb + i0, tb, sizeof(int64_t) * m, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(d_rec + i0, rec, sizeof(McOption) * m, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_tb + i0, tb, sizeof(int64_t) * m, cudaMemcpyHostToDevice, st);
+        // the stack chunk is rewritten next: wait until this one is consumed
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
-    if (e == cudaSuccess) e = cudaMemcpy(d_tb + in.n, &running, sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_tb + in.n, &running, sizeof(int64_t), cudaMemcpyHostToDevice, st);
 
     if (e == cudaSuccess && running > 0) {
         SimArgs a;
@@ -131,13 +155,20 @@ NoAllocStatus noalloc_heston_batch(const BatchInput& in, double* out_prices, dou
         a.n_tiles = running;
         a.partials = d_part;
         a.max_ctas = 0x7fffffff;
-        e = launch_simulate(kFamHeston, true, kBlock, kUpt, 1, a, 0);
+        e = injected_fault(kFaultLaunch);
+        if (e == cudaSuccess) e = launch_simulate(kFamHeston, true, kBlock, kUpt, 1, a, st);
     }
-    if (e == cudaSuccess) e = launch_finalize(d_rec, in.n, d_part, d_price, d_se, nullptr, nullptr, 0);
+    if (e == cudaSuccess) e = launch_finalize(d_rec, in.n, d_part, d_price, d_se, nullptr, nullptr, st);
+    if (e == cudaSuccess) e = injected_fault(kFaultCopy);
     if (e == cudaSuccess)
-        e = cudaMemcpy(out_prices, d_price, sizeof(double) * in.n, cudaMemcpyDeviceToHost);
+        e = cudaMemcpyAsync(out_prices, d_price, sizeof(double) * in.n, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && out_stderr)
-        e = cudaMemcpy(out_stderr, d_se, sizeof(double) * in.n, cudaMemcpyDeviceToHost);
+        e = cudaMemcpyAsync(out_stderr, d_se, sizeof(double) * in.n, cudaMemcpyDeviceToHost, st);
+    // the results are in the caller's arrays only once the stream is done; on
+    // an error, drain what was queued before returning so that the next call
+    // never overlaps it
+    const cudaError_t es = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = es;
     if (e != cudaSuccess) {
         *cuda_err = e;
         return NoAllocStatus::kCudaError;

@@ -12,7 +12,7 @@ struct BatchInput;
 
 // Capacity of the fixed device array (one per GPU, held until exit).
 constexpr int32_t kNoAllocMaxOptions = 4096;
-constexpr int64_t kNoAllocMaxTiles = 262144;  // tiles of 512 antithetic pairs
+constexpr int64_t kNoAllocMaxTiles = 262144;  // an option takes min(4096, ceil(pairs/512))
 constexpr size_t kNoAllocScratchBytes = 17400064;  // 16.6 MiB
 
 enum class NoAllocStatus { kOk, kTooManyOptions, kTooManyTiles, kCudaError };

@@ -462,7 +462,7 @@ int32_t qk_mcm_heston_monte_carlo_price_batch_noalloc(
             return QK_ERR_BAD_SIZE;
         case qkb::NoAllocStatus::kTooManyTiles:
             set_error_fmt("bad batch size: %lld tiles exceed the no-allocation limit of %lld "
-                          "(one tile = 512 path pairs of one option)",
+                          "(an option of P paths takes min(4096, ceil(ceil(P/2)/512)) tiles)",
                           (long long)tiles, (long long)qkb::kNoAllocMaxTiles);
             return QK_ERR_BAD_SIZE;
         default:

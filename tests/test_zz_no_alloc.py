@@ -69,3 +69,43 @@ def test_noalloc_rejects_batches_beyond_its_limits(qk):
     rc, _, _ = _noalloc(qk, too_long)
     assert rc == -2
     assert "tiles exceed the no-allocation limit of 262144" in qk.get_last_error()
+
+
+def test_noalloc_tile_geometry_past_2_22_paths(qk):
+    # one option of 2^23 paths: past 2^22 paths an option keeps 4096 tiles and
+    # each tile holds more than 512 pairs
+    big = workloads.heston(1, paths=2**23, steps=3, seed=23)
+    want_p, want_se = qk.heston_monte_carlo_price_se_batch(**big)
+    rc, got_p, got_se = _noalloc(qk, big)
+    assert rc == 0, qk.get_last_error()
+    np.testing.assert_allclose(got_p, want_p, rtol=1e-13, atol=0)
+    np.testing.assert_allclose(got_se, want_se, rtol=1e-10, atol=0)
+
+
+def test_noalloc_at_exactly_the_tile_limit(qk):
+    # 64 options of 2^22 paths take 64 x 4096 = 262,144 tiles: the limit itself
+    edge = workloads.heston(64, paths=2**22, steps=2, seed=24)
+    rc, got_p, got_se = _noalloc(qk, edge)
+    assert rc == 0, qk.get_last_error()
+    want_p, want_se = qk.heston_monte_carlo_price_se_batch(**edge)
+    np.testing.assert_allclose(got_p, want_p, rtol=1e-13, atol=0)
+    np.testing.assert_allclose(got_se, want_se, rtol=1e-10, atol=0)
+
+
+@pytest.mark.parametrize("site,err", [("launch", "cudaErrorLaunchFailure"),
+                                      ("copy", "cudaErrorUnknown")])
+def test_noalloc_injected_failures_leave_the_next_call_correct(qk, monkeypatch, site, err):
+    # host-side injection: the call reports the failure without touching the
+    # GPU at that site, and the next call, disarmed, prices as the regular entry
+    batch = workloads.heston(8, paths=8192, steps=16, seed=25)
+    want_p, want_se = qk.heston_monte_carlo_price_se_batch(**batch)
+    monkeypatch.setenv("QK_B200_FAULT", site)
+    rc, _, _ = _noalloc(qk, batch)
+    assert rc == -4
+    msg = qk.get_last_error()
+    assert err in msg and "[injected]" in msg
+    monkeypatch.delenv("QK_B200_FAULT")
+    rc, got_p, got_se = _noalloc(qk, batch)
+    assert rc == 0, qk.get_last_error()
+    np.testing.assert_allclose(got_p, want_p, rtol=1e-13, atol=0)
+    np.testing.assert_allclose(got_se, want_se, rtol=1e-10, atol=0)
