@@ -46,11 +46,28 @@ METRIC = "Heston prices/sec at <=5e-4*S err: surrogate vs plain GPU MC; path-ste
 UNIT = "path-steps/s"
 N_OPT, PATHS, STEPS = 1024, 262144, 200
 WORKLOAD = f"heston full-truncation Euler: {N_OPT} calls x {PATHS} paths x {STEPS} steps"
-# Algorithmic cost of one Heston path-step (reference formulas: 2 normals by
-# Box-Muller with half a Philox4x32-10 call, sqrt(v), exp): 6 special-function
-# ops, ~20 FP32 ops, ~30 INT32 ops.
-XU_PER_UNIT, ALU_PER_UNIT = 6, 50
-SMS, ISSUE_PER_CLK, XU_PER_CLK = 148, 128, 16
+# Algorithmic cost per path-step, counted from the reference formulas
+# (model_concepts.h) under antithetic pairing, where the two paths of a pair
+# share their normals:
+#   Heston      one Box-Muller pair per pair-step (log, sqrt, sin, cos) and per
+#               path sqrt(v) and exp: 8 XU per pair-step = 4 per path-step;
+#               ALU ~30 per path-step: the step's ~12 FMA-fused FP32 ops, half
+#               a Box-Muller pair's ~6 FP ops, a quarter of a Philox4x32-10
+#               call (~60 integer instructions per call)
+#   Euler / LV  one normal per pair-step (half a Box-Muller pair: 2 XU): 1 XU
+#               per path-step; ALU ~13 (step ~4, Box-Muller ~1.5, Philox 1/8
+#               call ~7.5)
+#   Milstein    as Euler plus 3 FP32 ops: 1 XU, ALU ~16
+XU_PER_UNIT, ALU_PER_UNIT = 4, 30
+STEP_COST = {2: (1, 13), 3: (1, 16), 4: (1, 13), 6: (XU_PER_UNIT, ALU_PER_UNIT)}  # model: (XU, ALU)
+# FP64 operations per antithetic pair of the terminal model (make_bsm_terminal
+# with one normal per pair): half a Box-Muller pair (log 20, sqrt 6, sin+cos
+# 17 and ~6 arithmetic: ~25), two exp (16 each), d0 + d1 z twice with one
+# multiply (3), two spot * exp (2), two payoffs (4): ~66, on the FP64 pipe.
+# (exp, log, sin/cos and sqrt are costed as textbook range reduction plus a
+# polynomial of the degree FP64 accuracy needs.)
+FP64_PER_PAIR = 66
+SMS, ISSUE_PER_CLK, XU_PER_CLK, FP64_PER_CLK = 148, 128, 16, 64
 SUR_CHECKPOINT = ROOT / "quant-kernel_b200" / "quantkernel_b200" / "data" / "heston_surrogate.qksur"
 SUR_FLOP_PER_ROW = 2 * (9 * 256 + 256 * 256 * 2 + 256)  # forward multiply-adds x 2
 
@@ -97,30 +114,12 @@ HESTON_KEYS = ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma",
 CPU_TIMER = ROOT / "oracle" / "_ref" / "cpu_timer"
 
 
-def _time_cpu_cxx(b):
-    """The compiled reference's qk_mcm_heston_monte_carlo_price_batch timed by
-    the C++ harness (oracle/cpu_timer.cpp, std::chrono around the call)."""
-    import tempfile
-
+def _time_cpu_cxx(b, symbol="qk_mcm_heston_monte_carlo_price_batch"):
+    """The compiled reference's batch entry point `symbol` timed by the C++
+    harness (oracle/cpu_timer.cpp, std::chrono around the call)."""
     from oracle import oracle as orc
 
-    n = len(b["spot"])
-    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
-        f.write(np.int32(n).tobytes())
-        for k in HESTON_KEYS[:10]:
-            f.write(np.ascontiguousarray(b[k], np.float64).tobytes())
-        for k in ("option_type", "paths", "steps"):
-            f.write(np.ascontiguousarray(b[k], np.int32).tobytes())
-        f.write(np.ascontiguousarray(b["seed"], np.uint64).tobytes())
-        path = f.name
-    try:
-        r = subprocess.run([str(CPU_TIMER), str(orc.REF_SO), "qk_mcm_heston_monte_carlo_price_batch",
-                            path, "1"], capture_output=True, text=True, timeout=1800)
-    finally:
-        os.unlink(path)
-    if r.returncode != 0:
-        raise RuntimeError(f"cpu_timer failed: {r.stderr[-1000:]}")
-    return json.loads(r.stdout.strip().splitlines()[-1])["seconds"][0]
+    return orc.time_reference_batch(symbol, b)[0][0]
 
 
 def _time_cpu(impl, n_opt, paths, threads):
@@ -223,6 +222,80 @@ def _vr_cpu_leg(s):
     print(json.dumps(out))
 
 
+def _bsm_cpu_leg(s):
+    """The reference's qk_mcm_antithetic_variates_price_batch (OpenMP over
+    options, FP64) on the 64-option terminal workload, timed from C++, paths
+    scaled to about s["seconds"] (cost is linear in paths)."""
+    from oracle import oracle as orc
+    from quantkernel_b200 import workloads
+
+    paths = 4096
+    while True:
+        b = workloads.bsm_terminal(64, paths=paths)
+        if s["impl"] == "reference" and orc.timer_available():
+            dt = _time_cpu_cxx(b, "qk_mcm_antithetic_variates_price_batch")
+        else:
+            o = orc.Oracle()
+            t0 = time.perf_counter()
+            for i in range(64):
+                o.price(orc.ANTITHETIC, *(b[k][i].item() for k in ("spot", "strike", "t", "vol",
+                                                                     "r", "q", "option_type",
+                                                                     "paths")),
+                        seed=int(b["seed"][i]))
+            dt = time.perf_counter() - t0
+        if dt >= 0.5 * s["seconds"] or paths >= (1 << 24):
+            break
+        paths = min(1 << 24, max(2 * paths, int(paths * s["seconds"] / max(dt, 1e-3))))
+    print(json.dumps({"paths_per_option": paths, "seconds": dt, "paths": 64 * paths}))
+
+
+def mixed_cpu_batch(div):
+    """The mixed workload with every option's paths divided by `div` (at least
+    16): the same options, models, steps and weighting of path-steps by model."""
+    from quantkernel_b200 import workloads
+
+    b = workloads.mixed()
+    b["paths"] = np.maximum(16, b["paths"] // div).astype(np.int32)
+    return b
+
+
+def _mixed_cpu_leg(s):
+    """The reference's own batch entry point per model (Euler-Maruyama,
+    Milstein, local vol, Heston; each an OpenMP loop over its options) on the
+    mixed workload with paths divided by a factor that brings the four calls
+    to about s["seconds"]; timed from C++ and summed."""
+    from oracle import oracle as orc
+
+    div = 4096
+    while True:
+        b = mixed_cpu_batch(div)
+        tot, units = 0.0, 0
+        per = {}
+        for m in np.unique(b["model"]):
+            idx = np.nonzero(b["model"] == m)[0]
+            sub = {k: v[idx] for k, v in b.items()}
+            if s["impl"] == "reference" and orc.timer_available():
+                dt = _time_cpu_cxx(sub, orc.MODEL_BATCH_SYMBOL[int(m)])
+            else:
+                o = orc.Oracle()
+                t0 = time.perf_counter()
+                if int(m) == orc.HESTON:
+                    o.heston_batch(**{k: sub[k] for k in HESTON_KEYS})
+                else:
+                    o.bsm_family_batch(int(m), *(sub[k] for k in ("spot", "strike", "t", "vol",
+                                                                   "r", "q", "option_type",
+                                                                   "paths", "steps", "seed")))
+                dt = time.perf_counter() - t0
+            u = int((sub["paths"].astype(np.int64) * sub["steps"]).sum())
+            per[int(m)] = {"seconds": dt, "path_steps": u}
+            tot += dt
+            units += u
+        if tot >= 0.5 * s["seconds"] or div <= 1:
+            break
+        div = max(1, min(div // 2, int(div * tot / s["seconds"])))
+    print(json.dumps({"paths_divisor": div, "seconds": tot, "path_steps": units, "per_model": per}))
+
+
 def cpu_leg(spec):
     """Runs in a subprocess with OMP_NUM_THREADS set; prints one JSON line."""
     s = json.loads(spec)
@@ -230,6 +303,10 @@ def cpu_leg(spec):
         return _cf_cpu_leg(s)
     if s.get("kind") == "vr":
         return _vr_cpu_leg(s)
+    if s.get("kind") == "bsm":
+        return _bsm_cpu_leg(s)
+    if s.get("kind") == "mixed":
+        return _mixed_cpu_leg(s)
     target = s["seconds"]
     reps = s.get("reps", 1)
     n_opt, paths = 8, 4096
@@ -487,32 +564,15 @@ def main_gpu(args):
     value = world * units_per_step * args.steps / (total_ms / 1e3)
     sim_ms = statistics.mean(kern_ms)
     f_mhz = clk.get("sm_mhz") or 1965.0
-    achieved = units_per_step / (sim_ms / 1e3)  # path-steps/s of the simulate kernel
-    issue_peak = SMS * ISSUE_PER_CLK * f_mhz * 1e6  # thread-instructions/s
-    xu_peak = SMS * XU_PER_CLK * f_mhz * 1e6
-    bound_units = min(issue_peak / ALU_PER_UNIT, xu_peak / XU_PER_UNIT)
-    roofline = {
-        "bound": "alu" if issue_peak / ALU_PER_UNIT <= xu_peak / XU_PER_UNIT else "xu",
-        "achieved": achieved * ALU_PER_UNIT / 1e9,
-        "peak": bound_units * ALU_PER_UNIT / 1e9,
-        "unit": "Gop/s",
-        "frac": achieved / bound_units,
-        "traffic": None,
+    roofline = step_roofline({6: units_per_step}, sim_ms / 1e3, f_mhz)
+    roofline.update({
         "kernel": ("mc_simulate_kernel<Heston,{block},{units_per_thread},antithetic,"
                    "step_unroll {step_unroll}>").format(**plan_cfg),
         "launch_config": {**plan_cfg,
                           "chosen_by": "autotuner (block x paths per thread x step unrolling)"},
         "kernel_ms": sim_ms,
         "measured": {"source": "ncu, profiles/heston_simulate_ncu.md"},
-        "note": ("frac > 1: the reference formulas cost 6 XU + 50 ALU per path-step; this "
-                 "kernel needs 2.5 XU + ~23 (antithetic pairs share normals, log-space spot "
-                 "drops the per-step exp, sqrt(v) times the Box-Muller radius is one "
-                 "square root)"),
-        "per_unit": {"xu": XU_PER_UNIT, "alu": ALU_PER_UNIT, "unit": "path-step"},
-        "peak_source": ("nominal per-clock SM widths (148 SMs x 128 issue / 16 XU per clk) at "
-                        "the SM clock sampled during the timed region; the driver's measured "
-                        "peaks are HBM copy and bf16 GEMM, which do not bound this kernel"),
-    }
+    })
     # DRAM bytes per full launch, from the committed ncu summary (a small case
     # of the same kernel scaled by the option count; see that file)
     figs = ncu_figures()
@@ -521,10 +581,13 @@ def main_gpu(args):
     roofline["measured"].update(figs)
     m = roofline["measured"]
     if "thread_instructions_per_path_step" in m and "xu_per_path_step" in m:
-        # the same bound with this kernel's own (ncu-measured) instruction mix
+        # the same peaks against this kernel's own (ncu-measured) instruction
+        # mix: how close the kernel runs to what its own instructions allow
+        issue_peak = SMS * ISSUE_PER_CLK * f_mhz * 1e6
+        xu_peak = SMS * XU_PER_CLK * f_mhz * 1e6
         own = min(issue_peak / m["thread_instructions_per_path_step"],
                   xu_peak / m["xu_per_path_step"])
-        m["frac_of_own_mix_bound"] = achieved / own
+        roofline["frac_of_own_mix_bound"] = (units_per_step / (sim_ms / 1e3)) / own
 
     threads = host_threads()
     try:
@@ -546,8 +609,8 @@ def main_gpu(args):
     try:
         if world > 1:  # the secondary 1-GPU workloads run in the N = 1 line only
             raise RuntimeError("secondary legs run in the 1-GPU run only")
-        extras["mixed"] = mixed_leg(qk)
-        extras["bsm_terminal"] = bsm_terminal_leg(qk)
+        extras["mixed"] = mixed_leg(qk, f_mhz=f_mhz)
+        extras["bsm_terminal"] = bsm_terminal_leg(qk, f_mhz=f_mhz)
         extras["heston_cf"] = heston_cf_leg(qk)
         extras["variance_reduction"] = vr_leg(qk)
         if Path(args.sur_checkpoint).exists():
@@ -758,7 +821,63 @@ def _time_plan(plan, stream, flush, reps):
     return tot / reps
 
 
-def mixed_leg(qk, reps=5):
+def step_roofline(units_by_model, seconds, f_mhz):
+    """Roofline of the stepwise simulate kernels: each model's path-steps at the
+    tighter of its XU and issue bounds (STEP_COST, nominal per-clock SM widths
+    at the sampled SM clock); frac = that bound time / the measured time."""
+    issue_peak = SMS * ISSUE_PER_CLK * f_mhz * 1e6  # thread-instructions/s
+    xu_peak = SMS * XU_PER_CLK * f_mhz * 1e6
+    bound_s, xu_ops, alu_ops, limiters = 0.0, 0.0, 0.0, set()
+    for model, units in units_by_model.items():
+        xu, alu = STEP_COST[int(model)]
+        xu_b, alu_b = xu_peak / xu, issue_peak / alu
+        limiters.add("xu" if xu_b <= alu_b else "alu")
+        bound_s += units / min(xu_b, alu_b)
+        xu_ops += units * xu
+        alu_ops += units * alu
+    bound = limiters.pop() if len(limiters) == 1 else "xu+alu"
+    ops, peak = (xu_ops, xu_peak) if bound == "xu" else (alu_ops, issue_peak)
+    out = {"bound": bound, "unit": "Gop/s", "frac": bound_s / seconds, "traffic": None,
+           "per_unit": {str(m): {"xu": STEP_COST[int(m)][0], "alu": STEP_COST[int(m)][1]}
+                        for m in units_by_model},
+           "unit_of_work": "path-step (antithetic pairs share normals)",
+           "bound_ms": 1e3 * bound_s, "sm_mhz": f_mhz,
+           "peak_source": ("nominal per-clock SM widths (148 SMs x 128 issue / 16 XU per clk) at "
+                           "the SM clock sampled during the timed region; the measured peaks "
+                           "(HBM copy, bf16 GEMM) do not bound this kernel")}
+    if bound in ("xu", "alu"):
+        out["achieved"] = ops / seconds / 1e9
+        out["peak"] = peak / 1e9
+    else:  # mixed limiters: report the time-weighted fraction only
+        out["achieved"] = out["frac"]
+        out["peak"] = 1.0
+        out["unit"] = "fraction of the per-model bound time"
+    return out
+
+
+def _time_plan_kernel(plan, stream, flush, reps):
+    """(ms per execute, ms of the simulate kernels) of a plan built with
+    QK_PLAN_TIMING and no graph, CUDA events on `stream`, L2 flushed."""
+    import torch
+
+    for _ in range(3):
+        flush.zero_()
+        plan.execute(stream.cuda_stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tot, kern = 0.0, 0.0
+    for _ in range(reps):
+        flush.zero_()
+        e0.record(stream)
+        plan.execute(stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        tot += e0.elapsed_time(e1)
+        kern += plan.stats()["simulate_ms"]
+    return tot / reps, kern / reps
+
+
+def mixed_leg(qk, reps=5, f_mhz=1965.0, cpu=True):
     """Uneven batch: 4096 options, BSM-Euler / Milstein / local vol / Heston
     1:1:1:1, paths log-uniform 2^12..2^20, steps 16..512, as one plan in a
     CUDA graph: the persistent work-stealing kernel, per-family grids, and the
@@ -793,37 +912,99 @@ def mixed_leg(qk, reps=5):
         out[idx] = sub.results()[0]
         sub.close()
     assert np.allclose(out, p_pers, rtol=1e-12, atol=0)
-    return {"workload": "4096 options, Euler/Milstein/local-vol/Heston 1:1:1:1, paths 2^U[12,20], "
-                        "steps 2^U[4,9]", "path_steps": units,
-            "autotuned_graph_ms": ms, "path_steps_per_s": units / (ms / 1e3),
-            "persistent_graph_ms": ms_pers, "family_grids_graph_ms": ms_grids,
-            "per_model_plans_ms": per_model, "speedup_vs_per_model": per_model / ms,
-            "launch_config": cfg,
-            "launch_config_note": "units_per_thread 0 = persistent kernel, -1 = one grid per "
-                                  "family group"}
+    # kernel time of the autotuned launch (no graph: events around the
+    # simulate kernels only) for the roofline
+    plan = qk.plan(**b, flags=QK_PLAN_AUTOTUNE | QK_PLAN_TIMING)
+    _, kern_ms = _time_plan_kernel(plan, stream, flush, reps)
+    plan.close()
+    by_model = {int(m): workloads.path_steps({k: v[b["model"] == m] for k, v in b.items()})
+                for m in np.unique(b["model"])}
+    roof = step_roofline(by_model, kern_ms / 1e3, f_mhz)
+    roof["kernel_ms"] = kern_ms
+    res = {"workload": "4096 options, Euler/Milstein/local-vol/Heston 1:1:1:1, paths 2^U[12,20], "
+                       "steps 2^U[4,9]", "path_steps": units,
+           "autotuned_graph_ms": ms, "path_steps_per_s": units / (ms / 1e3),
+           "persistent_graph_ms": ms_pers, "family_grids_graph_ms": ms_grids,
+           "per_model_plans_ms": per_model, "speedup_vs_per_model": per_model / ms,
+           "launch_config": cfg,
+           "launch_config_note": "units_per_thread 0 = persistent kernel, -1 = one grid per "
+                                 "family group",
+           "roofline": roof}
+    if cpu:
+        res["cpu_baseline"] = _rate_baseline("mixed", "path_steps", "path-steps/s", 10.0, 4.0,
+                                             lambda c: (f"the 4096 options with paths divided by "
+                                                        f"{c['paths_divisor']} (at least 16): "
+                                                        f"{c['path_steps']:.3g} path-steps, one "
+                                                        f"reference batch call per model"))
+    return res
 
 
-def bsm_terminal_leg(qk, reps=20):
-    """64 BSM options x 131072 paths, terminal GBM with antithetic pairs."""
+def _rate_baseline(kind, units_key, unit, seconds, seconds_1core, describe):
+    """A CPU-leg rate on all host threads and on one core, as a cpu_baseline
+    record; never raises (the GPU line is printed either way)."""
+    threads = host_threads()
+    try:
+        c = run_cpu(cpu_kind(), threads, seconds=seconds, kind=kind)
+        out = {"value": c[units_key] / c["seconds"], "unit": unit, "cores": threads,
+               "kind": cpu_kind(), "cpu_model": cpu_model(), "timer": cpu_timer_name(),
+               "sample": describe(c)}
+        c1 = run_cpu(cpu_kind(), 1, seconds=seconds_1core, kind=kind)
+        out["value_1_core"] = c1[units_key] / c1["seconds"]
+        out["sample_1_core"] = describe(c1)
+        return out
+    except Exception as exc:
+        return {"value": None, "unit": unit, "cores": threads, "kind": cpu_kind(),
+                "sample": f"failed: {exc}"[:200]}
+
+
+def bsm_terminal_leg(qk, reps=20, f_mhz=1965.0, cpu=True):
+    """64 BSM options x 131072 paths, terminal GBM with antithetic pairs in
+    FP64 (FP64 normals and exponent, as the reference's make_bsm_terminal):
+    device time of a graph-replayed plan, the simulate kernel alone, end to
+    end through qk_mcm_antithetic_variates_price_batch with host buffers, and
+    the reference's own antithetic batch on the host cores."""
     import torch
 
-    from quantkernel_b200 import QK_MC_STANDARD, QK_PLAN_GRAPH, workloads
+    from quantkernel_b200 import QK_MC_ANTITHETIC, QK_PLAN_GRAPH, QK_PLAN_TIMING, workloads
 
     b = workloads.bsm_terminal()
+    n = len(b["spot"])
     stream = torch.cuda.current_stream()
     assert stream.cuda_stream != 0, "time on a non-default stream"
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    plan = qk.plan(model=np.full(64, QK_MC_STANDARD, np.int32), flags=QK_PLAN_GRAPH, **b)
+    plan = qk.plan(model=np.full(n, QK_MC_ANTITHETIC, np.int32), flags=QK_PLAN_GRAPH, **b)
     ms = _time_plan(plan, stream, flush, reps)
     plan.close()
+    plan = qk.plan(model=np.full(n, QK_MC_ANTITHETIC, np.int32), flags=QK_PLAN_TIMING, **b)
+    _, kern_ms = _time_plan_kernel(plan, stream, flush, reps)
+    plan.close()
+    args = [b[k] for k in ("spot", "strike", "t", "vol", "r", "q", "option_type", "paths", "seed")]
+    qk.antithetic_variates_price_batch(*args)
     t0 = time.perf_counter()
     for _ in range(reps):
-        qk.standard_monte_carlo_price_batch(**b)
+        qk.antithetic_variates_price_batch(*args)
     e2e = (time.perf_counter() - t0) / reps
     paths = int(b["paths"].sum())
-    return {"workload": "64 BSM calls/puts x 131072 paths (terminal, antithetic)",
-            "ms": ms, "paths_per_s": paths / (ms / 1e3), "e2e_ms": 1e3 * e2e,
-            "e2e_paths_per_s": paths / e2e}
+    pairs = paths // 2
+    fp64_peak = SMS * FP64_PER_CLK * f_mhz * 1e6
+    res = {"workload": "64 BSM calls/puts x 131072 paths (terminal GBM, antithetic pairs)",
+           "dtype": "f64", "ms": ms, "paths_per_s": paths / (ms / 1e3), "e2e_ms": 1e3 * e2e,
+           "e2e_paths_per_s": paths / e2e, "api": "qk_mcm_antithetic_variates_price_batch",
+           "h2d_bytes": n * 128 + (n + 1) * 8, "d2h_bytes": n * 8,
+           "roofline": {"bound": "fp64", "unit": "GFLOP/s",
+                        "achieved": pairs * FP64_PER_PAIR / (kern_ms / 1e3) / 1e9,
+                        "peak": fp64_peak / 1e9,
+                        "frac": pairs * FP64_PER_PAIR / (kern_ms / 1e3) / fp64_peak,
+                        "traffic": None, "kernel_ms": kern_ms,
+                        "per_unit": {"fp64_ops": FP64_PER_PAIR, "unit": "antithetic pair"},
+                        "peak_source": "nominal 148 SMs x 64 FP64 lanes per clk at the sampled "
+                                       "SM clock"}}
+    if cpu:
+        res["cpu_baseline"] = _rate_baseline(
+            "bsm", "paths", "paths/s", 6.0, 3.0,
+            lambda c: f"the 64 options with {c['paths_per_option']} paths each "
+                      f"(qk_mcm_antithetic_variates_price_batch)")
+    return res
 
 
 def _time_sur_device(sur, feats, layered, reps=10):

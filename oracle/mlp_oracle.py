@@ -47,6 +47,32 @@ def forward(p, x):
     return y, (z1, h1, z2, h2, z3, h3)
 
 
+def bf16_round(x):
+    """Round to the nearest bf16 value (ties to even), returned as float64."""
+    f = np.asarray(x, np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16) << 16
+    return r.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def forward_bf16(p, x):
+    """The network as the GPU evaluates it, in FP64 otherwise: weights of the
+    three hidden layers rounded to bf16, the activations of layers 1 and 2
+    rounded to bf16 after the SiLU (they are the next GEMM's bf16 operand),
+    layer 3's activations and the head (w4, b4) in full precision; exact SiLU
+    and FP64 sums (the GPU sums in FP32 and takes tanh from the
+    special-function unit, so it may round an activation to the neighbouring
+    bf16 value)."""
+    w = unpack(p)
+    h = np.asarray(x, np.float64)
+    for name in ("1", "2", "3"):
+        z = h @ bf16_round(w["W" + name]).T + w["b" + name]
+        h = z * _sig(z)
+        if name != "3":
+            h = bf16_round(h)
+    return h @ w["w4"] + w["b4"][0]
+
+
 def loss_and_grads(p, x, t):
     """Mean squared error over the batch and its gradient (parameter order)."""
     w = unpack(p)

@@ -372,3 +372,68 @@ def host_threads() -> int:
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------------------- C++ timing
+CPU_TIMER = HERE / "_ref" / "cpu_timer"
+_TERM_F64 = ("spot", "strike", "t", "vol", "r", "q")
+_HES_F64 = ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho")
+# The reference batch entry points the timer calls, with the batch keys of
+# their float64 and int32 arguments in declaration order (qk_api.h).
+TIMER_SIGNATURES = {
+    "qk_mcm_heston_monte_carlo_price_batch": (_HES_F64, ("option_type", "paths", "steps")),
+    "qk_mcm_standard_monte_carlo_price_batch": (_TERM_F64, ("option_type", "paths")),
+    "qk_mcm_antithetic_variates_price_batch": (_TERM_F64, ("option_type", "paths")),
+    "qk_mcm_euler_maruyama_price_batch": (_TERM_F64, ("option_type", "paths", "steps")),
+    "qk_mcm_milstein_price_batch": (_TERM_F64, ("option_type", "paths", "steps")),
+    "qk_mcm_local_vol_monte_carlo_price_batch": (_TERM_F64, ("option_type", "paths", "steps")),
+}
+# The reference batch entry point of each stepwise / terminal model code.
+MODEL_BATCH_SYMBOL = {
+    STANDARD: "qk_mcm_standard_monte_carlo_price_batch",
+    ANTITHETIC: "qk_mcm_antithetic_variates_price_batch",
+    EULER: "qk_mcm_euler_maruyama_price_batch",
+    MILSTEIN: "qk_mcm_milstein_price_batch",
+    LOCAL_VOL: "qk_mcm_local_vol_monte_carlo_price_batch",
+    HESTON: "qk_mcm_heston_monte_carlo_price_batch",
+}
+
+
+def timer_available() -> bool:
+    return CPU_TIMER.exists() and REF_SO.exists()
+
+
+def write_timer_input(path, symbol, batch):
+    """The cpu_timer input file for `symbol` on `batch` (dict of arrays)."""
+    f64, i32 = TIMER_SIGNATURES[symbol]
+    n = len(batch["spot"])
+    with open(path, "wb") as fh:
+        fh.write(np.array([len(f64), len(i32), 1, n], np.int32).tobytes())
+        for k in f64:
+            fh.write(np.ascontiguousarray(batch[k], np.float64).tobytes())
+        for k in i32:
+            fh.write(np.ascontiguousarray(batch[k], np.int32).tobytes())
+        fh.write(np.ascontiguousarray(batch["seed"], np.uint64).tobytes())
+
+
+def time_reference_batch(symbol, batch, reps=1, timeout=1800):
+    """Calls the reference's batch entry point `symbol` on `batch` `reps` times
+    from C++ (oracle/_ref/cpu_timer: dlopen, std::chrono::steady_clock around
+    each call; OpenMP threads from OMP_NUM_THREADS).  Returns (seconds of each
+    call, sum of the last call's prices)."""
+    import json
+    import subprocess
+    import tempfile
+
+    with tempfile.NamedTemporaryFile(suffix=".bin", delete=False) as f:
+        path = f.name
+    try:
+        write_timer_input(path, symbol, batch)
+        r = subprocess.run([str(CPU_TIMER), str(REF_SO), symbol, path, str(reps)],
+                           capture_output=True, text=True, timeout=timeout)
+    finally:
+        os.unlink(path)
+    if r.returncode != 0:
+        raise RuntimeError(f"cpu_timer failed: {r.stderr[-1000:]}")
+    out = json.loads(r.stdout.strip().splitlines()[-1])
+    return out["seconds"], out["price_sum"]

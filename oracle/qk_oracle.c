@@ -932,12 +932,13 @@ static double heston_cos_impl(double spot, double strike, double t, double r, do
  * The GPU kernels draw their normals from this counter layout:
  *   key      = (low 32 bits of seed, high 32 bits of seed)
  *   counter  = (unit, block, 0, c3)   c3 = 0 antithetic pairs, 1 plain paths
- *   output x0..x3 -> two Box-Muller pairs:
- *     u  = ((x0 >> 9) + 0.5) * 2^-23,  g = ((x1 >> 9) + 0.5) * 2^-22 - 1
+ * Terminal models (FP64 normals): normal k of the option (k = pair index, or
+ *   path index when plain) is slot k % 4 of quad k / 4; the quad's counters
+ *   (k / 4, 0, 0, c3) and (k / 4, 1, 0, c3) each give one FP64 Box-Muller pair
+ *   from 52-bit words  ub = x0 << 20 | x1 >> 12,  gb = x2 << 20 | x3 >> 12:
+ *     u  = (ub + 0.5) * 2^-52,         g = (gb + 0.5) * 2^-51 - 1
  *     n0 = sqrt(-2 ln u) cos(pi g),    n1 = sqrt(-2 ln u) sin(pi g)
- *     (x2, x3) -> n2, n3 the same way.
- * Terminal models: normal k of the option lives at unit k / 4, block 0,
- *   slot k % 4 (k = pair index, or path index when plain).
+ *   (control variates and importance sampling use the same quads, c3 = 1).
  * One-factor stepwise models: six normals per call as for Heston below;
  *   step j of unit u is block j / 6, normal j % 6.
  * Heston: one call gives six normals, three Box-Muller pairs with 23-bit
@@ -962,9 +963,13 @@ void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-static void box_muller(uint32_t xa, uint32_t xb, double* za, double* zb) {
-    const double u = ((double)(xa >> 9) + 0.5) * 0x1p-23;
-    const double g = ((double)(xb >> 9) + 0.5) * 0x1p-22 - 1.0;
+/* FP64 Box-Muller pair from one call's four words (52-bit radius and angle
+ * words; both conversions below are exact). */
+static void box_muller_f64(const uint32_t x[4], double* za, double* zb) {
+    const uint64_t ub = ((uint64_t)x[0] << 20) | (x[1] >> 12);
+    const uint64_t gb = ((uint64_t)x[2] << 20) | (x[3] >> 12);
+    const double u = ((double)ub + 0.5) * 0x1p-52;
+    const double g = ((double)gb + 0.5) * 0x1p-51 - 1.0;
     const double rad = sqrt(-2.0 * log(u));
     *za = rad * cos(M_PI * g);
     *zb = rad * sin(M_PI * g);
@@ -991,11 +996,13 @@ void qko_philox_normals6(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, d
 
 void qko_philox_normals4(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[4]) {
     const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-    const uint32_t ctr[4] = {c0, c1, 0u, c3};
+    const uint32_t ctr0[4] = {c0, c1, 0u, c3};
+    const uint32_t ctr1[4] = {c0, c1 + 1u, 0u, c3};
     uint32_t x[4];
-    qko_philox4x32_10(ctr, key, x);
-    box_muller(x[0], x[1], &z[0], &z[1]);
-    box_muller(x[2], x[3], &z[2], &z[3]);
+    qko_philox4x32_10(ctr0, key, x);
+    box_muller_f64(x, &z[0], &z[1]);
+    qko_philox4x32_10(ctr1, key, x);
+    box_muller_f64(x, &z[2], &z[3]);
 }
 
 /* One simulated path of unit u under sign sg (+1 / -1) for the stepwise

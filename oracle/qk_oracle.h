@@ -122,7 +122,8 @@ double qko_heston_cos_error_scale(double spot, double strike, double t, double r
 
 /* ---- 3. Philox replay of the GPU stream --------------------------------- */
 void qko_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
-/* The GPU's normal with index k of stream (seed, c0, c1, c3); see qk_oracle.c. */
+/* The terminal kernels' four FP64 normals of quad c0: counters (c0, c1, 0, c3)
+ * and (c0, c1 + 1, 0, c3), one Box-Muller pair each; see qk_oracle.c. */
 void qko_philox_normals4(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[4]);
 /* The Heston kernels' six normals of one call (three Box-Muller pairs). */
 void qko_philox_normals6(uint64_t seed, uint32_t c0, uint32_t c1, uint32_t c3, double z[6]);

@@ -86,28 +86,34 @@ __device__ __forceinline__ float unit_from_bits(uint32_t b23) {  // (b + 1/2) 2^
     return __uint_as_float(0x3F800000u | b23) - 0x1.fffffep-1f;   // y - (1 - 2^-24)
 }
 
-// Box-Muller on two 32-bit words (the layout the FP64 replay in the oracle
-// mirrors):  u = ((xa >> 9) + 1/2) 2^-23 in (0,1), g = ((xb >> 9) + 1/2) 2^-22 - 1
-// in (-1,1);  za = sqrt(-2 ln u) cos(pi g),  zb = sqrt(-2 ln u) sin(pi g).
-// ln u = log2(u) * ln 2, and sqrt(w) = sqrt.approx(w).  For the 23-bit angle,
-// y = 2 + b 2^-22 (exponent of 2.0f) and pi g = pi y - pi (3 - 2^-23): one FMA.
-__device__ __forceinline__ void box_muller(uint32_t xa, uint32_t xb, float& za, float& zb) {
-    constexpr float kPi = 3.14159265358979323846f;
-    constexpr float kOff = (float)(3.14159265358979323846 * (3.0 - 0x1p-23));
-    const float u = unit_from_bits(xa >> 9);
-    const float y = __uint_as_float(0x40000000u | (xb >> 9));
-    const float w = -1.38629436111989061883f * ptx_lg2(u);  // -2 ln u
-    const float rad = ptx_sqrt(w);
-    const float ang = fma_rn(y, kPi, -kOff);
-    za = rad * ptx_cos(ang);
-    zb = rad * ptx_sin(ang);
+// FP64 Box-Muller from one Philox call (the terminal models, which the
+// reference evaluates in FP64 end to end):  52-bit words
+//   ub = x << 20 | y >> 12,  gb = z << 20 | w >> 12,
+//   u = (ub + 1/2) 2^-52 in (0,1),  g = (gb + 1/2) 2^-51 - 1 in (-1,1),
+//   za = sqrt(-2 ln u) cos(pi g),  zb = sqrt(-2 ln u) sin(pi g).
+// Both are formed without an integer-to-double conversion: OR-ing the 52 bits
+// into the mantissa of 1.0 (of 2.0) gives y = 1 + ub 2^-52 (y = 2 + gb 2^-51)
+// exactly, and y - (1 - 2^-53) (y - (3 - 2^-52)) is exact (Sterbenz).
+__device__ __forceinline__ void box_muller_f64(U4 x, double& za, double& zb) {
+    const unsigned long long ub = ((unsigned long long)x.x << 20) | (x.y >> 12);
+    const unsigned long long gb = ((unsigned long long)x.z << 20) | (x.w >> 12);
+    const double u = __longlong_as_double((long long)(0x3FF0000000000000ull | ub)) -
+                     0x1.fffffffffffffp-1;
+    const double g = __longlong_as_double((long long)(0x4000000000000000ull | gb)) -
+                     (3.0 - 0x1p-52);
+    const double rad = sqrt(-2.0 * log(u));
+    double sn, cs;
+    sincospi(g, &sn, &cs);
+    za = rad * cs;
+    zb = rad * sn;
 }
 
-__device__ __forceinline__ void normals4(uint32_t unit, uint32_t block, uint32_t c3, uint32_t k0,
-                                         uint32_t k1, float z[4]) {
-    const U4 x = philox4x32_10(unit, block, 0u, c3, k0, k1);
-    box_muller(x.x, x.y, z[0], z[1]);
-    box_muller(x.z, x.w, z[2], z[3]);
+// Four FP64 normals of quad `unit`: counter (unit, 0, 0, c3) gives normals 0
+// and 1, counter (unit, 1, 0, c3) normals 2 and 3.
+__device__ __forceinline__ void normals4_f64(uint32_t unit, uint32_t c3, uint32_t k0, uint32_t k1,
+                                             double z[4]) {
+    box_muller_f64(philox4x32_10(unit, 0u, 0u, c3, k0, k1), z[0], z[1]);
+    box_muller_f64(philox4x32_10(unit, 1u, 0u, c3, k0, k1), z[2], z[3]);
 }
 
 // sqrt(2 ln 2): sqrt(-2 ln u) = kBmRadius * sqrt(-log2 u).

@@ -101,14 +101,18 @@ __device__ __forceinline__ double clamp_unit(double u) {
 }
 
 // ----------------------------------------------------------------------------
-// Terminal GBM (models 0, 1, 5).  Unit = quad of four normals (one Philox
-// call).  Normal k serves pair k (antithetic) or path k (plain); with an odd
-// antithetic path count, normal n_pairs drives the lone last path.
+// Terminal GBM (models 0, 1, 5), FP64 throughout like the reference's
+// make_bsm_terminal: S_T = spot exp(d0 + d1 z) with d0 = (r - q - vol^2/2) t
+// and d1 = vol sqrt(t) from the host, in that expression order (the down
+// path's d1 (-z) is -(d1 z) exactly, as in the reference).  Unit = quad of four
+// FP64 normals (two Philox calls).  Normal k serves pair k (antithetic) or
+// path k (plain); with an odd antithetic path count, normal n_pairs drives the
+// lone last path.
 // ----------------------------------------------------------------------------
 template <int UPT, bool ANTI>
 __device__ __forceinline__ void sim_terminal(const McOption& o, uint32_t unit0, uint32_t stride,
                                              uint32_t k0, uint32_t k1, Acc& acc) {
-    const float mu = o.p[0], sg = o.p[1];
+    const double d0 = o.d[0], d1 = o.d[1];
     const uint32_t n_pairs = (uint32_t)o.paths >> 1;
     const uint32_t n_norm = ANTI ? (uint32_t)(o.paths - (int32_t)n_pairs) : (uint32_t)o.paths;
     const bool odd = (o.paths & 1) != 0;
@@ -116,17 +120,18 @@ __device__ __forceinline__ void sim_terminal(const McOption& o, uint32_t unit0, 
     for (int k = 0; k < UPT; ++k) {
         const uint32_t unit = unit0 + (uint32_t)k * stride;
         if (unit * 4u >= n_norm) continue;
-        float z[4];
-        normals4(unit, 0u, ANTI ? 0u : 1u, k0, k1, z);
+        double z[4];
+        normals4_f64(unit, ANTI ? 0u : 1u, k0, k1, z);
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             const uint32_t idx = unit * 4u + (uint32_t)s;
             if (idx >= n_norm) break;
-            const double su = o.spot * exp((double)fma_rn(sg, z[s], mu));
+            const double dz = __dmul_rn(d1, z[s]);
+            const double su = o.spot * exp(__dadd_rn(d0, dz));
             const double a = payoff(su, o.strike, o.option_type);
             if (ANTI) {
                 if (idx < n_pairs) {
-                    const double sd = o.spot * exp((double)fma_rn(-sg, z[s], mu));
+                    const double sd = o.spot * exp(__dadd_rn(d0, -dz));
                     acc.add_pair(a, payoff(sd, o.strike, o.option_type));
                 } else if (odd) {
                     acc.add_lone(a);
@@ -357,9 +362,10 @@ __device__ __forceinline__ void sim_heston(const McOption& o, uint32_t unit0, ui
 // Terminal GBM with a variance-reduction estimator (models 8-12).  Unit = quad
 // of four consecutive paths 4u .. 4u+3; the path arithmetic is FP64 like the
 // reference's: S_T = spot exp(d0 + d1 z).
-//   control variates   z from the plain normal stream; sums of the payoff and
+//   control variates   z from the plain FP64 normal stream of the terminal
+//                      models (normals4_f64, c3 = 1); sums of the payoff and
 //                      of the centred control c = S_T - E[S_T]
-//   importance         z from the plain normal stream, y = z + shift,
+//   importance         z from the same FP64 normal stream, y = z + shift,
 //                      payoff(S_T(y)) exp(-shift y + shift^2 / 2)
 //   stratified         u = (i + U_i) / n with U_i uniform (Philox stream
 //                      c3 = 2), z = Acklam(u); q collects (y_2k - y_2k+1)^2 of
@@ -400,10 +406,7 @@ __device__ __forceinline__ void sim_vr(const McOption& o, uint32_t unit0, uint32
                 z[s] = acklam_inv(clamp_unit(u));
             }
         } else {
-            float zf[4];
-            normals4(unit, 0u, 1u, k0, k1, zf);
-#pragma unroll
-            for (int s = 0; s < 4; ++s) z[s] = (double)zf[s];
+            normals4_f64(unit, 1u, k0, k1, z);
         }
         double y[4];
 #pragma unroll

@@ -150,8 +150,9 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise) {
         const int32_t n_norm = o.antithetic ? paths - paths / 2 : paths;
         o.units = (int32_t)(((int64_t)n_norm + 3) / 4);
         o.samples = o.antithetic ? paths / 2 : paths;
-        o.p[0] = (float)((r - q - 0.5 * vol * vol) * t);
-        o.p[1] = (float)(vol * std::sqrt(smax(t, 0.0)));
+        // model_concepts.h:93-102, evaluated in the same order, kept in FP64
+        o.d[0] = (r - q - 0.5 * vol * vol) * t;
+        o.d[1] = vol * std::sqrt(smax(t, 0.0));
         return o;
     }
     if (m == kEuler || m == kMilstein || m == kLocalVol) {

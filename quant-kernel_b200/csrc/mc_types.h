@@ -36,8 +36,7 @@ enum : int32_t { kModeSimulate = 0, kModeConstant = 1 };
 // ---------------------------------------------------------------------------
 // Option record: 128 bytes, packed on the host, read once per tile.
 //
-// Model constants (FP32, rounded from FP64 host values):
-//   terminal (0,1,5):  p0 = (r - q - vol^2/2) t     p1 = vol sqrt(t)
+// Model constants of the stepwise models (FP32, rounded from FP64 host values):
 //   Euler/LV (2,4):    p0 = (r - q) dt               p1 = vol sqrt(dt)
 //                      p2 = 1e-12 / spot (floor of S/spot)
 //   Milstein (3):      p0 = (r - q) dt - c           p1 = vol sqrt(dt)
@@ -49,7 +48,8 @@ enum : int32_t { kModeSimulate = 0, kModeConstant = 1 };
 //                      p9 = log(1e-12 / spot) (floor of log(S/spot))
 //   Heston LR delta (7): the Heston constants; the record's weight_clip
 //                      bounds the first-step score z1 / (sqrt(v0) sqrt(dt) S0)
-// Variance-reduction models (8-12) keep FP64 constants in d[] (the same bytes):
+// The terminal models (0, 1, 5) and the variance-reduction models (8-12) keep
+// FP64 constants in d[] (the same bytes):
 //   d0 = (r - q - vol^2/2) t      d1 = vol sqrt(t)
 //   d2 = importance-sampling shift
 //   d3 = spot exp((r - q) t), the mean of S_T (control-variate centre)

@@ -60,14 +60,15 @@ void dfree(T*& p) {
 __global__ void init_params_kernel(float* P, uint64_t seed) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= SurLayout::total) return;
-    float z[4];
-    normals4(static_cast<uint32_t>(i), 0u, 7u, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32), z);
+    double z[4];
+    normals4_f64(static_cast<uint32_t>(i), 7u, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32), z);
+    const float z0 = static_cast<float>(z[0]);
     float v = 0.0f;
     if (i < SurLayout::b1) {
         const int col = (i - SurLayout::W1) % kSurInPad;
-        v = col < kSurIn ? z[0] * sqrtf(2.0f / kSurIn) : 0.0f;
+        v = col < kSurIn ? z0 * sqrtf(2.0f / kSurIn) : 0.0f;
     } else if ((i >= SurLayout::W2 && i < SurLayout::b2) || (i >= SurLayout::W3 && i < SurLayout::b3)) {
-        v = z[0] * sqrtf(2.0f / kSurHid);
+        v = z0 * sqrtf(2.0f / kSurHid);
     }
     P[i] = v;
 }

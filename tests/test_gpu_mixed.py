@@ -169,3 +169,45 @@ def test_autotuner_chooses_step_unrolling(qk):
     assert term.config()["step_unroll"] == 1
     for pl in (base, tuned, term):
         pl.close()
+
+
+def test_mixed_workload_at_full_size_vs_reference_cpu_mc(qk):
+    """The full uneven workload (4096 options, Euler / Milstein / local vol /
+    Heston, paths 2^12..2^20, steps 16..511) priced by the autotuned plan in a
+    CUDA graph, as the benchmark runs it; 256 of its options -- per model the
+    ones with the most steps, paths and path-steps (the corner where FP32 path
+    state drifts longest) and a seeded random rest -- against the reference's
+    own CPU Monte Carlo on the same inputs (tests/golden/mixed_reference.json,
+    produced by the oracle that equals the reference bit for bit):
+    z = difference / combined SE, per model and over the whole subset."""
+    import json
+    import sys
+    from pathlib import Path
+
+    from stat_check import check_z, z_scores
+
+    golden = Path(__file__).parent / "golden"
+    sys.path.insert(0, str(golden))
+    from make_mixed_reference import fingerprint
+
+    doc = json.loads((golden / "mixed_reference.json").read_text())
+    b = workloads.mixed()
+    idx = np.array(doc["index"])
+    assert fingerprint(b, idx) == doc["fingerprint"], "the mixed workload changed"
+    ref_p = np.array([float.fromhex(x) for x in doc["price"]])
+    ref_se = np.array([float.fromhex(x) for x in doc["stderr"]])
+    plan = qk.plan(**b, flags=QK_PLAN_AUTOTUNE | QK_PLAN_GRAPH)
+    plan.execute()
+    p, se = plan.results()
+    plan.close()
+    assert np.all(np.isfinite(p)) and np.all(se > 0)
+    z = z_scores(p[idx], ref_p, np.hypot(se[idx], ref_se))
+    models = b["model"][idx]
+    for m in np.unique(models):
+        check_z(z[models == m], f"mixed workload model {int(m)} GPU vs reference CPU MC")
+    check_z(z, "mixed workload (256 of 4096 options) GPU vs reference CPU MC")
+    # the corner: at least one option per model with >= 500 steps and one with
+    # >= 2^20 - 2^15 paths is in the checked set
+    for m in np.unique(models):
+        k = idx[models == m]
+        assert b["steps"][k].max() >= 500 and b["paths"][k].max() >= (1 << 20) - (1 << 15)

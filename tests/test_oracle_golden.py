@@ -224,18 +224,24 @@ def test_philox_published_known_answers(oracle):
 
 
 def test_philox_box_muller_layout(oracle):
+    """The terminal models' FP64 normals: a quad is two Philox calls (blocks
+    c1 and c1 + 1), each one Box-Muller pair with a 52-bit radius word
+    x0 << 20 | x1 >> 12 and a 52-bit angle word x2 << 20 | x3 >> 12."""
     seed = 0x123456789ABCDEF
     key = [seed & 0xFFFFFFFF, seed >> 32]
     for c0, c1, c3 in [(0, 0, 0), (5, 7, 0), (2**31, 99, 1)]:
-        x = _philox_py([c0, c1, 0, c3], key)
         z = oracle.philox_normals4(seed, c0, c1, c3)
         want = []
-        for a, b in ((x[0], x[1]), (x[2], x[3])):
-            u = ((a >> 9) + 0.5) * 2.0**-23
-            g = ((b >> 9) + 0.5) * 2.0**-22 - 1.0
+        for blk in (c1, c1 + 1):
+            x = _philox_py([c0, blk, 0, c3], key)
+            ub = (x[0] << 20) | (x[1] >> 12)
+            gb = (x[2] << 20) | (x[3] >> 12)
+            u = (ub + 0.5) * 2.0**-52
+            g = (gb + 0.5) * 2.0**-51 - 1.0
+            assert 0.0 < u < 1.0 and -1.0 < g < 1.0
             rad = math.sqrt(-2.0 * math.log(u))
             want += [rad * math.cos(math.pi * g), rad * math.sin(math.pi * g)]
-        assert np.allclose(z, want, rtol=0, atol=1e-14)
+        assert np.array_equal(z, want)
     # the replayed stream is standard normal
     zs = np.concatenate([oracle.philox_normals4(seed, i, 0, 0) for i in range(20000)])
     assert abs(zs.mean()) < 0.02 and abs(zs.var() - 1.0) < 0.02
@@ -283,36 +289,34 @@ def test_philox_replay_estimator_is_statistically_the_reference(oracle):
         assert abs(z) < 4.0, (model, a, b, z)
 
 
-def test_cpu_timer_calls_the_reference_batch(ref, tmp_path):
-    """The C++ timing harness behind the benchmark's CPU baseline calls the
-    reference's Heston batch entry point with the benchmark's inputs: its
-    prices sum to the Python binding's, bit for bit."""
-    import subprocess
-
+@pytest.mark.parametrize("model", ["heston", 0, 1, 2, 3, 4])
+def test_cpu_timer_calls_the_reference_batch(ref, model):
+    """The C++ timing harness behind the benchmark's CPU baselines calls the
+    reference's batch entry points (Heston, terminal, stepwise signatures)
+    with the benchmark's inputs: its prices sum to the Python binding's, bit
+    for bit."""
     from oracle import oracle as orc
 
-    timer = Path(__file__).resolve().parent.parent / "oracle" / "_ref" / "cpu_timer"
-    if not timer.exists():
+    if not orc.timer_available():
         pytest.skip("cpu_timer not built")
     rng = np.random.default_rng(3)
     n = 6
     b = dict(spot=np.full(n, 100.0), strike=rng.uniform(80, 120, n), t=rng.uniform(0.2, 2, n),
-             r=rng.uniform(0, 0.05, n), q=np.zeros(n), v0=rng.uniform(0.01, 0.09, n),
-             kappa=rng.uniform(0.5, 5, n), theta=rng.uniform(0.01, 0.09, n),
-             sigma=rng.uniform(0.1, 1, n), rho=rng.uniform(-0.9, 0, n),
-             option_type=(np.arange(n) % 2).astype(np.int32), paths=np.full(n, 500, np.int32),
-             steps=np.full(n, 20, np.int32), seed=np.arange(n, dtype=np.uint64) + 7)
-    f = tmp_path / "in.bin"
-    with open(f, "wb") as fh:
-        fh.write(np.int32(n).tobytes())
-        for k in ("spot", "strike", "t", "r", "q", "v0", "kappa", "theta", "sigma", "rho"):
-            fh.write(b[k].astype(np.float64).tobytes())
-        for k in ("option_type", "paths", "steps"):
-            fh.write(b[k].astype(np.int32).tobytes())
-        fh.write(b["seed"].astype(np.uint64).tobytes())
-    r = subprocess.run([str(timer), str(orc.REF_SO), "qk_mcm_heston_monte_carlo_price_batch",
-                        str(f), "2"], capture_output=True, text=True, check=True)
-    out = json.loads(r.stdout)
-    assert len(out["seconds"]) == 2 and all(s > 0 for s in out["seconds"])
-    want = float(np.sum(ref.heston_batch(**b)))
-    assert out["price_sum"] == want
+             vol=rng.uniform(0.1, 0.5, n), r=rng.uniform(0, 0.05, n), q=np.zeros(n),
+             v0=rng.uniform(0.01, 0.09, n), kappa=rng.uniform(0.5, 5, n),
+             theta=rng.uniform(0.01, 0.09, n), sigma=rng.uniform(0.1, 1, n),
+             rho=rng.uniform(-0.9, 0, n), option_type=(np.arange(n) % 2).astype(np.int32),
+             paths=np.full(n, 500, np.int32), steps=np.full(n, 20, np.int32),
+             seed=np.arange(n, dtype=np.uint64) + 7)
+    if model == "heston":
+        symbol = "qk_mcm_heston_monte_carlo_price_batch"
+        want = float(np.sum(ref.heston_batch(**{k: v for k, v in b.items() if k != "vol"})))
+    else:
+        symbol = orc.MODEL_BATCH_SYMBOL[model]
+        want = float(np.sum([ref.price(model, b["spot"][i], b["strike"][i], b["t"][i], b["vol"][i],
+                                       b["r"][i], b["q"][i], int(b["option_type"][i]),
+                                       int(b["paths"][i]), int(b["steps"][i]), int(b["seed"][i]))
+                             for i in range(n)]))
+    secs, price_sum = orc.time_reference_batch(symbol, b, reps=2)
+    assert len(secs) == 2 and all(s > 0 for s in secs)
+    assert price_sum == want
