@@ -551,17 +551,6 @@ __device__ __forceinline__ void run_tile(const McOption& o, int64_t tile, TilePa
     reduce_tile<BLOCK, FAMILY == kFamVr>(acc, partials + tile, smem);
 }
 
-// Each model family's tile as a separate call from the persistent kernel:
-// every body is register-allocated and scheduled on its own, as in the
-// single-family kernels, instead of sharing one allocation across all paths
-// of the dispatch (measured: the inlined form ran the Heston and Milstein
-// tiles 4-6% slower than their own kernels).
-template <int FAMILY, int BLOCK, int UPT, bool ANTI>
-__device__ __noinline__ void run_tile_call(const McOption& o, int64_t tile, TilePartial* partials,
-                                           DD* smem) {
-    run_tile<FAMILY, BLOCK, UPT, ANTI>(o, tile, partials, smem);
-}
-
 // ----------------------------------------------------------------------------
 // Kernel 1a: single-family simulate, grid-stride over tiles [tile0, tile0 +
 // n_tiles) of the options opts[0, n).
@@ -585,76 +574,110 @@ __global__ void __launch_bounds__(BLOCK)
 // ----------------------------------------------------------------------------
 // Kernel 1b: persistent work-stealing simulate for mixed batches.  One CTA per
 // resident slot; each CTA takes the next tile from a global counter until the
-// list is exhausted, then dispatches on the tile's model.  The next tile is
-// claimed when the current one starts and its index is only read when the
-// current one ends, so the atomic's round trip overlaps the simulation.  The
-// counter is reset by the finalize kernel of the same execute, so a captured
-// graph can replay without a memset.  The counter only grows: all CTAs
-// together claim at most n_tiles + 2 * gridDim.x indices, so every loop ends.
+// list is exhausted.  The records are in work order, in runs ("groups") of one
+// (family, antithetic) pair, so consecutive claims mostly fall in one group:
+// a CTA enters a group's loop once -- one call of that family's code, compiled
+// and register-allocated on its own -- and keeps claiming and simulating
+// tiles inside it until a claim lands past the group, with the owning record
+// found by a forward search from the previous one (claims only grow).  The
+// next tile is claimed when the current one starts and its index is only read
+// when the current one ends, so the atomic's round trip overlaps the
+// simulation.  The counter is reset by the finalize kernel of the same
+// execute, so a captured graph can replay without a memset.  The counter only
+// grows: all CTAs together claim at most n_tiles + gridDim.x indices, so every
+// loop ends.
 // ----------------------------------------------------------------------------
+
+// Last record i in [lo, hi) with tile_begin[i] <= tile, given tile_begin[lo] <=
+// tile and tile_begin non-decreasing: gallop forward, then bisect.
+__device__ __forceinline__ int32_t advance_option(const int64_t* __restrict__ tile_begin,
+                                                  int32_t lo, int32_t hi, int64_t tile) {
+    int32_t step = 1;
+    while (lo + step < hi && __ldg(tile_begin + lo + step) <= tile) {
+        lo += step;
+        step <<= 1;
+    }
+    int32_t top = (lo + step < hi ? lo + step : hi) - 1;
+    while (lo < top) {
+        const int32_t mid = (lo + top + 1) >> 1;
+        if (__ldg(tile_begin + mid) <= tile)
+            lo = mid;
+        else
+            top = mid - 1;
+    }
+    return lo;
+}
+
+// Tiles of one group, from `tile` (claimed, inside the group) until a claim
+// lands past the group; returns that claim.
+template <int FAMILY, int BLOCK, int UPT, bool ANTI>
+__device__ __noinline__ int64_t run_group(const McOption* __restrict__ opts,
+                                          const int64_t* __restrict__ tile_begin, int32_t opt_lo,
+                                          int32_t opt_hi, int64_t tile_hi,
+                                          TilePartial* __restrict__ partials,
+                                          unsigned long long* __restrict__ work_counter, DD* smem,
+                                          long long* s_tile, int64_t tile) {
+    int32_t oi = advance_option(tile_begin, opt_lo, opt_hi, tile);
+    McOption o = opts[oi];
+    for (;;) {
+        // claim the next tile now; thread 0 first uses the result below
+        long long next = 0;
+        if (threadIdx.x == 0) next = (long long)atomicAdd(work_counter, 1ull);
+        run_tile<FAMILY, BLOCK, UPT, ANTI>(o, tile, partials, smem);  // ends in a CTA barrier
+        if (threadIdx.x == 0) *s_tile = next;
+        __syncthreads();
+        // every thread reads s_tile here, and the next write to it follows the
+        // barrier at the end of the next tile
+        tile = *s_tile;
+        if (tile >= tile_hi) return tile;
+        if (tile >= o.tile_begin + o.tiles) {
+            oi = advance_option(tile_begin, oi + 1, opt_hi, tile);
+            o = opts[oi];
+        }
+    }
+}
+
 template <int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
     mc_persistent_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
-                         int32_t n, int64_t n_tiles, TilePartial* __restrict__ partials,
-                         unsigned long long* __restrict__ work_counter) {
+                         int64_t n_tiles, TilePartial* __restrict__ partials,
+                         unsigned long long* __restrict__ work_counter,
+                         const GroupTable* __restrict__ groups) {
     __shared__ DD smem[5 * (BLOCK / 32)];
     __shared__ long long s_tile;
     if (threadIdx.x == 0) s_tile = (long long)atomicAdd(work_counter, 1ull);
     __syncthreads();
     int64_t tile = s_tile;
-    for (;;) {
-        __syncthreads();  // everyone has read s_tile before it is rewritten
-        if (tile >= n_tiles) break;
-        // claim the next tile now; thread 0 first uses the result below
-        long long next = 0;
-        if (threadIdx.x == 0) next = (long long)atomicAdd(work_counter, 1ull);
-        const int32_t oi = find_option(tile_begin, n, tile);
-        const McOption o = opts[oi];
-        const bool anti = o.antithetic != 0;
-        switch (o.model) {
-            case kStandard:
-            case kAntithetic:
-                run_tile_call<kFamTerminal, BLOCK, kUptTerminal, true>(o, tile, partials, smem);
-                break;
-            case kTerminalPlain:
-                run_tile_call<kFamTerminal, BLOCK, kUptTerminal, false>(o, tile, partials, smem);
-                break;
-            case kEuler:
-            case kLocalVol:
-                if (anti)
-                    run_tile_call<kFamEuler, BLOCK, kUptStepwise, true>(o, tile, partials, smem);
-                else
-                    run_tile_call<kFamEuler, BLOCK, kUptStepwise, false>(o, tile, partials, smem);
-                break;
-            case kMilstein:
-                if (anti)
-                    run_tile_call<kFamMilstein, BLOCK, kUptStepwise, true>(o, tile, partials, smem);
-                else
-                    run_tile_call<kFamMilstein, BLOCK, kUptStepwise, false>(o, tile, partials, smem);
-                break;
-            case kControlVariates:
-            case kImportanceSampling:
-            case kStratified:
-            case kQmcSobol:
-            case kQmcHalton:
-                run_tile_call<kFamVr, BLOCK, kUptVr, false>(o, tile, partials, smem);
-                break;
-            case kHestonLrDelta:
-                if (anti)
-                    run_tile_call<kFamHestonLr, BLOCK, kUptHeston, true>(o, tile, partials, smem);
-                else
-                    run_tile_call<kFamHestonLr, BLOCK, kUptHeston, false>(o, tile, partials, smem);
-                break;
-            default:  // kHeston
-                if (anti)
-                    run_tile_call<kFamHeston, BLOCK, kUptHeston, true>(o, tile, partials, smem);
-                else
-                    run_tile_call<kFamHeston, BLOCK, kUptHeston, false>(o, tile, partials, smem);
+    const int32_t count = groups->count;
+    int32_t g = 0;
+    while (tile < n_tiles) {
+        // claims only grow, so the group index only moves forward
+        while (g < count && tile >= groups->tile_hi[g]) ++g;
+        if (g >= count) break;  // the groups cover every tile; defensive
+        const int32_t lo = groups->opt_lo[g], hi = groups->opt_hi[g];
+        const int64_t th = groups->tile_hi[g];
+        switch (groups->code[g]) {
+#define QK_GROUP(FAM, UPT, ANTI)                                                                  \
+    case FAM * 2 + (ANTI ? 1 : 0):                                                               \
+        tile = run_group<FAM, BLOCK, UPT, ANTI>(opts, tile_begin, lo, hi, th, partials,          \
+                                                work_counter, smem, &s_tile, tile);              \
+        break;
+            QK_GROUP(kFamTerminal, kUptTerminal, true)
+            QK_GROUP(kFamTerminal, kUptTerminal, false)
+            QK_GROUP(kFamEuler, kUptStepwise, true)
+            QK_GROUP(kFamEuler, kUptStepwise, false)
+            QK_GROUP(kFamMilstein, kUptStepwise, true)
+            QK_GROUP(kFamMilstein, kUptStepwise, false)
+            QK_GROUP(kFamHeston, kUptHeston, true)
+            QK_GROUP(kFamHeston, kUptHeston, false)
+            QK_GROUP(kFamHestonLr, kUptHeston, true)
+            QK_GROUP(kFamHestonLr, kUptHeston, false)
+            QK_GROUP(kFamVr, kUptVr, false)
+#undef QK_GROUP
+            default:
+                tile = n_tiles;  // unknown code: the host never builds one
                 break;
         }
-        if (threadIdx.x == 0) s_tile = next;
-        __syncthreads();
-        tile = s_tile;
     }
 }
 
@@ -832,17 +855,17 @@ cudaError_t launch_simulate(int family, bool anti, int block, int upt, int su, c
     }
 }
 
-cudaError_t launch_persistent(int block, const SimArgs& a, unsigned long long* work_counter,
-                              cudaStream_t st) {
+cudaError_t launch_persistent(int block, const SimArgs& a, const GroupTable* groups,
+                              unsigned long long* work_counter, cudaStream_t st) {
     if (a.n_tiles <= 0) return cudaSuccess;
     const int64_t cap = (int64_t)a.max_ctas;
     const unsigned grid = (unsigned)(a.n_tiles < cap ? a.n_tiles : cap);
     if (block == 128)
-        mc_persistent_kernel<128><<<grid, 128, 0, st>>>(a.opts, a.tile_begin, a.n, a.n_tiles,
-                                                        a.partials, work_counter);
+        mc_persistent_kernel<128><<<grid, 128, 0, st>>>(a.opts, a.tile_begin, a.n_tiles,
+                                                        a.partials, work_counter, groups);
     else if (block == 256)
-        mc_persistent_kernel<256><<<grid, 256, 0, st>>>(a.opts, a.tile_begin, a.n, a.n_tiles,
-                                                        a.partials, work_counter);
+        mc_persistent_kernel<256><<<grid, 256, 0, st>>>(a.opts, a.tile_begin, a.n_tiles,
+                                                        a.partials, work_counter, groups);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();

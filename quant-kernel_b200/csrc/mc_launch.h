@@ -41,14 +41,28 @@ struct SimArgs {
     int64_t tile0 = 0;         // absolute index of this launch's first tile
 };
 
+// The persistent kernel's view of a plan's work order: runs of consecutive
+// records of one (family, antithetic) pair.  Group g holds records
+// [opt_lo, opt_hi) and tiles [tile_hi of g - 1 (0 for g = 0), tile_hi); every
+// record of a group has at least one tile, and the groups cover all tiles.
+constexpr int kMaxGroups = 16;
+struct GroupTable {
+    int32_t count;
+    int32_t code[kMaxGroups];  // family * 2 + antithetic
+    int32_t opt_lo[kMaxGroups];
+    int32_t opt_hi[kMaxGroups];
+    int64_t tile_hi[kMaxGroups];
+};
+
 int family_of(int32_t model);
 
 // su: step blocks per loop iteration of the stepwise families (1 or 2; 2 only
 // with upt 1 or 2); other families take 1.
 cudaError_t launch_simulate(int family, bool anti, int block, int upt, int su, const SimArgs& a,
                             cudaStream_t st);
-cudaError_t launch_persistent(int block, const SimArgs& a, unsigned long long* work_counter,
-                              cudaStream_t st);
+// groups: device copy of the plan's GroupTable.
+cudaError_t launch_persistent(int block, const SimArgs& a, const GroupTable* groups,
+                              unsigned long long* work_counter, cudaStream_t st);
 // out_index (nullable): record k's results go to slot out_index[k].
 cudaError_t launch_finalize(const McOption* opts, int32_t n, const TilePartial* partials,
                             double* out_price, double* out_se, const int32_t* out_index,

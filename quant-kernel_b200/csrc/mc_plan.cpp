@@ -414,6 +414,8 @@ cudaError_t Plan::release() {
         d_counter_.release();
         d_out_index_.release();
         h_out_index_.release();
+        d_groups_.release();
+        h_groups_.release();
         h_opts_.release();
         h_tile_begin_.release();
         h_price_.release();
@@ -592,6 +594,8 @@ cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
     if (persistent_) {
         if ((e = d_out_index_.ensure(ix_bytes)) != cudaSuccess) return e;
         if ((e = h_out_index_.ensure(ix_bytes)) != cudaSuccess) return e;
+        if ((e = d_groups_.ensure(sizeof(GroupTable))) != cudaSuccess) return e;
+        if ((e = h_groups_.ensure(sizeof(GroupTable))) != cudaSuccess) return e;
     }
     // The previous upload from these staging buffers may still be in flight.
     if ((e = cudaStreamSynchronize(stream_)) != cudaSuccess) return e;
@@ -601,6 +605,21 @@ cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
     if (persistent_) {
         std::memcpy(h_out_index_.p, order_.data(), sizeof(int32_t) * (size_t)n);
         if ((e = cudaMemcpyAsync(d_out_index_.p, h_out_index_.p, sizeof(int32_t) * (size_t)n,
+                                 cudaMemcpyHostToDevice, stream_)) != cudaSuccess)
+            return e;
+        // the persistent kernel's group table (at most 2 groups per family:
+        // antithetic and plain; constant records carry no tiles)
+        GroupTable* gt = static_cast<GroupTable*>(h_groups_.p);
+        std::memset(gt, 0, sizeof(GroupTable));
+        if (groups_.size() > (size_t)kMaxGroups) return cudaErrorInvalidConfiguration;
+        gt->count = (int32_t)groups_.size();
+        for (size_t k = 0; k < groups_.size(); ++k) {
+            gt->code[k] = groups_[k].family * 2 + (groups_[k].anti ? 1 : 0);
+            gt->opt_lo[k] = groups_[k].opt_lo;
+            gt->opt_hi[k] = groups_[k].opt_hi;
+            gt->tile_hi[k] = groups_[k].tile_hi;
+        }
+        if ((e = cudaMemcpyAsync(d_groups_.p, h_groups_.p, sizeof(GroupTable),
                                  cudaMemcpyHostToDevice, stream_)) != cudaSuccess)
             return e;
     }
@@ -633,7 +652,8 @@ cudaError_t Plan::launch_all(cudaStream_t st, bool timing) {
     const bool use_counter = persistent_ && cfg_.upt == kUptPersistent;
     if (n_tiles_ > 0) {
         if (use_counter) {
-            e = launch_persistent(cfg_.block, a, counter, st);
+            e = launch_persistent(cfg_.block, a, static_cast<const GroupTable*>(d_groups_.p),
+                                  counter, st);
         } else if (persistent_) {
             // one grid per (family, antithetic) group, back to back
             for (const Group& g : groups_) {

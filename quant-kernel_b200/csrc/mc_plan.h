@@ -130,8 +130,9 @@ private:
         int64_t tile_lo, tile_hi;
     };
     std::vector<Group> groups_;        // filled for multi-family plans
-    DevBuf d_opts_, d_tile_begin_, d_partials_, d_price_, d_se_, d_counter_, d_out_index_;
-    PinnedBuf h_opts_, h_tile_begin_, h_price_, h_se_, h_out_index_;
+    DevBuf d_opts_, d_tile_begin_, d_partials_, d_price_, d_se_, d_counter_, d_out_index_,
+        d_groups_;
+    PinnedBuf h_opts_, h_tile_begin_, h_price_, h_se_, h_out_index_, h_groups_;
     cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
     cudaGraph_t graph_ = nullptr;
     cudaGraphExec_t graph_exec_ = nullptr;

@@ -200,7 +200,9 @@ def test_mixed_workload_at_full_size_vs_reference_cpu_mc(qk):
     plan.execute()
     p, se = plan.results()
     plan.close()
-    assert np.all(np.isfinite(p)) and np.all(se > 0)
+    # a deep out-of-the-money option may pay nothing on every path (SE 0);
+    # z_scores then requires both sides to be exactly 0
+    assert np.all(np.isfinite(p)) and np.all(se >= 0)
     z = z_scores(p[idx], ref_p, np.hypot(se[idx], ref_se))
     models = b["model"][idx]
     for m in np.unique(models):
