@@ -483,6 +483,11 @@ def main_gpu(args):
 
     qk = QuantKernel()
     qk.set_device(local)
+    # one batch split across all ranks (run first, while every rank still
+    # builds plans at the default launch shape: the ranks' tilings must agree)
+    strong = None
+    if not args.profile:
+        strong = sharded_leg(qk, world, rank, dev, args.steps, args.warmup)
     n_opt = args.options
     h = workloads.heston(n_opt, paths=PATHS, steps=STEPS, seed=2 + 1000 * rank,
                          seed_base=5000 + 10_000_000 * rank)
@@ -639,10 +644,74 @@ def main_gpu(args):
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clk,
+        "strong_scaling": strong,
         **extras,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def sharded_leg(qk, world, rank, dev, steps, warmup):
+    """Strong scaling through the library's own multi-GPU path: the same
+    1024-option Heston batch on every rank, each rank simulating its share of
+    the tiles (qk_mcm_plan_execute_sharded: NCCL exchange of the tile sums,
+    finalize on every rank).  Timed with CUDA events, max over ranks; at one
+    GPU the results are checked against a plain execute bit for bit."""
+    import torch
+    import torch.distributed as dist
+
+    from quantkernel_b200 import QK_MC_HESTON, workloads
+    from quantkernel_b200.sharding import DistContext, new_id
+
+    ident = new_id(qk) if rank == 0 else None
+    if world > 1:
+        obj = [ident]
+        dist.broadcast_object_list(obj, src=0)
+        ident = obj[0]
+    ctx = DistContext(ident, world, rank, qk)
+    h = workloads.heston(N_OPT, paths=PATHS, steps=STEPS)
+    plan = qk.plan(model=np.full(N_OPT, QK_MC_HESTON, np.int32), **h)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(warmup):
+        flush.zero_()
+        ctx.execute(plan, stream.cuda_stream)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        flush.zero_()
+        ctx.execute(plan, stream.cuda_stream)
+    e1.record(stream)
+    barrier()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item()) / steps
+    p, se = plan.results()
+    same = None
+    if world == 1:
+        plan.execute()
+        p1, se1 = plan.results()
+        same = bool(np.array_equal(p, p1) and np.array_equal(se, se1))
+        assert same, "sharded execute differs from execute"
+    bounds = plan.shard_bounds(world)
+    plan.close()
+    ctx.close()
+    units = N_OPT * PATHS * STEPS
+    return {"workload": WORKLOAD + " (one batch for all ranks)", "n_gpus": world,
+            "value": units / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "scaling": "strong",
+            "api": "qk_mcm_plan_execute_sharded (NCCL broadcast of tile sums, finalize on every "
+                   "rank)",
+            "tiles_per_rank": [int(b) for b in np.diff(bounds)],
+            "equals_single_gpu_bitwise": same,
+            "l2": "flushed between steps"}
 
 
 # --------------------------------------------------------------------------- surrogate

@@ -378,6 +378,72 @@ QK_EXPORT int32_t qk_mcm_plan_config(qk_mc_plan* plan, int32_t* block, int32_t* 
 QK_EXPORT int32_t qk_mcm_plan_step_unroll(qk_mc_plan* plan, int32_t* step_unroll);
 QK_EXPORT int32_t qk_mcm_plan_destroy(qk_mc_plan* plan);
 
+/* ----------------------------------------------------------------------- *
+ * One batch across several GPUs (ABI 2.13, no counterpart in the reference,
+ * which prices a batch with OpenMP threads on one host).  One rank per GPU
+ * (a process or a thread each); every rank builds the same plan from the
+ * same inputs.  A sharded execute simulates this rank's contiguous range of
+ * the plan's tiles (balanced by path-steps), exchanges every rank's tile
+ * sums over NCCL (one grouped broadcast step) and finalizes all options on
+ * every rank, so results() gives the whole batch, bit for bit what a
+ * single-GPU execute gives.  NCCL is loaded at run time (libnccl.so.2, or the
+ * path in QK_B200_NCCL_PATH); without it these calls return
+ * QK_ERR_RUNTIME_INIT ("nccl unavailable: ...").  The collective blocks
+ * until every rank has joined it: a rank that never joins holds the others
+ * until qk_dist_abort() is called on them (from another thread) or they are
+ * stopped.
+ * ----------------------------------------------------------------------- */
+#define QK_DIST_ID_BYTES 128
+typedef struct qk_dist qk_dist;
+
+/* A new communicator id (QK_DIST_ID_BYTES bytes), made once on one rank and
+ * handed to every rank (file, socket, the launcher's own store). */
+QK_EXPORT int32_t qk_dist_unique_id(uint8_t* out_id);
+/* Joins rank `rank` of `world` on the calling thread's current device
+ * (qk_set_device first).  All ranks must call it with the same id. */
+QK_EXPORT int32_t qk_dist_create(const uint8_t* id, int32_t world, int32_t rank, qk_dist** out);
+QK_EXPORT int32_t qk_dist_info(const qk_dist* dist, int32_t* world, int32_t* rank,
+                               int32_t* device);
+/* Ends the communicator's pending and future collectives with an error. */
+QK_EXPORT int32_t qk_dist_abort(qk_dist* dist);
+QK_EXPORT int32_t qk_dist_destroy(qk_dist* dist);
+/* The partition rule of the sharded execute, on any list of costs: bounds
+ * (world + 1 entries) of contiguous ranges with near-equal total cost;
+ * bounds[r] is the item boundary whose cumulative cost is nearest r/world of
+ * the total (ties: the earlier one).  Host only (no GPU, no NCCL). */
+QK_EXPORT int32_t qk_dist_partition(const double* cost, int64_t n, int32_t world,
+                                    int64_t* bounds);
+/* This rank's share of a plan on `stream` (NULL: the plan's stream), then
+ * qk_mcm_plan_results() as after qk_mcm_plan_execute().  The plan must live
+ * on the communicator's device, and every rank's plan must have the same
+ * tiling: same inputs, flags and launch shape (a shape chosen by
+ * QK_PLAN_AUTOTUNE, or cached from another plan's tuning, can differ between
+ * ranks).  Each call first max-reduces a fingerprint of the tiling over the
+ * ranks (one small collective and a wait for it) and returns
+ * QK_ERR_INVALID_INPUT on every rank when they differ. */
+QK_EXPORT int32_t qk_mcm_plan_execute_sharded(qk_mc_plan* plan, qk_dist* dist, void* stream);
+/* The pieces of a sharded execute, for callers that move the tile sums with
+ * their own transport: the partition (world + 1 tile bounds, host only), the
+ * simulate kernels over tiles [tile_begin, tile_end) only, the plan's device
+ * array of per-tile sums (n_tiles records of bytes_per_tile bytes, indexed by
+ * tile), and the finalize kernel over every option (after every tile's sums
+ * are in place).  execute_tiles over each range of the partition, in any
+ * order, then finalize, gives what execute() gives. */
+QK_EXPORT int32_t qk_mcm_plan_shard_bounds(qk_mc_plan* plan, int32_t world, int64_t* bounds);
+QK_EXPORT int32_t qk_mcm_plan_execute_tiles(qk_mc_plan* plan, int64_t tile_begin,
+                                            int64_t tile_end, void* stream);
+QK_EXPORT int32_t qk_mcm_plan_device_partials(qk_mc_plan* plan, void** d_partials,
+                                              int64_t* n_tiles, int32_t* bytes_per_tile);
+QK_EXPORT int32_t qk_mcm_plan_finalize(qk_mc_plan* plan, void* stream);
+/* qk_mcm_mixed_price_batch across the ranks of `dist`: every rank passes the
+ * whole batch and receives every result (equal to the single-GPU call's). */
+QK_EXPORT int32_t qk_mcm_mixed_price_batch_sharded(
+    qk_dist* dist, const int32_t* model, const double* spot, const double* strike,
+    const double* t, const double* vol, const double* r, const double* q, const double* v0,
+    const double* kappa, const double* theta, const double* sigma, const double* rho,
+    const int32_t* option_type, const int32_t* paths, const int32_t* steps,
+    const uint64_t* seed, int32_t n, double* out_prices, double* out_stderr);
+
 /* ======================================================================= *
  * Part 3 -- Heston surrogate (ABI 2.13, no counterpart in the reference)
  * ======================================================================= */

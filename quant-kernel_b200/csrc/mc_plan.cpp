@@ -532,6 +532,8 @@ static int family_rank(int fam) {
 
 cudaError_t Plan::layout_tiles(const LaunchConfig& cfg) {
     const int32_t n = n_;
+    shard_world_ = 0;  // the tile geometry may change: partitions are stale
+    shard_bounds_.clear();
     // tile geometry per option (independent of the order)
     for (int32_t i = 0; i < n; ++i) {
         McOption& o = opts_[(size_t)i];
@@ -680,6 +682,106 @@ cudaError_t Plan::launch_all(cudaStream_t st, bool timing) {
                            use_counter ? counter : nullptr, st);
 }
 
+void partition_by_cost(const double* cost, int64_t n, int world, int64_t* bounds) {
+    bounds[0] = 0;
+    if (world <= 1 || n <= 0) {
+        for (int r = 1; r <= world; ++r) bounds[r] = n > 0 ? n : 0;
+        return;
+    }
+    double total = 0.0;
+    for (int64_t i = 0; i < n; ++i) total += cost[i];
+    int r = 1;
+    double before = 0.0;  // cost of items [0, i)
+    for (int64_t i = 0; i < n && r < world; ++i) {
+        const double after = before + cost[i];
+        // every target that item i reaches: cut before or after it, whichever
+        // cumulative cost is nearer the target
+        while (r < world && after >= total * (double)r / (double)world) {
+            const double target = total * (double)r / (double)world;
+            const int64_t cut = (target - before <= after - target) ? i : i + 1;
+            bounds[r] = std::max(cut, bounds[r - 1]);
+            ++r;
+        }
+        before = after;
+    }
+    for (; r < world; ++r) bounds[r] = n;
+    bounds[world] = n;
+}
+
+const std::vector<int64_t>& Plan::shard_bounds(int world) {
+    if (shard_world_ == world && (int)shard_bounds_.size() == world + 1) return shard_bounds_;
+    // path-steps of every tile, in work order (the last tile of an option
+    // holds the remainder of its units)
+    std::vector<double> cost((size_t)std::max<int64_t>(n_tiles_, 0));
+    for (int32_t k = 0; k < n_; ++k) {
+        const McOption& o = opts_[(size_t)order_[(size_t)k]];
+        if (o.tiles <= 0) continue;
+        const int64_t per_tile = (int64_t)cfg_.block *
+                                 upt_for(family_of(o.model), persistent_, cfg_) * o.unit_iters;
+        const double steps = (double)std::max(o.steps, 1);
+        for (int32_t t = 0; t < o.tiles; ++t) {
+            const int64_t left = (int64_t)o.units - (int64_t)t * per_tile;
+            cost[(size_t)(o.tile_begin + t)] = (double)std::min(per_tile, left) * steps;
+        }
+    }
+    shard_bounds_.assign((size_t)world + 1, 0);
+    partition_by_cost(cost.data(), n_tiles_, world, shard_bounds_.data());
+    shard_world_ = world;
+    return shard_bounds_;
+}
+
+cudaError_t Plan::order_after_upload(cudaStream_t st) {
+    if (!st || st == stream_) return cudaSuccess;
+    cudaEvent_t ready;
+    cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+    e = cudaEventRecord(ready, stream_);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ready, 0);
+    cudaEventDestroy(ready);
+    return e;
+}
+
+cudaError_t Plan::launch_tiles(cudaStream_t st, int64_t lo, int64_t hi, bool timing) {
+    if (cudaError_t fe = injected_fault(kFaultLaunch)) return fe;
+    SimArgs a;
+    a.opts = static_cast<const McOption*>(d_opts_.p);
+    a.tile_begin = static_cast<const int64_t*>(d_tile_begin_.p);
+    a.n = n_;
+    a.partials = static_cast<TilePartial*>(d_partials_.p);
+    a.max_ctas = std::numeric_limits<int32_t>::max();
+    cudaError_t e = cudaSuccess;
+    if (timing && (e = cudaEventRecord(ev0_, st)) != cudaSuccess) return e;
+    if (!persistent_) {
+        a.tile0 = lo;
+        a.n_tiles = hi - lo;
+        if (a.n_tiles > 0) e = launch_simulate(family_, anti_, cfg_.block, cfg_.upt, cfg_.su, a, st);
+    } else {
+        for (const Group& g : groups_) {
+            const int64_t t0 = std::max(lo, g.tile_lo), t1 = std::min(hi, g.tile_hi);
+            if (t1 <= t0) continue;
+            SimArgs ga = a;
+            ga.opts = a.opts + g.opt_lo;
+            ga.tile_begin = a.tile_begin + g.opt_lo;
+            ga.n = g.opt_hi - g.opt_lo;
+            ga.tile0 = t0;
+            ga.n_tiles = t1 - t0;
+            e = launch_simulate(g.family, g.anti, cfg_.block, upt_for(g.family, true, cfg_), 1, ga,
+                                st);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    if (e != cudaSuccess) return e;
+    if (timing && (e = cudaEventRecord(ev1_, st)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+cudaError_t Plan::launch_finalize_all(cudaStream_t st) {
+    const int32_t* out_index = persistent_ ? static_cast<const int32_t*>(d_out_index_.p) : nullptr;
+    return launch_finalize(static_cast<const McOption*>(d_opts_.p), n_,
+                           static_cast<const TilePartial*>(d_partials_.p), d_price(), d_se(),
+                           out_index, nullptr, st);
+}
+
 cudaError_t Plan::capture_graph() {
     drop_graph();
     cudaError_t e = cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal);
@@ -696,15 +798,8 @@ cudaError_t Plan::execute(cudaStream_t stream) {
     if (device_ < 0) return cudaErrorInvalidResourceHandle;
     DeviceGuard g(device_);
     cudaStream_t st = stream ? stream : stream_;
-    if (stream && stream != stream_) {
-        // Order this execute after the plan's own uploads.
-        cudaEvent_t ready;
-        cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
-        if (e != cudaSuccess) return e;
-        cudaEventRecord(ready, stream_);
-        cudaStreamWaitEvent(st, ready, 0);
-        cudaEventDestroy(ready);
-    }
+    // order this execute after the plan's own uploads
+    if (cudaError_t oe = order_after_upload(st)) return oe;
     const bool timing = (flags_ & kFlagTiming) != 0;
     cudaError_t e;
     if (flags_ & kFlagGraph) {

@@ -97,6 +97,22 @@ public:
     double* d_price() const { return static_cast<double*>(d_price_.p); }
     double* d_se() const { return static_cast<double*>(d_se_.p); }
     int device() const { return device_; }
+    TilePartial* d_partials() const { return static_cast<TilePartial*>(d_partials_.p); }
+    cudaStream_t stream() const { return stream_; }
+
+    // ---- one rank's share of a batch priced on several GPUs ----
+    // Tile bounds b[0..world] of a contiguous partition of the plan's tiles
+    // (work order) balanced by path-steps: rank k simulates [b[k], b[k+1]).
+    // The same plan on every rank gives the same bounds.
+    const std::vector<int64_t>& shard_bounds(int world);
+    // Orders work on `st` after the plan's own uploads (no-op on its stream).
+    cudaError_t order_after_upload(cudaStream_t st);
+    // The simulate kernels over tiles [lo, hi) only (per-family grids).
+    cudaError_t launch_tiles(cudaStream_t st, int64_t lo, int64_t hi, bool timing);
+    // The finalize kernel over every option (results in the caller's order).
+    cudaError_t launch_finalize_all(cudaStream_t st);
+    // The stream results() waits on.
+    void note_stream(cudaStream_t st) { last_stream_ = st; }
 
 private:
     cudaError_t ensure_stream();
@@ -130,6 +146,8 @@ private:
         int64_t tile_lo, tile_hi;
     };
     std::vector<Group> groups_;        // filled for multi-family plans
+    std::vector<int64_t> shard_bounds_;  // cached partition (shard_world_ ranks)
+    int shard_world_ = 0;
     DevBuf d_opts_, d_tile_begin_, d_partials_, d_price_, d_se_, d_counter_, d_out_index_,
         d_groups_;
     PinnedBuf h_opts_, h_tile_begin_, h_price_, h_se_, h_out_index_, h_groups_;
@@ -143,6 +161,12 @@ McOption pack_option(const BatchInput& in, int32_t i, bool anti_stepwise);
 // Fills o.tiles / o.unit_iters for a launch of `block` threads with `upt`
 // units each; returns o.tiles.
 int32_t tile_option(McOption& o, int block, int upt);
+
+// Contiguous partition of n items with the given costs into `world` ranges
+// of near-equal total cost: bounds[0] = 0, bounds[world] = n, and bounds[r]
+// is the item boundary whose cumulative cost is nearest r/world of the total
+// (ties: the earlier boundary; never below bounds[r - 1]).  Host only.
+void partition_by_cost(const double* cost, int64_t n, int world, int64_t* bounds);
 
 // Per-thread, per-device scratch plan used by the one-shot batch calls.
 Plan* thread_scratch_plan(int device);

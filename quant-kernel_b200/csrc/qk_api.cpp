@@ -18,8 +18,9 @@
 
 #include "cf_kernels.h"
 #include "mc_noalloc.h"
+#include "qk_dist.h"
 #include "qk_error.h"
-#include "mc_plan.h"
+#include "qk_handles.h"
 
 namespace {
 
@@ -261,9 +262,6 @@ int32_t mixed_input(const int32_t* model, const double* spot, const double* stri
 
 }  // namespace
 
-struct qk_mc_plan {
-    qkb::Plan plan;
-};
 
 extern "C" {
 
@@ -701,6 +699,92 @@ int32_t qk_mcm_mixed_price_batch(const int32_t* model, const double* spot, const
     if (rc != QK_OK) return rc;
     if (!out_prices) return fail_null("out_prices");
     return run_batch(in, qkb::kFlagPersistent, out_prices, out_stderr, "qk_mcm_mixed_price_batch");
+}
+
+int32_t qk_mcm_mixed_price_batch_sharded(qk_dist* dist, const int32_t* model, const double* spot,
+                                         const double* strike, const double* t, const double* vol,
+                                         const double* r, const double* q, const double* v0,
+                                         const double* kappa, const double* theta,
+                                         const double* sigma, const double* rho,
+                                         const int32_t* option_type, const int32_t* paths,
+                                         const int32_t* steps, const uint64_t* seed, int32_t n,
+                                         double* out_prices, double* out_stderr) {
+    static const char* where = "qk_mcm_mixed_price_batch_sharded";
+    if (!dist) return fail_null("dist");
+    qkb::BatchInput in;
+    int32_t rc = mixed_input(model, spot, strike, t, vol, r, q, v0, kappa, theta, sigma, rho,
+                             option_type, paths, steps, seed, n, &in);
+    if (rc != QK_OK) return rc;
+    if (!out_prices) return fail_null("out_prices");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail_cuda(e, where);
+    // the tile geometry of the single-GPU mixed call, so the results match it
+    qkb::Plan* plan = qkb::thread_scratch_plan(dev);
+    std::string err;
+    if ((e = plan->build(in, qkb::kFlagPersistent, &err)) != cudaSuccess) return fail_cuda(e, where);
+    if ((rc = qkb::dist_execute(*plan, dist, nullptr, where)) != QK_OK) return rc;
+    if ((e = plan->results(out_prices, out_stderr)) != cudaSuccess) return fail_cuda(e, where);
+    return QK_OK;
+}
+
+int32_t qk_mcm_plan_shard_bounds(qk_mc_plan* plan, int32_t world, int64_t* bounds) {
+    if (!plan) return fail_null("plan");
+    if (!bounds) return fail_null("bounds");
+    if (world <= 0) return fail_size(world);
+    const std::vector<int64_t>& b = plan->plan.shard_bounds(world);
+    std::memcpy(bounds, b.data(), sizeof(int64_t) * ((size_t)world + 1));
+    return QK_OK;
+}
+
+int32_t qk_mcm_plan_execute_tiles(qk_mc_plan* plan, int64_t tile_begin, int64_t tile_end,
+                                  void* stream) {
+    static const char* where = "qk_mcm_plan_execute_tiles";
+    if (!plan) return fail_null("plan");
+    qkb::Plan& p = plan->plan;
+    if (tile_begin < 0 || tile_end < tile_begin || tile_end > p.n_tiles()) {
+        set_error_fmt("invalid input: tiles [%lld, %lld) outside [0, %lld) in %s",
+                      (long long)tile_begin, (long long)tile_end, (long long)p.n_tiles(), where);
+        return QK_ERR_INVALID_INPUT;
+    }
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e == cudaSuccess && prev != p.device()) e = cudaSetDevice(p.device());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : p.stream();
+    if (e == cudaSuccess) e = p.order_after_upload(st);
+    if (e == cudaSuccess) e = p.launch_tiles(st, tile_begin, tile_end, false);
+    if (e == cudaSuccess) p.note_stream(st);
+    if (prev >= 0 && prev != p.device()) cudaSetDevice(prev);
+    return e == cudaSuccess ? QK_OK : fail_cuda(e, where);
+}
+
+int32_t qk_mcm_plan_device_partials(qk_mc_plan* plan, void** d_partials, int64_t* n_tiles,
+                                    int32_t* bytes_per_tile) {
+    if (!plan) return fail_null("plan");
+    if (d_partials) *d_partials = plan->plan.d_partials();
+    if (n_tiles) *n_tiles = plan->plan.n_tiles();
+    if (bytes_per_tile) *bytes_per_tile = (int32_t)sizeof(qkb::TilePartial);
+    return QK_OK;
+}
+
+int32_t qk_mcm_plan_finalize(qk_mc_plan* plan, void* stream) {
+    if (!plan) return fail_null("plan");
+    qkb::Plan& p = plan->plan;
+    int prev = -1;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e == cudaSuccess && prev != p.device()) e = cudaSetDevice(p.device());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : p.stream();
+    if (e == cudaSuccess) e = p.order_after_upload(st);
+    if (e == cudaSuccess) e = p.launch_finalize_all(st);
+    if (e == cudaSuccess) p.note_stream(st);
+    if (prev >= 0 && prev != p.device()) cudaSetDevice(prev);
+    return e == cudaSuccess ? QK_OK : fail_cuda(e, "qk_mcm_plan_finalize");
+}
+
+int32_t qk_mcm_plan_execute_sharded(qk_mc_plan* plan, qk_dist* dist, void* stream) {
+    if (!plan) return fail_null("plan");
+    return qkb::dist_execute(plan->plan, dist, static_cast<cudaStream_t>(stream),
+                             "qk_mcm_plan_execute_sharded");
 }
 
 int32_t qk_mcm_plan_create(const int32_t* model, const double* spot, const double* strike,

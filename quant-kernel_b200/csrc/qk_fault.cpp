@@ -19,6 +19,7 @@ int armed_sites() {
     if (std::strstr(v, "alloc")) sites |= kFaultAlloc;
     if (std::strstr(v, "launch")) sites |= kFaultLaunch;
     if (std::strstr(v, "copy")) sites |= kFaultCopy;
+    if (std::strstr(v, "collective")) sites |= kFaultCollective;
     return sites;
 }
 

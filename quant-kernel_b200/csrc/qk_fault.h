@@ -5,6 +5,8 @@
 //   alloc   device / pinned allocations report cudaErrorMemoryAllocation
 //   launch  kernel launches report cudaErrorLaunchFailure before launching
 //   copy    host<->device copies report cudaErrorUnknown before copying
+//   collective  the sharded execute reports cudaErrorUnknown instead of
+//               issuing its NCCL exchange (after its own simulate kernels)
 // The variable is read at every site, so a process can arm and disarm it.
 // An injected failure is reported like a real one (QK_ERR_RUNTIME_INIT and a
 // "cuda error: ..." message) with "[injected]" appended to the message.
@@ -17,7 +19,7 @@
 
 namespace qkb {
 
-enum FaultSite : int { kFaultAlloc = 1, kFaultLaunch = 2, kFaultCopy = 4 };
+enum FaultSite : int { kFaultAlloc = 1, kFaultLaunch = 2, kFaultCopy = 4, kFaultCollective = 8 };
 
 // cudaSuccess, or the injected error for `site` when QK_B200_FAULT arms it.
 cudaError_t injected_fault(FaultSite site);

@@ -36,3 +36,5 @@ QK_PLAN_TIMING = 0x8
 QK_PLAN_AUTOTUNE = 0x10
 QK_PLAN_FAMILY_GRIDS = 0x20
 QK_PLAN_STEP_UNROLL2 = 0x40
+
+QK_DIST_ID_BYTES = 128  # communicator id of the sharded calls (qk_dist_unique_id)

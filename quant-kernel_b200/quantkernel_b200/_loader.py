@@ -102,6 +102,18 @@ FUNCTION_SIGNATURES = [
     ("qk_mcm_plan_config", I32, [VP, PI32, PI32, PI32]),
     ("qk_mcm_plan_step_unroll", I32, [VP, PI32]),
     ("qk_mcm_plan_destroy", I32, [VP]),
+    ("qk_dist_unique_id", I32, [VP]),
+    ("qk_dist_create", I32, [VP, I32, I32, ct.POINTER(VP)]),
+    ("qk_dist_info", I32, [VP, PI32, PI32, PI32]),
+    ("qk_dist_abort", I32, [VP]),
+    ("qk_dist_destroy", I32, [VP]),
+    ("qk_dist_partition", I32, [PD, I64, I32, PI64]),
+    ("qk_mcm_plan_execute_sharded", I32, [VP, VP, VP]),
+    ("qk_mcm_plan_shard_bounds", I32, [VP, I32, PI64]),
+    ("qk_mcm_plan_execute_tiles", I32, [VP, I64, I64, VP]),
+    ("qk_mcm_plan_device_partials", I32, [VP, ct.POINTER(VP), PI64, PI32]),
+    ("qk_mcm_plan_finalize", I32, [VP, VP]),
+    ("qk_mcm_mixed_price_batch_sharded", I32, [VP] + _mixed_arrays + [PD, PD]),
     ("qk_sur_gemm_bf16", I32, [VP, VP, VP, I32, I32, I32, I32, VP]),
     ("qk_sur_heston_create", I32, [PD, PD, U64, ct.POINTER(VP)]),
     ("qk_sur_heston_destroy", I32, [VP]),

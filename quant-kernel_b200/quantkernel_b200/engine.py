@@ -639,6 +639,34 @@ class McPlan:
         self._lib.qk_mcm_plan_device_results(self._h, ct.byref(p), ct.byref(s))
         return p.value, s.value
 
+    def shard_bounds(self, world: int) -> np.ndarray:
+        """Tile bounds of the sharded execute's partition (world + 1 entries)."""
+        b = np.empty(int(world) + 1, np.int64)
+        rc = self._lib.qk_mcm_plan_shard_bounds(self._h, int(world),
+                                                b.ctypes.data_as(ct.POINTER(ct.c_int64)))
+        if rc != QK_OK:
+            self._qk._raise_rc("qk_mcm_plan_shard_bounds", rc)
+        return b
+
+    def execute_tiles(self, tile_begin: int, tile_end: int, stream: int = 0) -> None:
+        """The simulate kernels over tiles [tile_begin, tile_end) only."""
+        rc = self._lib.qk_mcm_plan_execute_tiles(self._h, int(tile_begin), int(tile_end),
+                                                 ct.c_void_p(stream) if stream else None)
+        if rc != QK_OK:
+            self._qk._raise_rc("qk_mcm_plan_execute_tiles", rc)
+
+    def finalize(self, stream: int = 0) -> None:
+        """The finalize kernel over every option (after all tiles' sums are in place)."""
+        rc = self._lib.qk_mcm_plan_finalize(self._h, ct.c_void_p(stream) if stream else None)
+        if rc != QK_OK:
+            self._qk._raise_rc("qk_mcm_plan_finalize", rc)
+
+    def device_partials(self):
+        """(device pointer, tiles, bytes per tile) of the per-tile sums."""
+        p, n, b = ct.c_void_p(), ct.c_int64(0), ct.c_int32(0)
+        self._lib.qk_mcm_plan_device_partials(self._h, ct.byref(p), ct.byref(n), ct.byref(b))
+        return p.value, n.value, b.value
+
     def stats(self):
         ms = ct.c_double(0.0)
         launches = ct.c_int32(0)

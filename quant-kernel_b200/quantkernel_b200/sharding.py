@@ -1,79 +1,103 @@
-"""Pricing one batch across several GPUs, one process per GPU.
+"""One batch priced across several GPUs, one rank (process or thread) per GPU.
 
-Options are independent, so a batch shards by option with no exchange during
-pricing: each rank prices a contiguous range whose Monte Carlo cost
-(paths x steps) is about 1/world of the total, then one all-gather of
-(price, standard error) puts every result on every rank in the original
-option order.  Each rank's results are computed exactly as a single-GPU call
-would compute them (a path's random stream depends only on its option's seed
-and path index), so the sharded answer equals the unsharded one bit for bit.
+Thin wrapper over the library's C ABI (qk_dist_*, qk_mcm_*_sharded in
+include/qk_api.h); no framework is needed.  Every rank builds the same plan
+from the same inputs; a sharded execute simulates this rank's contiguous range
+of the plan's tiles (balanced by path-steps), exchanges every rank's tile sums
+over NCCL in one grouped step, and finalizes every option on every rank.  A
+path's random stream depends only on its option's seed and path index and the
+merge order is fixed, so each rank ends up with exactly the single-GPU
+results.
+
+The communicator id (QK_DIST_ID_BYTES bytes) is made once, by one rank, with
+`new_id()` and handed to the others by any channel the job already has (a
+shared file, a socket, the launcher's key-value store).
 """
+
+import ctypes as ct
 
 import numpy as np
 
-
-def option_cost(batch) -> np.ndarray:
-    """Relative Monte Carlo cost of each option: paths x max(steps, 1)."""
-    p = np.asarray(batch["paths"], np.int64)
-    s = batch.get("steps")
-    s = np.ones_like(p) if s is None else np.maximum(np.asarray(s, np.int64), 1)
-    return np.maximum(p, 0) * s
+from ._abi import QK_DIST_ID_BYTES, QK_OK
+from .engine import McPlan, QuantKernel
 
 
-def partition_by_cost(cost, world: int):
-    """Contiguous [begin, end) ranges, one per rank, with near-equal total cost.
-
-    Boundary r is the first option whose cumulative cost reaches r/world of
-    the total; every rank gets a (possibly empty) range and the ranges cover
-    0..n exactly once in order."""
-    cost = np.asarray(cost, np.float64)
-    n = cost.size
-    if world <= 1 or n == 0:
-        return [(0, n)] + [(n, n)] * max(world - 1, 0)
-    cum = np.cumsum(cost)
-    total = cum[-1] if cum.size else 0.0
-    bounds = [0]
-    for r in range(1, world):
-        target = total * r / world
-        b = int(np.searchsorted(cum, target, side="left"))
-        bounds.append(min(max(b, bounds[-1]), n))
-    bounds.append(n)
-    return [(bounds[i], bounds[i + 1]) for i in range(world)]
+def new_id(qk: QuantKernel = None) -> bytes:
+    """A fresh communicator id; call on one rank only."""
+    qk = qk or QuantKernel()
+    buf = (ct.c_uint8 * QK_DIST_ID_BYTES)()
+    rc = qk._lib.qk_dist_unique_id(buf)
+    if rc != QK_OK:
+        qk._raise_rc("qk_dist_unique_id", rc)
+    return bytes(buf)
 
 
-def price_sharded(batch, pricer, group=None, device=None):
-    """Price `batch` (dict of equal-length arrays) across the ranks of `group`.
+def partition(cost, world: int) -> np.ndarray:
+    """The sharded execute's partition rule on a list of costs: `world` + 1
+    bounds of contiguous ranges with near-equal total cost (host only)."""
+    qk = QuantKernel()
+    c = np.ascontiguousarray(cost, np.float64)
+    bounds = np.empty(int(world) + 1, np.int64)
+    rc = qk._lib.qk_dist_partition(c.ctypes.data_as(ct.POINTER(ct.c_double)), int(c.size),
+                                   int(world), bounds.ctypes.data_as(ct.POINTER(ct.c_int64)))
+    if rc != QK_OK:
+        qk._raise_rc("qk_dist_partition", rc)
+    return bounds
 
-    `pricer(sub_batch) -> (prices, stderr)` runs on this rank's range (for a
-    GPU library: ``lambda b: qk.mixed_price_batch(**b)``).  Returns the full
-    (prices, stderr) on every rank.  Uses torch.distributed: NCCL for CUDA
-    tensors (pass `device`), gloo on CPU."""
-    import torch
-    import torch.distributed as dist
 
-    world = dist.get_world_size(group)
-    rank = dist.get_rank(group)
-    n = len(next(iter(batch.values())))
-    ranges = partition_by_cost(option_cost(batch), world)
-    b0, b1 = ranges[rank]
-    sub = {k: np.asarray(v)[b0:b1] for k, v in batch.items()}
-    if b1 > b0:
-        p, se = pricer(sub)
-    else:
-        p, se = np.empty(0), np.empty(0)
-    width = max(e - b for b, e in ranges)
-    buf = np.full((2, max(width, 1)), np.nan)
-    buf[0, : b1 - b0] = p
-    buf[1, : b1 - b0] = se
-    t = torch.from_numpy(buf)
-    if device is not None:
-        t = t.to(device)
-    parts = [torch.empty_like(t) for _ in range(world)]
-    dist.all_gather(parts, t, group=group)
-    prices = np.empty(n)
-    stderr = np.empty(n)
-    for r, (b, e) in enumerate(ranges):
-        arr = parts[r].cpu().numpy()
-        prices[b:e] = arr[0, : e - b]
-        stderr[b:e] = arr[1, : e - b]
-    return prices, stderr
+class DistContext:
+    """Rank `rank` of `world`, on the calling thread's current device (set it
+    first with QuantKernel.set_device)."""
+
+    def __init__(self, unique_id: bytes, world: int, rank: int, qk: QuantKernel = None):
+        if len(unique_id) != QK_DIST_ID_BYTES:
+            raise ValueError(f"communicator id must be {QK_DIST_ID_BYTES} bytes")
+        self.qk = qk or QuantKernel()
+        self._lib = self.qk._lib
+        self._h = ct.c_void_p()
+        buf = (ct.c_uint8 * QK_DIST_ID_BYTES).from_buffer_copy(unique_id)
+        rc = self._lib.qk_dist_create(buf, int(world), int(rank), ct.byref(self._h))
+        if rc != QK_OK:
+            self.qk._raise_rc("qk_dist_create", rc)
+        self.world, self.rank = int(world), int(rank)
+
+    def execute(self, plan: McPlan, stream: int = 0) -> None:
+        """This rank's share of `plan`; then plan.results() holds every option."""
+        rc = self._lib.qk_mcm_plan_execute_sharded(plan._h, self._h,
+                                                   ct.c_void_p(stream) if stream else None)
+        if rc != QK_OK:
+            self.qk._raise_rc("qk_mcm_plan_execute_sharded", rc)
+
+    def mixed_price_batch(self, model, spot, strike, t, vol=None, r=None, q=None, v0=None,
+                          kappa=None, theta=None, sigma=None, rho=None, option_type=None,
+                          paths=None, steps=None, seed=None):
+        """QuantKernel.mixed_price_batch across the ranks: every rank passes the
+        whole batch and gets (prices, standard errors) of every option."""
+        arrays = self.qk._mixed_arrays(model, spot, strike, t, vol, r, q, v0, kappa, theta,
+                                       sigma, rho, option_type, paths, steps, seed)
+        n = int(arrays[0].shape[0])
+        out = np.empty(n)
+        se = np.empty(n)
+        from .engine import _ptr
+
+        rc = self._lib.qk_mcm_mixed_price_batch_sharded(
+            self._h, *[_ptr(a) for a in arrays], n, out.ctypes.data_as(ct.POINTER(ct.c_double)),
+            se.ctypes.data_as(ct.POINTER(ct.c_double)))
+        if rc != QK_OK:
+            self.qk._raise_rc("qk_mcm_mixed_price_batch_sharded", rc)
+        return out, se
+
+    def abort(self) -> None:
+        if self._h:
+            self._lib.qk_dist_abort(self._h)
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.qk_dist_destroy(self._h)
+            self._h = ct.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
