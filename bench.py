@@ -671,7 +671,10 @@ def sharded_leg(qk, world, rank, dev, steps, warmup):
     ctx = DistContext(ident, world, rank, qk)
     h = workloads.heston(N_OPT, paths=PATHS, steps=STEPS)
     plan = qk.plan(model=np.full(N_OPT, QK_MC_HESTON, np.int32), **h)
-    stream = torch.cuda.current_stream(dev)
+    # a dedicated stream: the flush, the plan's kernels, the exchange and the
+    # timing events are all ordered on it
+    stream = torch.cuda.Stream(dev)
+    assert stream.cuda_stream != 0
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
@@ -679,17 +682,18 @@ def sharded_leg(qk, world, rank, dev, steps, warmup):
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    for _ in range(warmup):
-        flush.zero_()
-        ctx.execute(plan, stream.cuda_stream)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(steps):
-        flush.zero_()
-        ctx.execute(plan, stream.cuda_stream)
-    e1.record(stream)
-    barrier()
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            flush.zero_()
+            ctx.execute(plan, stream.cuda_stream)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            flush.zero_()
+            ctx.execute(plan, stream.cuda_stream)
+        e1.record(stream)
+        barrier()
     t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

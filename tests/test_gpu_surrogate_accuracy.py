@@ -8,13 +8,17 @@ judged by the library's plain GPU Monte Carlo.
   standard error is about 5e-5 x S.  Bars, stated against that judge: at
   least 99% of the queries within 5e-4 x S, none beyond 1e-3 x S (twice the
   bar: the network's worst in-box error plus four judge standard errors),
-  mean error at most 1.2e-4 x S.
+  mean error at most 1.2e-4 x S.  Measured: mean 5.4e-5, p99 2.1e-4, max
+  3.2e-4 x S, all 1024 within 5e-4 x S; the largest errors sit at Feller
+  ratios 2 kappa theta / sigma^2 below 0.5 with sigma above 0.8 and long
+  maturities, where the variance process spends most time at zero.
 * Arithmetic: the fused inference kernel against the oracle's FP64
   evaluation of the same bf16 network (weights and the bf16 operands of
   layers 2 and 3 rounded as the GPU rounds them).  What is left is FP32
   summation order and the special-function tanh of the SiLU, which can move
-  an activation to the neighbouring bf16 value; the bars are the measured
-  spread on this checkpoint with a margin.  Against the FP64 network on the
+  an activation to the neighbouring bf16 value; measured on 20,000 box rows
+  of this checkpoint: mean 2.0e-7 x S, max 2.7e-5 x S, and the bars are
+  mean 1e-6 and max 1e-4 (x S).  Against the FP64 network on the
   FP32 master weights (no bf16 rounding of weights or activations) the
   trained bf16 network differs by about 6.4e-4 x S on average and 5.4e-3 x S
   at most -- the network was trained in its bf16 form, which is the function
@@ -82,4 +86,4 @@ def test_shipped_surrogate_fused_kernel_vs_fp64_bf16_network(shipped):
     err = np.abs(y - (mo.forward_bf16(p, x) + base))
     print(f"fused kernel vs FP64 bf16 network: mean {err.mean():.2e} p999 "
           f"{np.quantile(err, 0.999):.2e} max {err.max():.2e}")
-    assert err.mean() <= 1e-4 and err.max() <= 2e-3, (err.mean(), err.max())
+    assert err.mean() <= 1e-6 and err.max() <= 1e-4, (err.mean(), err.max())
