@@ -89,6 +89,11 @@ def parse():
     ap.add_argument("--heston-cf", action="store_true",
                     help="Heston characteristic-function leg only")
     ap.add_argument("--cf-options", type=int, default=65536)
+    ap.add_argument("--mixed", action="store_true",
+                    help="mixed-model leg only (with --profile: the first --options options, "
+                         "persistent kernel and per-family grids, two executes each)")
+    ap.add_argument("--bsm", action="store_true",
+                    help="FP64 terminal BSM leg only (with --profile: three plain executes)")
     ap.add_argument("--vr", action="store_true",
                     help="variance-reduction leg only (device + e2e; no CPU with --profile)")
     ap.add_argument("--sur-device-rows", type=int, default=0,
@@ -1232,6 +1237,35 @@ def heston_cf_leg(qk, reps=5, n=65536, cpu=True):
     return res
 
 
+def profile_plans(qk, which, n_opt):
+    """Small launches for ncu captures: the mixed workload's first n_opt
+    options as the persistent kernel, then as per-family grids (two executes
+    each), or the FP64 terminal workload (three executes)."""
+    import torch
+
+    from quantkernel_b200 import (QK_MC_ANTITHETIC, QK_PLAN_FAMILY_GRIDS, QK_PLAN_PERSISTENT,
+                                  workloads)
+
+    out = {"profile": which}
+    if which == "mixed":
+        b = {k: v[:n_opt] for k, v in workloads.mixed().items()}
+        for name, fl in (("persistent", QK_PLAN_PERSISTENT), ("grids", QK_PLAN_FAMILY_GRIDS)):
+            plan = qk.plan(**b, flags=fl)
+            for _ in range(2):
+                plan.execute(torch.cuda.current_stream().cuda_stream)
+            out[name] = float(plan.results()[0].sum())
+            plan.close()
+        out["options"] = n_opt
+    else:
+        b = workloads.bsm_terminal()
+        plan = qk.plan(model=np.full(len(b["spot"]), QK_MC_ANTITHETIC, np.int32), **b)
+        for _ in range(3):
+            plan.execute(torch.cuda.current_stream().cuda_stream)
+        out["price_sum"] = float(plan.results()[0].sum())
+        plan.close()
+    return out
+
+
 def main():
     args = parse()
     if args.surrogate_train:
@@ -1260,6 +1294,21 @@ def main():
         torch.cuda.set_stream(torch.cuda.Stream())
         leg = vr_leg(QuantKernel(), cpu=not args.profile)
         print(json.dumps({"leg": "variance_reduction", **leg}), flush=True)
+        return 0
+    if args.mixed or args.bsm:
+        import torch
+
+        from quantkernel_b200 import QuantKernel
+
+        torch.cuda.set_stream(torch.cuda.Stream())
+        qk = QuantKernel()
+        if args.profile:
+            print(json.dumps(profile_plans(qk, "mixed" if args.mixed else "bsm", args.options)),
+                  flush=True)
+        elif args.mixed:
+            print(json.dumps({"leg": "mixed", **mixed_leg(qk)}), flush=True)
+        else:
+            print(json.dumps({"leg": "bsm_terminal", **bsm_terminal_leg(qk)}), flush=True)
         return 0
     if args.heston_cf:
         from quantkernel_b200 import QuantKernel
