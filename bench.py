@@ -990,6 +990,20 @@ def mixed_leg(qk, reps=5, f_mhz=1965.0, cpu=True):
         out[idx] = sub.results()[0]
         sub.close()
     assert np.allclose(out, p_pers, rtol=1e-12, atol=0)
+    # a small uneven batch (the first 48 options): per-family grids of a few
+    # waves each leave tails that the persistent kernel's work stealing fills
+    small = {k: v[:48] for k, v in b.items()}
+    sm = {}
+    for name, fl in (("persistent_graph_ms", QK_PLAN_PERSISTENT),
+                     ("family_grids_graph_ms", QK_PLAN_FAMILY_GRIDS),
+                     ("autotuned_graph_ms", QK_PLAN_AUTOTUNE)):
+        plan = qk.plan(**small, flags=fl | QK_PLAN_GRAPH | QK_PLAN_TIMING)
+        sm[name] = _time_plan(plan, stream, flush, reps)
+        if fl == QK_PLAN_AUTOTUNE:
+            sm["launch_config"] = plan.config()
+        plan.close()
+    sm["workload"] = (f"the first 48 options of the batch, "
+                      f"{workloads.path_steps(small):.3g} path-steps")
     # kernel time of the autotuned launch (no graph: events around the
     # simulate kernels only) for the roofline
     plan = qk.plan(**b, flags=QK_PLAN_AUTOTUNE | QK_PLAN_TIMING)
@@ -1007,6 +1021,7 @@ def mixed_leg(qk, reps=5, f_mhz=1965.0, cpu=True):
            "launch_config": cfg,
            "launch_config_note": "units_per_thread 0 = persistent kernel, -1 = one grid per "
                                  "family group",
+           "small_batch": sm,
            "roofline": roof}
     if cpu:
         res["cpu_baseline"] = _rate_baseline("mixed", "path_steps", "path-steps/s", 10.0, 4.0,
