@@ -4,6 +4,7 @@
 
 #include <dlfcn.h>
 
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -83,6 +84,9 @@ struct qk_dist {
     int rank = 0;
     int device = -1;
     int64_t* d_check = nullptr;  // 4 int64 on `device`: the tiling check
+    // set by qk_dist_abort (possibly from another thread); NCCL frees an
+    // aborted communicator, so no call may use `comm` afterwards
+    std::atomic<bool> aborted{false};
 };
 
 namespace {
@@ -112,6 +116,10 @@ namespace qkb {
 int32_t dist_execute(Plan& plan, qk_dist* d, cudaStream_t stream, const char* where) {
     if (!d) return fail_null("dist");
     if (!nccl().load_error.empty()) return nccl_missing(where);
+    if (d->aborted.load()) {
+        set_error_fmt("invalid input: the communicator was aborted in %s", where);
+        return QK_ERR_INVALID_INPUT;
+    }
     if (plan.device() != d->device) {
         set_error_fmt("invalid input: plan on device %d, communicator on device %d in %s",
                       plan.device(), d->device, where);
@@ -243,18 +251,15 @@ int32_t qk_dist_info(const qk_dist* d, int32_t* world, int32_t* rank, int32_t* d
 
 int32_t qk_dist_abort(qk_dist* d) {
     if (!d) return qkb::fail_null("dist");
-    if (d->comm) {
-        const ncclResult_t r = nccl().comm_abort(d->comm);
-        d->comm = nullptr;
-        if (r != ncclSuccess) return fail_nccl(r, "qk_dist_abort");
-    }
-    return QK_OK;
+    if (d->aborted.exchange(true)) return QK_OK;  // already aborted
+    const ncclResult_t r = nccl().comm_abort(d->comm);
+    return r == ncclSuccess ? QK_OK : fail_nccl(r, "qk_dist_abort");
 }
 
 int32_t qk_dist_destroy(qk_dist* d) {
     if (!d) return QK_OK;
     ncclResult_t r = ncclSuccess;
-    if (d->comm) r = nccl().comm_destroy(d->comm);
+    if (d->comm && !d->aborted.load()) r = nccl().comm_destroy(d->comm);
     if (d->d_check) {
         int prev = -1;
         if (cudaGetDevice(&prev) == cudaSuccess && prev != d->device) cudaSetDevice(d->device);
