@@ -95,3 +95,21 @@ def test_injected_collective_failure_leaves_the_next_call_correct(qk, dist, monk
     monkeypatch.delenv("QK_B200_FAULT")
     p, _ = dist.mixed_price_batch(**b)
     assert np.array_equal(p, want_p)
+
+
+def test_aborted_communicator_refuses_further_work(qk):
+    # host-side failure handling: after qk_dist_abort (what a watchdog thread
+    # calls when a peer is lost) the communicator is never used again
+    qk.set_device(0)
+    ctx = DistContext(new_id(qk), 1, 0, qk)
+    b = workloads.mixed(16, seed=35, log2_paths=(8.0, 10.0), log2_steps=(2.0, 3.0))
+    plan = qk.plan(**b)
+    ctx.execute(plan)
+    want = plan.results()[0]
+    ctx.abort()
+    with pytest.raises(QKInvalidInputError, match="aborted"):
+        ctx.execute(plan)
+    ctx.close()
+    plan.execute()  # the plan and the device stay usable
+    assert np.array_equal(plan.results()[0], want)
+    plan.close()
