@@ -296,6 +296,10 @@ SurModel::~SurModel() {
         if (p) cudaFree(p);
     if (perm_) cudaFree(perm_);
     if (state_) cudaFree(state_);
+    for (cudaEvent_t& e : ev_)
+        if (e) cudaEventDestroy(e);
+    for (cudaStream_t& a : aux_)
+        if (a) cudaStreamDestroy(a);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -303,6 +307,8 @@ cudaError_t SurModel::init(uint64_t seed, const SurBox& box) {
     QK_TRY(cudaGetDevice(&device_));
     box_ = box;
     QK_TRY(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (cudaStream_t& a : aux_) QK_TRY(cudaStreamCreateWithFlags(&a, cudaStreamNonBlocking));
+    for (cudaEvent_t& e : ev_) QK_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     QK_TRY(dalloc(&P_, SurLayout::total));
     QK_TRY(dalloc(&M_, SurLayout::total));
     QK_TRY(dalloc(&V_, SurLayout::total));
@@ -470,31 +476,45 @@ cudaError_t SurModel::run_step(cudaStream_t st, bool update) {
     l.target = Tb_; l.y_out = y_; l.dy_out = dy_; l.loss_scale = 2.0f / static_cast<float>(B);
     l.d_out = dZ3_; l.dt_out = dZ3T_; l.t_out = H3T_; l.ldt = B;
     QK_TRY(launch_umma_gemm(kEpiLast, 256, tH2, tW3, l, 1, st));
-    loss_kernel<<<1, 256, 0, st>>>(y_, Tb_, dy_, state_, db4_, loss_hist_, loss_cap_);
-    rowsum_kernel<<<kSurHid / 8, 256, 0, st>>>(dZ3T_, kSurHid, B, nullptr, db3_);
-    rowsum_kernel<<<kSurHid / 8, 256, 0, st>>>(H3T_, kSurHid, B, dy_, dw4_);
+    // Side branch 1 (aux_[0]): the loss, db3, dw4 and the dW3 GEMM read only
+    // what layer 3's epilogue wrote; they run beside the backward chain.
+    QK_TRY(cudaEventRecord(ev_[0], st));
+    QK_TRY(cudaStreamWaitEvent(aux_[0], ev_[0], 0));
+    loss_kernel<<<1, 256, 0, aux_[0]>>>(y_, Tb_, dy_, state_, db4_, loss_hist_, loss_cap_);
+    rowsum_kernel<<<kSurHid / 8, 256, 0, aux_[0]>>>(dZ3T_, kSurHid, B, nullptr, db3_);
+    rowsum_kernel<<<kSurHid / 8, 256, 0, aux_[0]>>>(H3T_, kSurHid, B, dy_, dw4_);
     QK_TRY(cudaGetLastError());
-    // layer 3 backward to layer 2, and dW3
+    GemmArgs w{};
+    w.err = err;
+    w.M = kSurHid; w.N = kSurHid; w.K = B; w.k_per_split = 128; w.c_f32 = dW3p_;
+    QK_TRY(launch_umma_gemm(kEpiF32, 128, tdZ3T, tH2T, w, S, aux_[0]));
+    QK_TRY(cudaEventRecord(ev_[1], aux_[0]));
+    // layer 3 backward to layer 2
     GemmArgs b{};
     b.err = err;
     b.M = B; b.N = kSurHid; b.K = kSurHid; b.k_per_split = kSurHid; b.ldt = B;
     b.z_in = Z2_; b.d_out = dZ2_; b.dt_out = dZ2T_;
     QK_TRY(launch_umma_gemm(kEpiBwd, 128, tdZ3, tW3T, b, 1, st));
-    GemmArgs w{};
-    w.err = err;
-    w.M = kSurHid; w.N = kSurHid; w.K = B; w.k_per_split = 128; w.c_f32 = dW3p_;
-    QK_TRY(launch_umma_gemm(kEpiF32, 128, tdZ3T, tH2T, w, S, st));
-    // layer 2 backward to layer 1, and dW2
+    // Side branch 2 (aux_[1]): dW2 and db2 read layer 2's gradient
+    QK_TRY(cudaEventRecord(ev_[2], st));
+    QK_TRY(cudaStreamWaitEvent(aux_[1], ev_[2], 0));
+    GemmArgs w2 = w;
+    w2.c_f32 = dW2p_;
+    QK_TRY(launch_umma_gemm(kEpiF32, 128, tdZ2T, tH1T, w2, S, aux_[1]));
+    rowsum_kernel<<<kSurHid / 8, 256, 0, aux_[1]>>>(dZ2T_, kSurHid, B, nullptr, db2_);
+    QK_TRY(cudaGetLastError());
+    QK_TRY(cudaEventRecord(ev_[3], aux_[1]));
+    // layer 2 backward to layer 1, dW1 (N = 64 padded inputs) and db1
     b.z_in = Z1_; b.d_out = dZ1_; b.dt_out = dZ1T_;
     QK_TRY(launch_umma_gemm(kEpiBwd, 128, tdZ2, tW2T, b, 1, st));
-    w.c_f32 = dW2p_;
-    QK_TRY(launch_umma_gemm(kEpiF32, 128, tdZ2T, tH1T, w, S, st));
-    // dW1 (N = 64 padded inputs)
-    w.N = kSurInPad; w.c_f32 = dW1p_;
-    QK_TRY(launch_umma_gemm(kEpiF32, 64, tdZ1T, tXTb, w, S, st));
-    rowsum_kernel<<<kSurHid / 8, 256, 0, st>>>(dZ2T_, kSurHid, B, nullptr, db2_);
+    GemmArgs w1 = w;
+    w1.N = kSurInPad; w1.c_f32 = dW1p_;
+    QK_TRY(launch_umma_gemm(kEpiF32, 64, tdZ1T, tXTb, w1, S, st));
     rowsum_kernel<<<kSurHid / 8, 256, 0, st>>>(dZ1T_, kSurHid, B, nullptr, db1_);
     QK_TRY(cudaGetLastError());
+    // join both branches before Adam reads every gradient
+    QK_TRY(cudaStreamWaitEvent(st, ev_[1], 0));
+    QK_TRY(cudaStreamWaitEvent(st, ev_[3], 0));
 
     AdamArgs a{};
     const int hid2 = kSurHid * kSurHid;

@@ -105,6 +105,11 @@ private:
 
     int device_ = -1;
     cudaStream_t stream_ = nullptr;
+    // the training step's side branches (loss and bias sums with the dW3
+    // GEMM; the dW2 GEMM with db2) run on these beside the backward chain,
+    // forked and joined by events (inside the captured step graph too)
+    cudaStream_t aux_[2] = {nullptr, nullptr};
+    cudaEvent_t ev_[4] = {nullptr, nullptr, nullptr, nullptr};
     SurBox box_{};
     int32_t base_kind_ = kSurBaseBsmMeanVar;
     // parameters, Adam moments, gradient
