@@ -405,43 +405,53 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
 
 // ----------------------------------------------------------------------------
-// Fused MLP inference.  One persistent CTA per SM walks 128-row tiles with
-// three warp roles:
-//   warp 16 (one lane)  TMA producer: per tile the input rows X and the nine
-//                       32 KiB weight k-blocks W1, W2[0..3], W3[0..3] through
-//                       a 4-slot ring (a slot is reloaded once the MMA that
-//                       read it has completed);
-//   warp 17 (one lane)  MMA issuer: layer 1 (K = 64), then layers 2 and 3 k-block
-//                       by k-block, each k-block as soon as the epilogue has
-//                       written that 64-column block of the previous layer's
-//                       activations;
-//   warps 0-15          epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31
-//                       (its tile rows) and, in each 64-column block kb,
-//                       columns 64 kb + 16 (w / 4) .. + 15; bias + SiLU, BF16
-//                       into shared memory in the 128-byte-swizzled K-major
-//                       layout the next layer's MMA reads as its A operand.
-// Two TMEM accumulators (2 x 256 columns) alternate between consecutive
-// layers, so layer l + 1's MMAs run while layer l's epilogue is still
-// reading: all 16 epilogue warps finish block kb of the activations before
-// any starts block kb + 1, and the MMA issuer takes the blocks in that order.
+// Fused MLP inference.  One persistent CTA per SM walks its 128-row tiles two
+// at a time, ping-pong: tile slot s (0, 1) owns TMEM accumulator s (256 fp32
+// columns) and a 64 KiB shared buffer that holds the slot's input rows, then
+// layer 1's and layer 2's activations.  While the epilogue warps work on one
+// slot's layer, the tensor core computes the other slot's, so neither waits
+// for the other's tail.  Four warp roles:
+//   warp 16 (one lane)  weight producer: the 32 KiB weight k-blocks in the
+//                       order the MMA issuer takes them (per tile pair: W1 for
+//                       A, W1 for B, W2[0..3] for A, for B, W3[0..3] for A,
+//                       for B) through a 2-slot ring;
+//   warp 17 (one lane)  MMA issuer: per tile pair, layer by layer, tile A's
+//                       then tile B's: layer 1 (K = 64) once the slot's input
+//                       rows have landed and its previous tile's head has
+//                       read the accumulator, layers 2 and 3 once the
+//                       epilogue has written the slot's previous layer;
+//   warp 18 (one lane)  input loader: a slot's next input rows once the MMAs
+//                       of its previous tile's layer 3 (the last reader of
+//                       the slot's buffer) have completed;
+//   warps 0-15          epilogue, in the MMA issuer's order: warp w reads TMEM
+//                       lanes 32 (w % 4) .. + 31 (its tile rows) and, in each
+//                       64-column block kb, columns 64 kb + 16 (w / 4) .. + 15;
+//                       bias + SiLU, BF16 into the slot's buffer in the
+//                       128-byte-swizzled K-major layout the next layer's MMA
+//                       reads as its A operand; the head sums partial chains
+//                       and writes the prices.
 // Every hand-off is an mbarrier with a bounded wait (no CTA-wide barrier
 // inside the loop), so a timeout anywhere ends every role with an error code.
-// Hazards, each closed by the order of the chain: a layer's accumulator is
-// rewritten two layers later, after every epilogue warp has reported the
-// intervening layer's activations (or, for the head, the next tile's first
-// layer); the activation buffer is rewritten only after the accumulator
-// commit of the layer that read it; the input rows are reloaded after the
-// commit of the layer-1 MMAs.
+// Barriers per slot: xfull (input rows landed), accfull (a layer's MMAs
+// complete: three phases per tile), hdone (all 16 epilogue warps finished a
+// layer of the slot: three phases per tile), pready (the head's partial sums,
+// one phase per tile).  Hazards, each closed by the chain: an accumulator is
+// rewritten only after hdone reports the epilogue read it; a buffer is
+// rewritten by the epilogue only after accfull reports that the MMAs which
+// read it completed, and by the input loader only after the slot's layer-3
+// accfull; the head's partial sums are double-buffered by slot.
 // The arithmetic and summation order are those of the layer-by-layer GEMMs
 // (kEpiFwd, kEpiLast), so the results are the same bits.
 // ----------------------------------------------------------------------------
-constexpr int kIWSlots = 4;
+constexpr int kIWSlots = 2;
 constexpr uint32_t kWBlock = 256 * kBK * 2;        // 32 KiB: 256 rows x 64 bf16
 constexpr uint32_t kHBytes = 4 * kABytes;          // 64 KiB: 128 rows x 256 bf16
-constexpr size_t kInferSmem = kHBytes + kABytes + kIWSlots * kWBlock + 1024;
+constexpr int kTileSlots = 2;
+constexpr size_t kInferSmem = kTileSlots * kHBytes + kIWSlots * kWBlock + 1024;
 constexpr int kInferEpiWarps = 16;                 // 4 per TMEM lane quarter
-constexpr int kInferThreads = (kInferEpiWarps + 2) * 32;
-constexpr int kProducerWarp = kInferEpiWarps, kMmaWarp = kInferEpiWarps + 1;
+constexpr int kInferThreads = (kInferEpiWarps + 3) * 32;
+constexpr int kProducerWarp = kInferEpiWarps, kMmaWarp = kInferEpiWarps + 1,
+              kXWarp = kInferEpiWarps + 2;
 
 // 16 consecutive fp32 columns of this thread's TMEM lane (no wait).
 __device__ __forceinline__ void tmem_ld16_async(uint32_t taddr, uint32_t (&r)[16]) {
@@ -481,21 +491,22 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                ~static_cast<uintptr_t>(1023));
-    uint8_t* hbuf = smem;
-    uint8_t* xbuf = smem + kHBytes;
-    uint8_t* wbuf = xbuf + kABytes;
-    __shared__ __align__(8) uint64_t xfull, xempty, drain, pready;
-    __shared__ __align__(8) uint64_t accfull[2];
-    __shared__ __align__(8) uint64_t hfull[4];
-    __shared__ __align__(8) uint64_t wfull[kIWSlots];
-    __shared__ __align__(8) uint64_t wempty[kIWSlots];
+    uint8_t* hbufs = smem;  // [kTileSlots][kHBytes]: a slot's input rows, then its activations
+    uint8_t* wbuf = smem + kTileSlots * kHBytes;
+    __shared__ __align__(8) uint64_t xfull[kTileSlots], slotfree[kTileSlots], accfull[kTileSlots];
+    __shared__ __align__(8) uint64_t hdone[kTileSlots], pready[kTileSlots];
+    __shared__ __align__(8) uint64_t wfull[kIWSlots], wempty[kIWSlots], drain;
     __shared__ float sb1[kSurHidden], sb2[kSurHidden], sb3[kSurHidden], sw4[kSurHidden];
-    __shared__ float part[4][kBM];  // head partial sums per column group
+    __shared__ float part[kTileSlots][4][kBM];  // head partial sums per slot and column group
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int64_t n_tiles = (a.n + kBM - 1) / kBM;
+    // this CTA's tiles i = 0, 1, ...: tile blockIdx.x + i gridDim.x, slot i % 2,
+    // the slot's use u = i / 2; tiles 2p and 2p + 1 form pair p
+    const int64_t my_tiles =
+        blockIdx.x < n_tiles ? (n_tiles - 1 - static_cast<int64_t>(blockIdx.x)) / gridDim.x + 1 : 0;
 
     if (tid < kSurHidden) {
         sb1[tid] = 0.5f * a.b1[tid];  // halved biases for silu_from_acc (exact)
@@ -504,20 +515,22 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         sw4[tid] = a.w4[tid];
     }
     if (tid == 0) {
-        mbar_init(smem_u32(&xfull), 1);
-        mbar_init(smem_u32(&xempty), 1);
-        mbar_init(smem_u32(&drain), 1);
-        mbar_init(smem_u32(&pready), kInferEpiWarps);
-        for (int i = 0; i < 2; ++i) mbar_init(smem_u32(&accfull[i]), 1);
-        for (int kb = 0; kb < 4; ++kb) mbar_init(smem_u32(&hfull[kb]), kInferEpiWarps);
+        for (int s = 0; s < kTileSlots; ++s) {
+            mbar_init(smem_u32(&xfull[s]), 1);
+            mbar_init(smem_u32(&slotfree[s]), 1);
+            mbar_init(smem_u32(&accfull[s]), 1);
+            mbar_init(smem_u32(&hdone[s]), kInferEpiWarps);
+            mbar_init(smem_u32(&pready[s]), kInferEpiWarps);
+        }
         for (int s = 0; s < kIWSlots; ++s) {
             mbar_init(smem_u32(&wfull[s]), 1);
             mbar_init(smem_u32(&wempty[s]), 1);
         }
+        mbar_init(smem_u32(&drain), 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {  // two accumulators of 256 fp32 columns
+    if (warp == 0) {  // one accumulator of 256 fp32 columns per tile slot
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_slot)),
                      "r"(512u)
@@ -533,14 +546,13 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         atomicExch(a.err, code);
     };
 
-    // producer bookkeeping for the teardown drain
-    int last_round[kIWSlots] = {-1, -1, -1, -1};
-    int x_loads = 0;
+    // bookkeeping for the teardown drain
+    int last_round[kIWSlots] = {-1, -1};
+    int64_t x_last[kTileSlots] = {-1, -1};
 
     if (warp == kProducerWarp) {
         if (lane == 0) {
             uint32_t wl = 0;
-            int it = 0;
             auto load_w = [&](const CUtensorMap* m, int kx) -> bool {
                 const uint32_t s = wl % kIWSlots, round = wl / kIWSlots;
                 if (round > 0 && !mbar_wait(smem_u32(&wempty[s]), (round - 1) & 1)) return false;
@@ -550,29 +562,45 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 ++wl;
                 return true;
             };
-            for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+            for (int64_t i0 = 0; i0 < my_tiles; i0 += 2) {
                 if (abort_flag) break;
-                if (it > 0 && !mbar_wait(smem_u32(&xempty), (it - 1) & 1)) {
-                    fail(21);
-                    break;
-                }
-                mbar_expect_tx(smem_u32(&xfull), kABytes);
-                tma_load_2d(smem_u32(xbuf), &tx, 0, static_cast<int>(t * kBM), smem_u32(&xfull));
-                ++x_loads;
-                bool ok = load_w(&tw1, 0);
-                for (int kb = 0; ok && kb < 4; ++kb) ok = load_w(&tw2, kb * kBK);
-                for (int kb = 0; ok && kb < 4; ++kb) ok = load_w(&tw3, kb * kBK);
+                const int nt = (my_tiles - i0) >= 2 ? 2 : 1;
+                // the MMA issuer's order: each layer for tile A, then tile B
+                bool ok = true;
+                for (int k = 0; ok && k < nt; ++k) ok = load_w(&tw1, 0);
+                for (int k = 0; ok && k < nt; ++k)
+                    for (int kb = 0; ok && kb < 4; ++kb) ok = load_w(&tw2, kb * kBK);
+                for (int k = 0; ok && k < nt; ++k)
+                    for (int kb = 0; ok && kb < 4; ++kb) ok = load_w(&tw3, kb * kBK);
                 if (!ok) {
                     fail(22);
                     break;
                 }
             }
         }
+    } else if (warp == kXWarp) {
+        if (lane == 0) {
+            for (int64_t i = 0; i < my_tiles; ++i) {
+                if (abort_flag) break;
+                const int s = static_cast<int>(i & 1);
+                const int64_t u = i >> 1;
+                // the slot's previous tile's layer-3 MMAs, the last readers of
+                // its buffer, have completed (one slotfree phase per tile)
+                if (u > 0 && !mbar_wait(smem_u32(&slotfree[s]), static_cast<uint32_t>((u - 1) & 1))) {
+                    fail(21);
+                    break;
+                }
+                mbar_expect_tx(smem_u32(&xfull[s]), kABytes);
+                const int64_t t = blockIdx.x + i * gridDim.x;
+                tma_load_2d(smem_u32(hbufs + s * kHBytes), &tx, 0, static_cast<int>(t * kBM),
+                            smem_u32(&xfull[s]));
+                x_last[s] = u;
+            }
+        }
     } else if (warp == kMmaWarp) {
         if (lane == 0) {
             constexpr uint32_t idesc = idesc_bf16<256>();
-            uint32_t wc = 0, L = 0, hp = 0;
-            int it = 0;
+            uint32_t wc = 0;
             // one k-block of W from the ring into accumulator acc
             auto mma_kblock = [&](uint32_t acc, uint32_t sa, bool first) -> bool {
                 const uint32_t s = wc % kIWSlots;
@@ -587,37 +615,37 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 ++wc;
                 return true;
             };
-            for (int64_t t = blockIdx.x; t < n_tiles; t += gridDim.x, ++it) {
+            bool ok = true;
+            for (int64_t i0 = 0; ok && i0 < my_tiles; i0 += 2) {
                 if (abort_flag) break;
-                if (!mbar_wait(smem_u32(&xfull), it & 1)) {
-                    fail(23);
-                    break;
-                }
-                // layer 1 (K = 64)
-                uint32_t acc = tmem + (L & 1) * 256;
-                if (!mma_kblock(acc, smem_u32(xbuf), true)) {
-                    fail(24);
-                    break;
-                }
-                umma_commit(smem_u32(&xempty));
-                umma_commit(smem_u32(&accfull[L & 1]));
-                ++L;
-                // layers 2 and 3, k-block by k-block behind the epilogue
-                bool ok = true;
-                for (int l = 1; ok && l <= 2; ++l) {
-                    acc = tmem + (L & 1) * 256;
-                    for (int kb = 0; ok && kb < 4; ++kb) {
-                        ok = mbar_wait(smem_u32(&hfull[kb]), hp & 1);
-                        if (ok) ok = mma_kblock(acc, smem_u32(hbuf + kb * kABytes), kb == 0);
+                const int nt = (my_tiles - i0) >= 2 ? 2 : 1;
+                const int64_t u = i0 >> 1;
+                for (int l = 0; ok && l < 3; ++l) {
+                    for (int s = 0; ok && s < nt; ++s) {
+                        const uint32_t acc = tmem + s * 256;
+                        const uint8_t* hb = hbufs + s * kHBytes;
+                        if (l == 0) {
+                            // the slot's input rows, and its previous tile's
+                            // head done reading the accumulator
+                            ok = mbar_wait(smem_u32(&xfull[s]), static_cast<uint32_t>(u & 1));
+                            if (ok && u > 0)
+                                ok = mbar_wait(smem_u32(&hdone[s]), static_cast<uint32_t>((3 * u - 1) & 1));
+                            fence_after();
+                            if (ok) ok = mma_kblock(acc, smem_u32(hb), true);  // K = 64
+                        } else {
+                            // layer l's activations written (and its
+                            // accumulator read) by every epilogue warp
+                            ok = mbar_wait(smem_u32(&hdone[s]), static_cast<uint32_t>((3 * u + l - 1) & 1));
+                            fence_after();
+                            for (int kb = 0; ok && kb < 4; ++kb)
+                                ok = mma_kblock(acc, smem_u32(hb + kb * kABytes), kb == 0);
+                        }
+                        if (!ok) break;
+                        umma_commit(smem_u32(&accfull[s]));
+                        if (l == 2) umma_commit(smem_u32(&slotfree[s]));
                     }
-                    ++hp;
-                    if (ok) umma_commit(smem_u32(&accfull[L & 1]));
-                    ++L;
                 }
-                if (!ok) {
-                    fail(25);
-                    break;
-                }
+                if (!ok) fail(24);
             }
         }
     } else {
@@ -636,85 +664,95 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         const int r = q * 32 + lane;
         const uint32_t lane_off = static_cast<uint32_t>(q * 32) << 16;
         const float b4 = __ldg(a.b4);
-        uint32_t L = 0;
-        int it = 0;
         bool ok = true;
-        for (int64_t t = blockIdx.x; ok && t < n_tiles; t += gridDim.x, ++it) {
-            for (int l = 0; ok && l < 3; ++l, ++L) {
-                const uint32_t acc = tmem + (L & 1) * 256 + lane_off;
-                ok = warp_wait(smem_u32(&accfull[L & 1]), (L >> 1) & 1);
-                fence_after();
-                if (!ok) {
-                    if (lane == 0) fail(26);
-                    break;
-                }
-                if (l < 2) {
-                    const float* bias = l == 0 ? sb1 : sb2;
+        for (int64_t i0 = 0; ok && i0 < my_tiles; i0 += 2) {
+            const int nt = (my_tiles - i0) >= 2 ? 2 : 1;
+            const int64_t u = i0 >> 1;
+            for (int l = 0; ok && l < 3; ++l) {
+                for (int s = 0; ok && s < nt; ++s) {
+                    const uint32_t acc = tmem + s * 256 + lane_off;
+                    ok = warp_wait(smem_u32(&accfull[s]), static_cast<uint32_t>((3 * u + l) & 1));
+                    fence_after();
+                    if (!ok) {
+                        if (lane == 0) fail(26);
+                        break;
+                    }
+                    if (l < 2) {
+                        const float* bias = l == 0 ? sb1 : sb2;
+                        uint8_t* hbuf = hbufs + s * kHBytes;
 #pragma unroll
-                    for (int kb = 0; kb < 4; ++kb) {
-                        const int col0 = kb * 64 + g * 16;
-                        uint32_t u[16];
-                        tmem_ld16_async(acc + col0, u);
-                        tmem_wait_ld();
-                        float v[16];
+                        for (int kb = 0; kb < 4; ++kb) {
+                            const int col0 = kb * 64 + g * 16;
+                            uint32_t uu[16];
+                            tmem_ld16_async(acc + col0, uu);
+                            tmem_wait_ld();
+                            float v[16];
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            float hz, t;
-                            v[j] = silu_from_acc(__uint_as_float(u[j]), bias[col0 + j], hz, t);
+                            for (int j = 0; j < 16; ++j) {
+                                float hz, t;
+                                v[j] = silu_from_acc(__uint_as_float(uu[j]), bias[col0 + j], hz, t);
+                            }
+                            store_h16_sw128(hbuf, r, col0, v);
                         }
-                        store_h16_sw128(hbuf, r, col0, v);
                         // the shared stores to the tensor core's (async) proxy,
                         // the TMEM reads before the hand-off
                         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                         fence_before();
                         __syncwarp();
-                        if (lane == 0) mbar_arrive(smem_u32(&hfull[kb]));
-                    }
-                } else {
-                    // head: this warp's chain over columns 64 kb + 16 g + j
-                    float p = 0.0f;
+                        if (lane == 0) mbar_arrive(smem_u32(&hdone[s]));
+                    } else {
+                        // head: this warp's chain over columns 64 kb + 16 g + j
+                        float p = 0.0f;
 #pragma unroll
-                    for (int kb = 0; kb < 4; ++kb) {
-                        const int col0 = kb * 64 + g * 16;
-                        uint32_t u[16];
-                        tmem_ld16_async(acc + col0, u);
-                        tmem_wait_ld();
+                        for (int kb = 0; kb < 4; ++kb) {
+                            const int col0 = kb * 64 + g * 16;
+                            uint32_t uu[16];
+                            tmem_ld16_async(acc + col0, uu);
+                            tmem_wait_ld();
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            float hz, t;
-                            const float h = silu_from_acc(__uint_as_float(u[j]), sb3[col0 + j], hz, t);
-                            p = fmaf(h, sw4[col0 + j], p);
+                            for (int j = 0; j < 16; ++j) {
+                                float hz, t;
+                                const float h = silu_from_acc(__uint_as_float(uu[j]), sb3[col0 + j], hz, t);
+                                p = fmaf(h, sw4[col0 + j], p);
+                            }
                         }
-                    }
-                    part[g][r] = p;
-                    fence_before();
-                    __syncwarp();
-                    if (lane == 0) mbar_arrive(smem_u32(&pready));
-                    if (g == 0) {
-                        ok = warp_wait(smem_u32(&pready), it & 1);
-                        if (!ok) {
-                            if (lane == 0) fail(27);
-                            break;
+                        // the accumulator is read: the slot's next tile may
+                        // start its layer 1
+                        fence_before();
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(smem_u32(&hdone[s]));
+                        part[s][g][r] = p;
+                        __syncwarp();
+                        if (lane == 0) mbar_arrive(smem_u32(&pready[s]));
+                        if (g == 0) {
+                            ok = warp_wait(smem_u32(&pready[s]), static_cast<uint32_t>(u & 1));
+                            if (!ok) {
+                                if (lane == 0) fail(27);
+                                break;
+                            }
+                            const float y =
+                                (((part[s][0][r] + part[s][1][r]) + part[s][2][r]) + part[s][3][r]) + b4;
+                            const int64_t row = (blockIdx.x + (i0 + s) * gridDim.x) * kBM + r;
+                            if (row < a.n) a.y[row] = a.base ? y + __ldg(a.base + row) : y;
                         }
-                        const float y = (((part[0][r] + part[1][r]) + part[2][r]) + part[3][r]) + b4;
-                        const int64_t row = t * kBM + r;
-                        if (row < a.n) a.y[row] = a.base ? y + __ldg(a.base + row) : y;
                     }
                 }
             }
         }
     }
 
-    // Teardown.  After an abort: the producer waits (bounded) for the loads
-    // it issued, the MMA issuer for its MMAs (a commit on `drain`), then the
-    // accumulators are freed.
+    // Teardown.  After an abort: the producer and the input loader wait
+    // (bounded) for the loads they issued, the MMA issuer for its MMAs (a
+    // commit on `drain`), then the accumulators are freed.
     fence_before();
     __syncthreads();
     if (abort_flag) {
         if (warp == kProducerWarp && lane == 0) {
             for (int s = 0; s < kIWSlots; ++s)
                 if (last_round[s] >= 0) mbar_wait(smem_u32(&wfull[s]), last_round[s] & 1);
-            if (x_loads > 0) mbar_wait(smem_u32(&xfull), (x_loads - 1) & 1);
+        } else if (warp == kXWarp && lane == 0) {
+            for (int s = 0; s < kTileSlots; ++s)
+                if (x_last[s] >= 0) mbar_wait(smem_u32(&xfull[s]), static_cast<uint32_t>(x_last[s] & 1));
         } else if (warp == kMmaWarp && lane == 0) {
             umma_commit(smem_u32(&drain));
             mbar_wait(smem_u32(&drain), 0);
