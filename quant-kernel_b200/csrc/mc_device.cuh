@@ -53,6 +53,17 @@ __device__ __forceinline__ float ptx_max_nan(float a, float b) {
 }
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 
+// Packed FP32 pairs (sm_100 f32x2 FMA / multiply / add: one instruction for
+// both lanes, each lane rounded exactly as its scalar form), used where two
+// units of a thread take the same operation: same bits as the scalar code,
+// fewer issued instructions.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+
 // ---------------------------------------------------------------------------
 // Philox4x32-10 (Salmon et al., SC'11).  Counter (c0, c1, 0, c3), key = seed.
 // ---------------------------------------------------------------------------
@@ -140,6 +151,23 @@ __device__ __forceinline__ void box_muller_parts(uint32_t ub, uint32_t gb, float
     s = ptx_sin(ang);
 }
 
+// box_muller_parts for two units at once (lane 0: ub0, gb0; lane 1: ub1,
+// gb1), the uniform's subtraction and the angle's FMA as packed pairs.
+template <int K>
+__device__ __forceinline__ void box_muller_parts2(uint32_t ub0, uint32_t gb0, uint32_t ub1,
+                                                  uint32_t gb1, float2& w, float2& c, float2& s) {
+    constexpr float kTwoPi = 6.28318530717958647692f;
+    constexpr float kOff = (float)(3.14159265358979323846 * (3.0 - 1.0 / (double)(1u << K)));
+    const float2 u = add2(f2(__uint_as_float(0x3F800000u | ub0), __uint_as_float(0x3F800000u | ub1)),
+                          f2(-0x1.fffffep-1f));
+    const float2 y = f2(__uint_as_float(0x3F800000u | (gb0 << (23 - K))),
+                        __uint_as_float(0x3F800000u | (gb1 << (23 - K))));
+    w = f2(-ptx_lg2(u.x), -ptx_lg2(u.y));
+    const float2 ang = fma2(y, f2(kTwoPi), f2(-kOff));
+    c = f2(ptx_cos(ang.x), ptx_cos(ang.y));
+    s = f2(ptx_sin(ang.x), ptx_sin(ang.y));
+}
+
 // The normals of box_muller_parts divided by kBmRadius (the callers fold that
 // factor into their step constants, which saves a multiply per pair):
 //   za = sqrt(w) c,  zb = sqrt(w) s.
@@ -179,6 +207,28 @@ struct Philox6 {
             box_muller_parts<18>(x.z >> 9, (x.x & 0x1FFu) | ((x.y & 0x1FFu) << 9), w, c, s);
     }
 };
+
+// parts() of pair p for two units' calls a (lane 0) and b (lane 1).
+__device__ __forceinline__ void philox6_parts2(const Philox6& a, const Philox6& b, int p, float2& w,
+                                               float2& c, float2& s) {
+    if (p == 0)
+        box_muller_parts2<16>(a.x.x >> 9, a.x.w & 0xFFFFu, b.x.x >> 9, b.x.w & 0xFFFFu, w, c, s);
+    else if (p == 1)
+        box_muller_parts2<16>(a.x.y >> 9, a.x.w >> 16, b.x.y >> 9, b.x.w >> 16, w, c, s);
+    else
+        box_muller_parts2<18>(a.x.z >> 9, (a.x.x & 0x1FFu) | ((a.x.y & 0x1FFu) << 9), b.x.z >> 9,
+                              (b.x.x & 0x1FFu) | ((b.x.y & 0x1FFu) << 9), w, c, s);
+}
+
+// pair() of pair p for two units' calls a (lane 0) and b (lane 1).
+__device__ __forceinline__ void philox6_pair2(const Philox6& a, const Philox6& b, int p, float2& za,
+                                              float2& zb) {
+    float2 w, c, s;
+    philox6_parts2(a, b, p, w, c, s);
+    const float2 rad = f2(ptx_sqrt(w.x), ptx_sqrt(w.y));
+    za = mul2(rad, c);
+    zb = mul2(rad, s);
+}
 
 // ---------------------------------------------------------------------------
 // Double-double accumulation (Knuth TwoSum).  A non-finite sum drops its error

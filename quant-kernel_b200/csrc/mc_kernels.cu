@@ -169,6 +169,18 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
         su[k] = 1.0f;
         sd[k] = 1.0f;
     }
+    // PK: units 2p and 2p + 1 of the thread form one packed pair (lane 0, lane
+    // 1) for every multiply and FMA of the step; the floors stay per lane.
+    // Same operations in the same order as the scalar step, so the same bits.
+    constexpr bool PK = (UPT % 2) == 0;
+    constexpr int NP = PK ? UPT / 2 : 1;
+    float2 su2[NP], sd2[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        su2[p] = f2(1.0f);
+        sd2[p] = f2(1.0f);
+    }
+    const float2 m02 = f2(m0), b2 = f2(b), c2 = f2(c);
     // steps <= kMaxSteps (checked when packing), so j0 + 12 never wraps
     uint32_t blk = 0;  // step block j / 6
     for (int32_t j0 = 0; j0 < steps; j0 += 6 * SU, blk += SU) {
@@ -184,27 +196,65 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
             const int32_t j = j0 + 6 * sb;
             const Philox6 (&r)[UPT] = rb[sb];
             const int32_t m = (steps - j) < 6 ? (steps - j) : 6;
-            float zp[UPT][2];
+            if constexpr (PK) {
+                float2 zp2[NP][2];
 #pragma unroll
-            for (int s = 0; s < 6; ++s) {
-                if (s < m) {
+                for (int s = 0; s < 6; ++s) {
+                    if (s < m) {
 #pragma unroll
-                    for (int k = 0; k < UPT; ++k) {
-                        if ((s & 1) == 0) r[k].pair(s >> 1, zp[k][0], zp[k][1]);
-                        const float zz = zp[k][s & 1];
-                        float iu, id;
-                        if (MIL) {
-                            iu = fma_rn(fma_rn(c, zz, b), zz, m0);
-                            id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
-                        } else {
-                            iu = fma_rn(b, zz, m0);
-                            id = fma_rn(-b, zz, m0);
+                        for (int p = 0; p < NP; ++p) {
+                            if ((s & 1) == 0)
+                                philox6_pair2(r[2 * p], r[2 * p + 1], s >> 1, zp2[p][0], zp2[p][1]);
+                            const float2 zz = zp2[p][s & 1];
+                            float2 iu, id;
+                            if (MIL) {
+                                iu = fma2(fma2(c2, zz, b2), zz, m02);
+                                id = fma2(fma2(neg2(c2), zz, b2), neg2(zz), m02);
+                            } else {
+                                iu = fma2(b2, zz, m02);
+                                id = fma2(neg2(b2), zz, m02);
+                            }
+                            const float2 u = fma2(su2[p], iu, su2[p]);
+                            su2[p] = f2(fmaxf(u.x, fl), fmaxf(u.y, fl));
+                            if (ANTI) {
+                                const float2 d = fma2(sd2[p], id, sd2[p]);
+                                sd2[p] = f2(fmaxf(d.x, fl), fmaxf(d.y, fl));
+                            }
                         }
-                        su[k] = fmaxf(fma_rn(su[k], iu, su[k]), fl);
-                        if (ANTI) sd[k] = fmaxf(fma_rn(sd[k], id, sd[k]), fl);
+                    }
+                }
+            } else {
+                float zp[UPT][2];
+#pragma unroll
+                for (int s = 0; s < 6; ++s) {
+                    if (s < m) {
+#pragma unroll
+                        for (int k = 0; k < UPT; ++k) {
+                            if ((s & 1) == 0) r[k].pair(s >> 1, zp[k][0], zp[k][1]);
+                            const float zz = zp[k][s & 1];
+                            float iu, id;
+                            if (MIL) {
+                                iu = fma_rn(fma_rn(c, zz, b), zz, m0);
+                                id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
+                            } else {
+                                iu = fma_rn(b, zz, m0);
+                                id = fma_rn(-b, zz, m0);
+                            }
+                            su[k] = fmaxf(fma_rn(su[k], iu, su[k]), fl);
+                            if (ANTI) sd[k] = fmaxf(fma_rn(sd[k], id, sd[k]), fl);
+                        }
                     }
                 }
             }
+        }
+    }
+    if constexpr (PK) {
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            su[2 * p] = su2[p].x;
+            su[2 * p + 1] = su2[p].y;
+            sd[2 * p] = sd2[p].x;
+            sd[2 * p + 1] = sd2[p].y;
         }
     }
     const uint32_t n_pairs = (uint32_t)o.paths >> 1;
@@ -275,6 +325,22 @@ __device__ __forceinline__ void sim_heston_form(const McOption& o, uint32_t unit
         vd[k] = v0;
         zfirst[k] = 0.0f;
     }
+    // PK: units 2p and 2p + 1 of the thread form one packed pair (lane 0, lane
+    // 1) for every multiply and FMA of the step; the square roots and the
+    // floors stay per lane.  Same operations in the same order as the scalar
+    // step, so the same bits.
+    constexpr bool PK = (UPT % 2) == 0;
+    constexpr int NP = PK ? UPT / 2 : 1;
+    float2 xu2[NP], vu2[NP], xd2[NP], vd2[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        xu2[p] = f2(0.0f);
+        xd2[p] = f2(0.0f);
+        vu2[p] = f2(v0);
+        vd2[p] = f2(v0);
+    }
+    const float2 sqdt2 = f2(sqdt), xr2 = f2(xr), xc2 = f2(xc), nhdt2 = f2(-hdt), omk2 = f2(omk),
+                 kth2 = f2(kth), cmu2 = f2(cmu);
     // steps <= kMaxSteps (checked when packing), so j0 + 6 never wraps
     uint32_t blk = 0;  // step block j / 3
     for (int32_t j0 = 0; j0 < steps; j0 += 3 * SU, blk += SU) {
@@ -294,35 +360,77 @@ __device__ __forceinline__ void sim_heston_form(const McOption& o, uint32_t unit
             for (int s = 0; s < 3; ++s) {
                 if (s < m) {
                     if (DF) fl -= cmu;  // the floor of y after this step
+                    if constexpr (PK) {
+                        const float flo = DF ? fl : xfl;
 #pragma unroll
-                    for (int k = 0; k < UPT; ++k) {
-                        // z1 = kBmRadius sqrt(w) c, z2 = kBmRadius sqrt(w) s; the
-                        // step needs sqrt(v) z1 and sqrt(v) z2 only, so sqrt(w)
-                        // joins the variance's square root: sqrt(v w)
-                        float w, c1, s1;
-                        r[k].parts(s, w, c1, s1);
-                        if (LR && j == 0 && s == 0) zfirst[k] = ptx_sqrt(w) * c1;
-                        const float sz1 = sqdt * c1;
-                        const float xw = fma_rn(xr, c1, xc * s1);
-                        {
-                            const float sv = ptx_sqrt(vu[k] * w);
-                            if (DF)
-                                xu[k] = ptx_max_nan(fma_rn(sv, sz1, fma_rn(-hdt, vu[k], xu[k])), fl);
-                            else
-                                xu[k] = ptx_max_nan(xu[k] + fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu)), xfl);
-                            vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
+                        for (int p = 0; p < NP; ++p) {
+                            float2 w, c1, s1;
+                            philox6_parts2(r[2 * p], r[2 * p + 1], s, w, c1, s1);
+                            if (LR && j == 0 && s == 0) {
+                                zfirst[2 * p] = ptx_sqrt(w.x) * c1.x;
+                                zfirst[2 * p + 1] = ptx_sqrt(w.y) * c1.y;
+                            }
+                            const float2 sz1 = mul2(sqdt2, c1);
+                            const float2 xw = fma2(xr2, c1, mul2(xc2, s1));
+                            {
+                                const float2 q = mul2(vu2[p], w);
+                                const float2 sv = f2(ptx_sqrt(q.x), ptx_sqrt(q.y));
+                                const float2 x = DF ? fma2(sv, sz1, fma2(nhdt2, vu2[p], xu2[p]))
+                                                    : add2(xu2[p], fma2(sv, sz1, fma2(nhdt2, vu2[p], cmu2)));
+                                xu2[p] = f2(ptx_max_nan(x.x, flo), ptx_max_nan(x.y, flo));
+                                const float2 v = fma2(sv, xw, fma2(vu2[p], omk2, kth2));
+                                vu2[p] = f2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
+                            }
+                            if (ANTI) {
+                                const float2 q = mul2(vd2[p], w);
+                                const float2 sv = f2(ptx_sqrt(q.x), ptx_sqrt(q.y));
+                                const float2 x = DF ? fma2(sv, neg2(sz1), fma2(nhdt2, vd2[p], xd2[p]))
+                                                    : add2(xd2[p], fma2(sv, neg2(sz1), fma2(nhdt2, vd2[p], cmu2)));
+                                xd2[p] = f2(ptx_max_nan(x.x, flo), ptx_max_nan(x.y, flo));
+                                const float2 v = fma2(sv, neg2(xw), fma2(vd2[p], omk2, kth2));
+                                vd2[p] = f2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
+                            }
                         }
-                        if (ANTI) {
-                            const float sv = ptx_sqrt(vd[k] * w);
-                            if (DF)
-                                xd[k] = ptx_max_nan(fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], xd[k])), fl);
-                            else
-                                xd[k] = ptx_max_nan(xd[k] + fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu)), xfl);
-                            vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < UPT; ++k) {
+                            // z1 = kBmRadius sqrt(w) c, z2 = kBmRadius sqrt(w) s; the
+                            // step needs sqrt(v) z1 and sqrt(v) z2 only, so sqrt(w)
+                            // joins the variance's square root: sqrt(v w)
+                            float w, c1, s1;
+                            r[k].parts(s, w, c1, s1);
+                            if (LR && j == 0 && s == 0) zfirst[k] = ptx_sqrt(w) * c1;
+                            const float sz1 = sqdt * c1;
+                            const float xw = fma_rn(xr, c1, xc * s1);
+                            {
+                                const float sv = ptx_sqrt(vu[k] * w);
+                                if (DF)
+                                    xu[k] = ptx_max_nan(fma_rn(sv, sz1, fma_rn(-hdt, vu[k], xu[k])), fl);
+                                else
+                                    xu[k] = ptx_max_nan(xu[k] + fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu)), xfl);
+                                vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
+                            }
+                            if (ANTI) {
+                                const float sv = ptx_sqrt(vd[k] * w);
+                                if (DF)
+                                    xd[k] = ptx_max_nan(fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], xd[k])), fl);
+                                else
+                                    xd[k] = ptx_max_nan(xd[k] + fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu)), xfl);
+                                vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
+                            }
                         }
                     }
                 }
             }
+        }
+    }
+    if constexpr (PK) {
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            xu[2 * p] = xu2[p].x;
+            xu[2 * p + 1] = xu2[p].y;
+            xd[2 * p] = xd2[p].x;
+            xd[2 * p + 1] = xd2[p].y;
         }
     }
     const uint32_t n_pairs = (uint32_t)o.paths >> 1;

@@ -134,6 +134,14 @@ __device__ __forceinline__ float silu_from_acc(float acc, float half_bias, float
     return fmaf(hz, t, hz);
 }
 
+// silu_from_acc on two adjacent columns, the two FMAs as packed f32x2
+// operations (each lane rounded as the scalar fmaf: the same bits).
+__device__ __forceinline__ float2 silu2_from_acc(float2 acc, float2 half_bias) {
+    const float2 hz = __ffma2_rn(acc, make_float2(0.5f, 0.5f), half_bias);
+    const float2 t = make_float2(tanh_approx(hz.x), tanh_approx(hz.y));
+    return __ffma2_rn(hz, t, hz);
+}
+
 // 32 bf16 values to 64 contiguous bytes.
 __device__ __forceinline__ void store_bf16x32(__nv_bfloat16* dst, const float (&v)[32]) {
     uint4* d = reinterpret_cast<uint4*>(dst);
@@ -496,7 +504,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     __shared__ __align__(8) uint64_t xfull[kTileSlots], slotfree[kTileSlots], accfull[kTileSlots];
     __shared__ __align__(8) uint64_t hdone[kTileSlots], pready[kTileSlots];
     __shared__ __align__(8) uint64_t wfull[kIWSlots], wempty[kIWSlots], drain;
-    __shared__ float sb1[kSurHidden], sb2[kSurHidden], sb3[kSurHidden], sw4[kSurHidden];
+    __shared__ __align__(16) float sb1[kSurHidden], sb2[kSurHidden], sb3[kSurHidden], sw4[kSurHidden];
     __shared__ float part[kTileSlots][4][kBM];  // head partial sums per slot and column group
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
@@ -688,9 +696,12 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                             tmem_wait_ld();
                             float v[16];
 #pragma unroll
-                            for (int j = 0; j < 16; ++j) {
-                                float hz, t;
-                                v[j] = silu_from_acc(__uint_as_float(uu[j]), bias[col0 + j], hz, t);
+                            for (int j = 0; j < 16; j += 2) {
+                                const float2 h = silu2_from_acc(
+                                    make_float2(__uint_as_float(uu[j]), __uint_as_float(uu[j + 1])),
+                                    *reinterpret_cast<const float2*>(bias + col0 + j));
+                                v[j] = h.x;
+                                v[j + 1] = h.y;
                             }
                             store_h16_sw128(hbuf, r, col0, v);
                         }
