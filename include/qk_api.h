@@ -238,8 +238,9 @@ QK_EXPORT int32_t qk_get_device(int32_t* device);
                                       * QK_PLAN_PERSISTENT is given) */
 #define QK_PLAN_FAMILY_GRIDS  0x20 /* several model families: one grid per family group,
                                       * back to back, instead of the persistent kernel */
-#define QK_PLAN_STEP_UNROLL2  0x40 /* stepwise single-family plans at 1 or 2 units per
-                                      * thread: two Philox step blocks per loop iteration
+#define QK_PLAN_STEP_UNROLL2  0x40 /* stepwise single-family plans (Euler, Milstein and
+                                      * local vol at 1, 2 or 4 units per thread, Heston at
+                                      * 1 or 2): two Philox step blocks per loop iteration
                                       * (same results bit for bit; the autotuner also
                                       * tries it) */
 

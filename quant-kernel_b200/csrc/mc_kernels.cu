@@ -745,8 +745,10 @@ __device__ __noinline__ int64_t run_group(const McOption* __restrict__ opts,
     }
 }
 
+// Seven 128-thread CTAs per SM (72 registers): every family body is compiled
+// within that budget; six (80 registers) and eight (64) measured slower.
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
+__global__ void __launch_bounds__(BLOCK, 896 / BLOCK)
     mc_persistent_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
                          int64_t n_tiles, TilePartial* __restrict__ partials,
                          unsigned long long* __restrict__ work_counter,
@@ -770,17 +772,17 @@ __global__ void __launch_bounds__(BLOCK, 768 / BLOCK)
         tile = run_group<FAM, BLOCK, UPT, ANTI>(opts, tile_begin, lo, hi, th, partials,          \
                                                 work_counter, smem, &s_tile, tile);              \
         break;
-            QK_GROUP(kFamTerminal, kUptTerminal, true)
-            QK_GROUP(kFamTerminal, kUptTerminal, false)
-            QK_GROUP(kFamEuler, kUptStepwise, true)
-            QK_GROUP(kFamEuler, kUptStepwise, false)
-            QK_GROUP(kFamMilstein, kUptStepwise, true)
-            QK_GROUP(kFamMilstein, kUptStepwise, false)
-            QK_GROUP(kFamHeston, kUptHeston, true)
-            QK_GROUP(kFamHeston, kUptHeston, false)
-            QK_GROUP(kFamHestonLr, kUptHeston, true)
-            QK_GROUP(kFamHestonLr, kUptHeston, false)
-            QK_GROUP(kFamVr, kUptVr, false)
+            QK_GROUP(kFamTerminal, kFamilyUpt<kFamTerminal>, true)
+            QK_GROUP(kFamTerminal, kFamilyUpt<kFamTerminal>, false)
+            QK_GROUP(kFamEuler, kFamilyUpt<kFamEuler>, true)
+            QK_GROUP(kFamEuler, kFamilyUpt<kFamEuler>, false)
+            QK_GROUP(kFamMilstein, kFamilyUpt<kFamMilstein>, true)
+            QK_GROUP(kFamMilstein, kFamilyUpt<kFamMilstein>, false)
+            QK_GROUP(kFamHeston, kFamilyUpt<kFamHeston>, true)
+            QK_GROUP(kFamHeston, kFamilyUpt<kFamHeston>, false)
+            QK_GROUP(kFamHestonLr, kFamilyUpt<kFamHestonLr>, true)
+            QK_GROUP(kFamHestonLr, kFamilyUpt<kFamHestonLr>, false)
+            QK_GROUP(kFamVr, kFamilyUpt<kFamVr>, false)
 #undef QK_GROUP
             default:
                 tile = n_tiles;  // unknown code: the host never builds one
@@ -891,17 +893,19 @@ constexpr bool is_stepwise(int family) {
            family == kFamHestonLr;
 }
 
-// Step unrolling 2 is compiled for the stepwise families at 1 and 2 units per
-// thread (4 units x 2 blocks of Philox words would exceed the register file
-// share that keeps 4+ CTAs resident).
+// Step unrolling 2 where step_unroll2_compiled() says so.
 template <int FAMILY, int BLOCK, bool ANTI>
 cudaError_t launch_upt(int upt, int su, const SimArgs& a, cudaStream_t st) {
     if constexpr (is_stepwise(FAMILY)) {
         if (su == 2) {
+            if (!step_unroll2_compiled(FAMILY, upt)) return cudaErrorInvalidValue;
             switch (upt) {
                 case 1: return launch_one<FAMILY, BLOCK, 1, ANTI, 2>(a, st);
                 case 2: return launch_one<FAMILY, BLOCK, 2, ANTI, 2>(a, st);
-                default: return cudaErrorInvalidValue;
+                default:
+                    if constexpr (step_unroll2_compiled(FAMILY, 4))
+                        return launch_one<FAMILY, BLOCK, 4, ANTI, 2>(a, st);
+                    return cudaErrorInvalidValue;
             }
         }
     }

@@ -20,15 +20,45 @@ enum : int {
     kNumFamilies = 6
 };
 
-// Units per thread compiled into the persistent mixed-model kernel.
+// Units per thread compiled into the persistent mixed-model kernel (and used
+// by the per-family grids of a mixed plan).  The stepwise families take four:
+// with the persistent kernel's 72-register budget (seven 128-thread CTAs per
+// SM) the mixed benchmark batch took 52.9 ms, against 53.5 ms at six CTAs per
+// SM and 56.1 ms with two stepwise units per thread; Heston keeps two, whose
+// four-unit body needs 93 registers.
+// Results do not depend on these (tile sums are exact double-double sums
+// merged in a fixed order).
 constexpr int kUptTerminal = 1;
-constexpr int kUptStepwise = 2;
+constexpr int kUptStepwise = 4;
 constexpr int kUptHeston = 2;
 constexpr int kUptVr = 1;
+
+// The one family -> units-per-thread map: the persistent kernel's family
+// bodies, the tiling of every mixed plan and the default single-family
+// tiling all take it, so a mixed launch and the per-method calls tile each
+// option alike and give the same bits.
+constexpr int family_upt(int family) {
+    return family == kFamTerminal ? kUptTerminal
+         : family == kFamVr ? kUptVr
+         : (family == kFamHeston || family == kFamHestonLr) ? kUptHeston
+         : kUptStepwise;
+}
+template <int FAMILY>
+constexpr int kFamilyUpt = family_upt(FAMILY);  // the same, as a compile-time constant for kernels
 
 inline bool family_is_stepwise(int family) {
     return family == kFamEuler || family == kFamMilstein || family == kFamHeston ||
            family == kFamHestonLr;
+}
+
+// Two Philox step blocks per loop iteration (step unrolling 2) are compiled
+// for the stepwise families at 1 and 2 units per thread, and for the
+// one-factor families also at 4 (their default tiling); Heston's four-unit
+// body has no registers to spare for a second block of Philox words.
+constexpr bool step_unroll2_compiled(int family, int upt) {
+    return (family == kFamEuler || family == kFamMilstein) ? (upt == 1 || upt == 2 || upt == 4)
+         : (family == kFamHeston || family == kFamHestonLr) ? (upt == 1 || upt == 2)
+         : false;
 }
 
 struct SimArgs {

@@ -74,13 +74,7 @@ void set_const(McOption& o, double price) {
 int32_t geti(const int32_t* a, int32_t i, int32_t dflt) { return a ? a[i] : dflt; }
 
 int upt_for(int family, bool persistent, const LaunchConfig& cfg) {
-    if (!persistent) return cfg.upt;
-    switch (family) {
-        case kFamTerminal: return kUptTerminal;
-        case kFamHeston: return kUptHeston;
-        case kFamVr: return kUptVr;
-        default: return kUptStepwise;
-    }
+    return persistent ? family_upt(family) : cfg.upt;
 }
 
 struct DeviceGuard {
@@ -333,12 +327,12 @@ void PinnedBuf::release() {
 // steps) block 128 ran 2.4% faster than 256 with the same registers (six CTAs
 // of 128 per SM instead of three of 256: finer tiles, a shorter tail), and the
 // autotuner picked it for the mixed-model batch too.  One block size for every
-// family keeps the persistent and single-family tilings identical, so both
-// give the same bits.
+// family, and each family's units per thread from family_upt(), keep the
+// persistent and single-family tilings identical, so both give the same bits.
 LaunchConfig default_config(int family) {
     LaunchConfig c;
     c.block = 128;
-    c.upt = (family == kFamTerminal || family == kFamVr) ? 1 : 2;
+    c.upt = family_upt(family);
     return c;
 }
 
@@ -369,7 +363,7 @@ void load_tune_file_locked() {
         if (std::sscanf(line, "%511s %d %d %d", key, &block, &upt, &su) < 3) continue;
         if ((block == 128 || block == 256) &&
             (upt == 1 || upt == 2 || upt == 4 || upt == kUptPersistent || upt == kUptFamilyGrids) &&
-            (su == 1 || (su == 2 && (upt == 1 || upt == 2))))
+            (su == 1 || (su == 2 && (upt == 1 || upt == 2 || upt == 4))))
             tune_map()[key] = LaunchConfig{block, upt, su};
     }
     std::fclose(f);
@@ -499,11 +493,10 @@ cudaError_t Plan::build(const BatchInput& in, int32_t flags, std::string* err) {
         if (!persistent_ || (tuned.upt <= 0 && !(flags & (kFlagPersistent | kFlagFamilyGrids))))
             cfg_.upt = tuned.upt;
         if (persistent_ && cfg_.upt > 0) cfg_.upt = kUptPersistent;
-        cfg_.su = (!persistent_ && family_is_stepwise(family_)) ? tuned.su : 1;
+        cfg_.su = (!persistent_ && step_unroll2_compiled(family_, cfg_.upt)) ? tuned.su : 1;
     }
     // QK_PLAN_STEP_UNROLL2: two step blocks per loop iteration where compiled
-    if ((flags & kFlagStepUnroll2) && !persistent_ && family_is_stepwise(family_) &&
-        (cfg_.upt == 1 || cfg_.upt == 2))
+    if ((flags & kFlagStepUnroll2) && !persistent_ && step_unroll2_compiled(family_, cfg_.upt))
         cfg_.su = 2;
     e = layout_tiles(cfg_);
     if (e != cudaSuccess) return e;
@@ -869,7 +862,7 @@ cudaError_t Plan::autotune() {
         for (int b : {128, 256})
             for (int u : {1, 2, 4}) {
                 cands.push_back(LaunchConfig{b, u, 1});
-                if (family_is_stepwise(family_) && u <= 2) cands.push_back(LaunchConfig{b, u, 2});
+                if (step_unroll2_compiled(family_, u)) cands.push_back(LaunchConfig{b, u, 2});
             }
     }
     LaunchConfig best = cfg_;
