@@ -68,6 +68,36 @@ STEP_COST = {2: (1, 13), 3: (1, 16), 4: (1, 13), 6: (XU_PER_UNIT, ALU_PER_UNIT)}
 # polynomial of the degree FP64 accuracy needs.)
 FP64_PER_PAIR = 66
 SMS, ISSUE_PER_CLK, XU_PER_CLK, FP64_PER_CLK = 148, 128, 16, 64
+# Per-SM-clock pipe widths the rooflines divide by: the nominal B200 figures,
+# replaced at start-up by the library's throughput probe on the GPU at hand
+# (qk_b200_pipe_probe, include/qk_diag.h) when it runs.
+PIPES = {"issue": float(ISSUE_PER_CLK), "xu": float(XU_PER_CLK), "fp64": float(FP64_PER_CLK),
+         "source": "nominal per-clock SM widths (148 SMs x 128 issue / 16 XU / 64 FP64 lanes per clk)"}
+PROBE_KINDS = (("issue", 1), ("xu", 0), ("fp64", 3), ("ffma2_lanes", 2), ("xu_in_heston_mix", 4))
+
+
+def measure_pipes(qk, device):
+    """Measure the pipe widths on `device` with the library's probe (FP32 FMA
+    lanes = the issue width, MUFU lanes, FP64 FMA lanes, packed-FMA lanes, and
+    MUFU lanes inside a Heston-like instruction mix), in lane-operations per
+    SM per clock, and make them the rooflines' denominators.  Returns the
+    measured dict, or None (and the nominal widths stay) if the probe fails."""
+    import ctypes as ct
+
+    fn = getattr(qk._lib, "qk_b200_pipe_probe", None)
+    if fn is None:
+        return None
+    out = {}
+    for key, kind in PROBE_KINDS:
+        v = ct.c_double(0.0)
+        if fn(int(device), int(kind), ct.byref(v)) != 0 or not v.value > 0:
+            return None
+        out[key] = v.value
+    PIPES.update(issue=out["issue"], xu=out["xu"], fp64=out["fp64"],
+                 source=("measured per-SM-clock widths on this GPU (qk_b200_pipe_probe: "
+                         f"{out['issue']:.1f} FP32 FMA = issue, {out['xu']:.2f} MUFU, "
+                         f"{out['fp64']:.1f} FP64 lanes per clk) x 148 SMs"))
+    return out
 SUR_CHECKPOINT = ROOT / "quant-kernel_b200" / "quantkernel_b200" / "data" / "heston_surrogate.qksur"
 SUR_FLOP_PER_ROW = 2 * (9 * 256 + 256 * 256 * 2 + 256)  # forward multiply-adds x 2
 
@@ -89,6 +119,8 @@ def parse():
     ap.add_argument("--heston-cf", action="store_true",
                     help="Heston characteristic-function leg only")
     ap.add_argument("--cf-options", type=int, default=65536)
+    ap.add_argument("--pipe-probe", action="store_true",
+                    help="print the measured per-SM-clock pipe widths (qk_b200_pipe_probe) and exit")
     ap.add_argument("--mixed", action="store_true",
                     help="mixed-model leg only (with --profile: the first --options options, "
                          "persistent kernel and per-family grids, two executes each)")
@@ -488,6 +520,7 @@ def main_gpu(args):
 
     qk = QuantKernel()
     qk.set_device(local)
+    pipes = measure_pipes(qk, local)  # the rooflines' measured denominators
     # one batch split across all ranks (run first, while every rank still
     # builds plans at the default launch shape: the ranks' tilings must agree)
     strong = None
@@ -582,6 +615,7 @@ def main_gpu(args):
                           "chosen_by": "autotuner (block x paths per thread x step unrolling)"},
         "kernel_ms": sim_ms,
         "measured": {"source": "ncu, profiles/heston_simulate_ncu.md"},
+        "pipe_probe": pipes,
     })
     # DRAM bytes per full launch, from the committed ncu summary (a small case
     # of the same kernel scaled by the option count; see that file)
@@ -593,8 +627,8 @@ def main_gpu(args):
     if "thread_instructions_per_path_step" in m and "xu_per_path_step" in m:
         # the same peaks against this kernel's own (ncu-measured) instruction
         # mix: how close the kernel runs to what its own instructions allow
-        issue_peak = SMS * ISSUE_PER_CLK * f_mhz * 1e6
-        xu_peak = SMS * XU_PER_CLK * f_mhz * 1e6
+        issue_peak = SMS * PIPES["issue"] * f_mhz * 1e6
+        xu_peak = SMS * PIPES["xu"] * f_mhz * 1e6
         own = min(issue_peak / m["thread_instructions_per_path_step"],
                   xu_peak / m["xu_per_path_step"])
         roofline["frac_of_own_mix_bound"] = (units_per_step / (sim_ms / 1e3)) / own
@@ -901,10 +935,10 @@ def _time_plan(plan, stream, flush, reps):
 
 def step_roofline(units_by_model, seconds, f_mhz):
     """Roofline of the stepwise simulate kernels: each model's path-steps at the
-    tighter of its XU and issue bounds (STEP_COST, nominal per-clock SM widths
+    tighter of its XU and issue bounds (STEP_COST, the PIPES per-clock SM widths
     at the sampled SM clock); frac = that bound time / the measured time."""
-    issue_peak = SMS * ISSUE_PER_CLK * f_mhz * 1e6  # thread-instructions/s
-    xu_peak = SMS * XU_PER_CLK * f_mhz * 1e6
+    issue_peak = SMS * PIPES["issue"] * f_mhz * 1e6  # thread-instructions/s
+    xu_peak = SMS * PIPES["xu"] * f_mhz * 1e6
     bound_s, xu_ops, alu_ops, limiters = 0.0, 0.0, 0.0, set()
     for model, units in units_by_model.items():
         xu, alu = STEP_COST[int(model)]
@@ -920,9 +954,9 @@ def step_roofline(units_by_model, seconds, f_mhz):
                         for m in units_by_model},
            "unit_of_work": "path-step (antithetic pairs share normals)",
            "bound_ms": 1e3 * bound_s, "sm_mhz": f_mhz,
-           "peak_source": ("nominal per-clock SM widths (148 SMs x 128 issue / 16 XU per clk) at "
-                           "the SM clock sampled during the timed region; the measured peaks "
-                           "(HBM copy, bf16 GEMM) do not bound this kernel")}
+           "peak_source": (PIPES["source"] + " at the SM clock sampled during the timed "
+                           "region; the HBM-copy and bf16-GEMM peaks do not bound this kernel"),
+           "pipe_widths_per_sm_clk": {k: PIPES[k] for k in ("issue", "xu", "fp64")}}
     if bound in ("xu", "alu"):
         out["achieved"] = ops / seconds / 1e9
         out["peak"] = peak / 1e9
@@ -1079,7 +1113,7 @@ def bsm_terminal_leg(qk, reps=20, f_mhz=1965.0, cpu=True):
     e2e = (time.perf_counter() - t0) / reps
     paths = int(b["paths"].sum())
     pairs = paths // 2
-    fp64_peak = SMS * FP64_PER_CLK * f_mhz * 1e6
+    fp64_peak = SMS * PIPES["fp64"] * f_mhz * 1e6
     res = {"workload": "64 BSM calls/puts x 131072 paths (terminal GBM, antithetic pairs)",
            "dtype": "f64", "ms": ms, "paths_per_s": paths / (ms / 1e3), "e2e_ms": 1e3 * e2e,
            "e2e_paths_per_s": paths / e2e, "api": "qk_mcm_antithetic_variates_price_batch",
@@ -1090,8 +1124,7 @@ def bsm_terminal_leg(qk, reps=20, f_mhz=1965.0, cpu=True):
                         "frac": pairs * FP64_PER_PAIR / (kern_ms / 1e3) / fp64_peak,
                         "traffic": None, "kernel_ms": kern_ms,
                         "per_unit": {"fp64_ops": FP64_PER_PAIR, "unit": "antithetic pair"},
-                        "peak_source": "nominal 148 SMs x 64 FP64 lanes per clk at the sampled "
-                                       "SM clock"}}
+                        "peak_source": PIPES["source"] + " at the sampled SM clock (FP64 lanes)"}}
     if cpu:
         res["cpu_baseline"] = _rate_baseline(
             "bsm", "paths", "paths/s", 6.0, 3.0,
@@ -1283,6 +1316,15 @@ def profile_plans(qk, which, n_opt):
 
 def main():
     args = parse()
+    if args.pipe_probe:
+        from quantkernel_b200 import QuantKernel
+
+        qk = QuantKernel()
+        runs = [measure_pipes(qk, 0) for _ in range(3)]
+        print(json.dumps({"leg": "pipe_probe", "unit": "lane-operations per SM per SM clock",
+                          "runs": runs, "nominal": {"issue": ISSUE_PER_CLK, "xu": XU_PER_CLK,
+                                                    "fp64": FP64_PER_CLK}}), flush=True)
+        return 0 if all(runs) else 1
     if args.surrogate_train:
         surrogate_train_leg(args)
         return 0

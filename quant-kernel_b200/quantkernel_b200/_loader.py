@@ -108,6 +108,7 @@ FUNCTION_SIGNATURES = [
     ("qk_dist_abort", I32, [VP]),
     ("qk_dist_destroy", I32, [VP]),
     ("qk_dist_partition", I32, [PD, I64, I32, PI64]),
+    ("qk_b200_pipe_probe", I32, [I32, I32, PD]),
     ("qk_mcm_plan_execute_sharded", I32, [VP, VP, VP]),
     ("qk_mcm_plan_shard_bounds", I32, [VP, I32, PI64]),
     ("qk_mcm_plan_execute_tiles", I32, [VP, I64, I64, VP]),

@@ -13,10 +13,11 @@ import pytest
 
 ROOT = Path(__file__).resolve().parents[1]
 HEADER = ROOT / "include" / "qk_api.h"
+HEADERS = sorted((ROOT / "include").glob("*.h"))
 
 
 def _declared_functions():
-    text = HEADER.read_text()
+    text = "".join(h.read_text() for h in HEADERS)
     return sorted(set(re.findall(r"QK_EXPORT\s+[\w\s\*]+?\b(qk_\w+)\s*\(", text)))
 
 
@@ -24,7 +25,7 @@ def test_library_exports_every_declared_symbol(qk):
     names = _declared_functions()
     assert len(names) >= 28
     for name in names:
-        assert hasattr(qk._lib, name), f"{name} declared in qk_api.h but not exported"
+        assert hasattr(qk._lib, name), f"{name} declared in include/ but not exported"
 
 
 def test_loader_binds_every_declared_symbol():

@@ -26,7 +26,8 @@ NOT_PRICING = ("qk_mcm_plan_", "qk_mcm_mixed_", "qk_mcm_heston_monte_carlo_price
 
 
 def _header_funcs():
-    return re.findall(r"QK_EXPORT\s+[\w\s\*]+?\b(qk_\w+)\s*\(", HEADER.read_text())
+    text = "".join(h.read_text() for h in sorted((ROOT / "include").glob("*.h")))
+    return re.findall(r"QK_EXPORT\s+[\w\s\*]+?\b(qk_\w+)\s*\(", text)
 
 
 def _pricing_scalars(funcs):
