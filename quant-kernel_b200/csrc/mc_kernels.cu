@@ -181,70 +181,87 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
         sd2[p] = f2(1.0f);
     }
     const float2 m02 = f2(m0), b2 = f2(b), c2 = f2(c);
+    // One step s of a step block (the block's Box-Muller pair s / 2 is drawn
+    // at even s), packed (units 2p, 2p + 1 as one pair) or scalar.
+    float2 zp2[NP][2];
+    float zp[UPT][2];
+    auto step = [&](const Philox6 (&r)[UPT], int s) {
+        if constexpr (PK) {
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                if ((s & 1) == 0) philox6_pair2(r[2 * p], r[2 * p + 1], s >> 1, zp2[p][0], zp2[p][1]);
+                const float2 zz = zp2[p][s & 1];
+                float2 iu, id;
+                if (MIL) {
+                    iu = fma2(fma2(c2, zz, b2), zz, m02);
+                    id = fma2(fma2(neg2(c2), zz, b2), neg2(zz), m02);
+                } else {
+                    iu = fma2(b2, zz, m02);
+                    id = fma2(neg2(b2), zz, m02);
+                }
+                const float2 u = fma2(su2[p], iu, su2[p]);
+                su2[p] = f2(fmaxf(u.x, fl), fmaxf(u.y, fl));
+                if (ANTI) {
+                    const float2 d = fma2(sd2[p], id, sd2[p]);
+                    sd2[p] = f2(fmaxf(d.x, fl), fmaxf(d.y, fl));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < UPT; ++k) {
+                if ((s & 1) == 0) r[k].pair(s >> 1, zp[k][0], zp[k][1]);
+                const float zz = zp[k][s & 1];
+                float iu, id;
+                if (MIL) {
+                    iu = fma_rn(fma_rn(c, zz, b), zz, m0);
+                    id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
+                } else {
+                    iu = fma_rn(b, zz, m0);
+                    id = fma_rn(-b, zz, m0);
+                }
+                su[k] = fmaxf(fma_rn(su[k], iu, su[k]), fl);
+                if (ANTI) sd[k] = fmaxf(fma_rn(sd[k], id, sd[k]), fl);
+            }
+        }
+    };
+    auto philox_block = [&](Philox6 (&r)[UPT], uint32_t bk) {
+#pragma unroll
+        for (int k = 0; k < UPT; ++k)
+            r[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, bk, 0u, c3, k0, k1);
+    };
     // steps <= kMaxSteps (checked when packing), so j0 + 12 never wraps
     uint32_t blk = 0;  // step block j / 6
-    for (int32_t j0 = 0; j0 < steps; j0 += 6 * SU, blk += SU) {
-        Philox6 rb[SU][UPT];
+    if constexpr (SU == 1) {
+        // whole blocks of six steps with no branch between the steps, then
+        // the steps left (as in the Heston kernel)
+        const int32_t full = steps - steps % 6;
+        int32_t j0 = 0;
+        for (; j0 < full; j0 += 6, ++blk) {
+            Philox6 r[UPT];
+            philox_block(r, blk);
 #pragma unroll
-        for (int sb = 0; sb < SU; ++sb)
+            for (int s = 0; s < 6; ++s) step(r, s);
+        }
+        if (j0 < steps) {
+            Philox6 r[UPT];
+            philox_block(r, blk);
+            const int32_t m = steps - j0;
 #pragma unroll
-            for (int k = 0; k < UPT; ++k)
-                rb[sb][k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk + (uint32_t)sb, 0u, c3,
-                                            k0, k1);
+            for (int s = 0; s < 5; ++s)
+                if (s < m) step(r, s);
+        }
+    } else {
+        for (int32_t j0 = 0; j0 < steps; j0 += 6 * SU, blk += SU) {
+            Philox6 rb[SU][UPT];
 #pragma unroll
-        for (int sb = 0; sb < SU; ++sb) {
-            const int32_t j = j0 + 6 * sb;
-            const Philox6 (&r)[UPT] = rb[sb];
-            const int32_t m = (steps - j) < 6 ? (steps - j) : 6;
-            if constexpr (PK) {
-                float2 zp2[NP][2];
+            for (int sb = 0; sb < SU; ++sb) philox_block(rb[sb], blk + (uint32_t)sb);
 #pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    if (s < m) {
+            for (int sb = 0; sb < SU; ++sb) {
+                const int32_t j = j0 + 6 * sb;
+                const int32_t m = (steps - j) < 6 ? (steps - j) : 6;
 #pragma unroll
-                        for (int p = 0; p < NP; ++p) {
-                            if ((s & 1) == 0)
-                                philox6_pair2(r[2 * p], r[2 * p + 1], s >> 1, zp2[p][0], zp2[p][1]);
-                            const float2 zz = zp2[p][s & 1];
-                            float2 iu, id;
-                            if (MIL) {
-                                iu = fma2(fma2(c2, zz, b2), zz, m02);
-                                id = fma2(fma2(neg2(c2), zz, b2), neg2(zz), m02);
-                            } else {
-                                iu = fma2(b2, zz, m02);
-                                id = fma2(neg2(b2), zz, m02);
-                            }
-                            const float2 u = fma2(su2[p], iu, su2[p]);
-                            su2[p] = f2(fmaxf(u.x, fl), fmaxf(u.y, fl));
-                            if (ANTI) {
-                                const float2 d = fma2(sd2[p], id, sd2[p]);
-                                sd2[p] = f2(fmaxf(d.x, fl), fmaxf(d.y, fl));
-                            }
-                        }
-                    }
-                }
-            } else {
-                float zp[UPT][2];
-#pragma unroll
-                for (int s = 0; s < 6; ++s) {
-                    if (s < m) {
-#pragma unroll
-                        for (int k = 0; k < UPT; ++k) {
-                            if ((s & 1) == 0) r[k].pair(s >> 1, zp[k][0], zp[k][1]);
-                            const float zz = zp[k][s & 1];
-                            float iu, id;
-                            if (MIL) {
-                                iu = fma_rn(fma_rn(c, zz, b), zz, m0);
-                                id = fma_rn(fma_rn(-c, zz, b), -zz, m0);
-                            } else {
-                                iu = fma_rn(b, zz, m0);
-                                id = fma_rn(-b, zz, m0);
-                            }
-                            su[k] = fmaxf(fma_rn(su[k], iu, su[k]), fl);
-                            if (ANTI) sd[k] = fmaxf(fma_rn(sd[k], id, sd[k]), fl);
-                        }
-                    }
-                }
+                for (int s = 0; s < 6; ++s)
+                    if (s < m) step(rb[sb], s);
             }
         }
     }
@@ -341,86 +358,109 @@ __device__ __forceinline__ void sim_heston_form(const McOption& o, uint32_t unit
     }
     const float2 sqdt2 = f2(sqdt), xr2 = f2(xr), xc2 = f2(xc), nhdt2 = f2(-hdt), omk2 = f2(omk),
                  kth2 = f2(kth), cmu2 = f2(cmu);
+    // One step s of a step block: packed (units 2p, 2p + 1 as one pair) or
+    // scalar; `first` marks step 0 of the path (the LR score's normal).
+    auto step = [&](const Philox6 (&r)[UPT], int s, bool first) {
+        if (DF) fl -= cmu;  // the floor of y after this step
+        if constexpr (PK) {
+            const float flo = DF ? fl : xfl;
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                float2 w, c1, s1;
+                philox6_parts2(r[2 * p], r[2 * p + 1], s, w, c1, s1);
+                if (LR && first) {
+                    zfirst[2 * p] = ptx_sqrt(w.x) * c1.x;
+                    zfirst[2 * p + 1] = ptx_sqrt(w.y) * c1.y;
+                }
+                const float2 sz1 = mul2(sqdt2, c1);
+                const float2 xw = fma2(xr2, c1, mul2(xc2, s1));
+                {
+                    const float2 q = mul2(vu2[p], w);
+                    const float2 sv = f2(ptx_sqrt(q.x), ptx_sqrt(q.y));
+                    const float2 x = DF ? fma2(sv, sz1, fma2(nhdt2, vu2[p], xu2[p]))
+                                        : add2(xu2[p], fma2(sv, sz1, fma2(nhdt2, vu2[p], cmu2)));
+                    xu2[p] = f2(ptx_max_nan(x.x, flo), ptx_max_nan(x.y, flo));
+                    const float2 v = fma2(sv, xw, fma2(vu2[p], omk2, kth2));
+                    vu2[p] = f2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
+                }
+                if (ANTI) {
+                    const float2 q = mul2(vd2[p], w);
+                    const float2 sv = f2(ptx_sqrt(q.x), ptx_sqrt(q.y));
+                    const float2 x = DF ? fma2(sv, neg2(sz1), fma2(nhdt2, vd2[p], xd2[p]))
+                                        : add2(xd2[p], fma2(sv, neg2(sz1), fma2(nhdt2, vd2[p], cmu2)));
+                    xd2[p] = f2(ptx_max_nan(x.x, flo), ptx_max_nan(x.y, flo));
+                    const float2 v = fma2(sv, neg2(xw), fma2(vd2[p], omk2, kth2));
+                    vd2[p] = f2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < UPT; ++k) {
+                // z1 = kBmRadius sqrt(w) c, z2 = kBmRadius sqrt(w) s; the
+                // step needs sqrt(v) z1 and sqrt(v) z2 only, so sqrt(w)
+                // joins the variance's square root: sqrt(v w)
+                float w, c1, s1;
+                r[k].parts(s, w, c1, s1);
+                if (LR && first) zfirst[k] = ptx_sqrt(w) * c1;
+                const float sz1 = sqdt * c1;
+                const float xw = fma_rn(xr, c1, xc * s1);
+                {
+                    const float sv = ptx_sqrt(vu[k] * w);
+                    if (DF)
+                        xu[k] = ptx_max_nan(fma_rn(sv, sz1, fma_rn(-hdt, vu[k], xu[k])), fl);
+                    else
+                        xu[k] = ptx_max_nan(xu[k] + fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu)), xfl);
+                    vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
+                }
+                if (ANTI) {
+                    const float sv = ptx_sqrt(vd[k] * w);
+                    if (DF)
+                        xd[k] = ptx_max_nan(fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], xd[k])), fl);
+                    else
+                        xd[k] = ptx_max_nan(xd[k] + fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu)), xfl);
+                    vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
+                }
+            }
+        }
+    };
+    auto philox_block = [&](Philox6 (&r)[UPT], uint32_t b) {
+#pragma unroll
+        for (int k = 0; k < UPT; ++k)
+            r[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, b, 0u, c3, k0, k1);
+    };
     // steps <= kMaxSteps (checked when packing), so j0 + 6 never wraps
     uint32_t blk = 0;  // step block j / 3
-    for (int32_t j0 = 0; j0 < steps; j0 += 3 * SU, blk += SU) {
-        Philox6 rb[SU][UPT];
+    if constexpr (SU == 1) {
+        // whole blocks of three steps with no branch between the steps (so
+        // one step's special-function work can be scheduled among the next
+        // step's arithmetic), then the one or two steps left
+        const int32_t full = steps - steps % 3;
+        int32_t j0 = 0;
+        for (; j0 < full; j0 += 3, ++blk) {
+            Philox6 r[UPT];
+            philox_block(r, blk);
+            step(r, 0, j0 == 0);
+            step(r, 1, false);
+            step(r, 2, false);
+        }
+        if (j0 < steps) {
+            Philox6 r[UPT];
+            philox_block(r, blk);
+            step(r, 0, j0 == 0);
+            if (j0 + 1 < steps) step(r, 1, false);
+        }
+    } else {
+        for (int32_t j0 = 0; j0 < steps; j0 += 3 * SU, blk += SU) {
+            Philox6 rb[SU][UPT];
 #pragma unroll
-        for (int sb = 0; sb < SU; ++sb)
+            for (int sb = 0; sb < SU; ++sb) philox_block(rb[sb], blk + (uint32_t)sb);
 #pragma unroll
-            for (int k = 0; k < UPT; ++k)
-                rb[sb][k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk + (uint32_t)sb, 0u, c3,
-                                            k0, k1);
+            for (int sb = 0; sb < SU; ++sb) {
+                const int32_t j = j0 + 3 * sb;
+                const int32_t m = (steps - j) < 3 ? (steps - j) : 3;
 #pragma unroll
-        for (int sb = 0; sb < SU; ++sb) {
-            const int32_t j = j0 + 3 * sb;
-            const Philox6 (&r)[UPT] = rb[sb];
-            const int32_t m = (steps - j) < 3 ? (steps - j) : 3;
-#pragma unroll
-            for (int s = 0; s < 3; ++s) {
-                if (s < m) {
-                    if (DF) fl -= cmu;  // the floor of y after this step
-                    if constexpr (PK) {
-                        const float flo = DF ? fl : xfl;
-#pragma unroll
-                        for (int p = 0; p < NP; ++p) {
-                            float2 w, c1, s1;
-                            philox6_parts2(r[2 * p], r[2 * p + 1], s, w, c1, s1);
-                            if (LR && j == 0 && s == 0) {
-                                zfirst[2 * p] = ptx_sqrt(w.x) * c1.x;
-                                zfirst[2 * p + 1] = ptx_sqrt(w.y) * c1.y;
-                            }
-                            const float2 sz1 = mul2(sqdt2, c1);
-                            const float2 xw = fma2(xr2, c1, mul2(xc2, s1));
-                            {
-                                const float2 q = mul2(vu2[p], w);
-                                const float2 sv = f2(ptx_sqrt(q.x), ptx_sqrt(q.y));
-                                const float2 x = DF ? fma2(sv, sz1, fma2(nhdt2, vu2[p], xu2[p]))
-                                                    : add2(xu2[p], fma2(sv, sz1, fma2(nhdt2, vu2[p], cmu2)));
-                                xu2[p] = f2(ptx_max_nan(x.x, flo), ptx_max_nan(x.y, flo));
-                                const float2 v = fma2(sv, xw, fma2(vu2[p], omk2, kth2));
-                                vu2[p] = f2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
-                            }
-                            if (ANTI) {
-                                const float2 q = mul2(vd2[p], w);
-                                const float2 sv = f2(ptx_sqrt(q.x), ptx_sqrt(q.y));
-                                const float2 x = DF ? fma2(sv, neg2(sz1), fma2(nhdt2, vd2[p], xd2[p]))
-                                                    : add2(xd2[p], fma2(sv, neg2(sz1), fma2(nhdt2, vd2[p], cmu2)));
-                                xd2[p] = f2(ptx_max_nan(x.x, flo), ptx_max_nan(x.y, flo));
-                                const float2 v = fma2(sv, neg2(xw), fma2(vd2[p], omk2, kth2));
-                                vd2[p] = f2(fmaxf(v.x, 0.0f), fmaxf(v.y, 0.0f));
-                            }
-                        }
-                    } else {
-#pragma unroll
-                        for (int k = 0; k < UPT; ++k) {
-                            // z1 = kBmRadius sqrt(w) c, z2 = kBmRadius sqrt(w) s; the
-                            // step needs sqrt(v) z1 and sqrt(v) z2 only, so sqrt(w)
-                            // joins the variance's square root: sqrt(v w)
-                            float w, c1, s1;
-                            r[k].parts(s, w, c1, s1);
-                            if (LR && j == 0 && s == 0) zfirst[k] = ptx_sqrt(w) * c1;
-                            const float sz1 = sqdt * c1;
-                            const float xw = fma_rn(xr, c1, xc * s1);
-                            {
-                                const float sv = ptx_sqrt(vu[k] * w);
-                                if (DF)
-                                    xu[k] = ptx_max_nan(fma_rn(sv, sz1, fma_rn(-hdt, vu[k], xu[k])), fl);
-                                else
-                                    xu[k] = ptx_max_nan(xu[k] + fma_rn(sv, sz1, fma_rn(-hdt, vu[k], cmu)), xfl);
-                                vu[k] = fmaxf(fma_rn(sv, xw, fma_rn(vu[k], omk, kth)), 0.0f);
-                            }
-                            if (ANTI) {
-                                const float sv = ptx_sqrt(vd[k] * w);
-                                if (DF)
-                                    xd[k] = ptx_max_nan(fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], xd[k])), fl);
-                                else
-                                    xd[k] = ptx_max_nan(xd[k] + fma_rn(sv, -sz1, fma_rn(-hdt, vd[k], cmu)), xfl);
-                                vd[k] = fmaxf(fma_rn(sv, -xw, fma_rn(vd[k], omk, kth)), 0.0f);
-                            }
-                        }
-                    }
-                }
+                for (int s = 0; s < 3; ++s)
+                    if (s < m) step(rb[sb], s, j == 0 && s == 0);
             }
         }
     }
