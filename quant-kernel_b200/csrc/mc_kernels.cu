@@ -785,10 +785,11 @@ __device__ __noinline__ int64_t run_group(const McOption* __restrict__ opts,
     }
 }
 
-// Seven 128-thread CTAs per SM (72 registers): every family body is compiled
-// within that budget; six (80 registers) and eight (64) measured slower.
+// Eight 128-thread CTAs per SM (64 registers): every family body is compiled
+// within that budget; five, six and seven CTAs per SM measured slower on the
+// mixed benchmark batch (52.1, 51.7, 51.2 vs 51.0 ms).
 template <int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 896 / BLOCK)
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK)
     mc_persistent_kernel(const McOption* __restrict__ opts, const int64_t* __restrict__ tile_begin,
                          int64_t n_tiles, TilePartial* __restrict__ partials,
                          unsigned long long* __restrict__ work_counter,

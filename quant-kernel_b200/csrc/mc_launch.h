@@ -22,10 +22,9 @@ enum : int {
 
 // Units per thread compiled into the persistent mixed-model kernel (and used
 // by the per-family grids of a mixed plan).  The stepwise families take four:
-// with the persistent kernel's 72-register budget (seven 128-thread CTAs per
-// SM) the mixed benchmark batch took 52.9 ms, against 53.5 ms at six CTAs per
-// SM and 56.1 ms with two stepwise units per thread; Heston keeps two, whose
-// four-unit body needs 93 registers.
+// the mixed benchmark batch ran 52.9 ms with four (persistent kernel, seven
+// CTAs per SM) against 56.1 ms with two stepwise units per thread; Heston
+// keeps two, whose four-unit body needs 79-93 registers.
 // Results do not depend on these (tile sums are exact double-double sums
 // merged in a fixed order).
 constexpr int kUptTerminal = 1;
