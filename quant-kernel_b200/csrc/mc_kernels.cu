@@ -232,19 +232,24 @@ __device__ __forceinline__ void sim_stepwise(const McOption& o, uint32_t unit0, 
     // steps <= kMaxSteps (checked when packing), so j0 + 12 never wraps
     uint32_t blk = 0;  // step block j / 6
     if constexpr (SU == 1) {
-        // whole blocks of six steps with no branch between the steps, then
-        // the steps left (as in the Heston kernel)
+        // whole blocks of six steps with no branch between the steps and the
+        // next block's Philox call after the first step, then the steps
+        // left (as in the Heston kernel)
         const int32_t full = steps - steps % 6;
         int32_t j0 = 0;
+        Philox6 r[UPT];
+        philox_block(r, 0u);
+#pragma unroll 2
         for (; j0 < full; j0 += 6, ++blk) {
-            Philox6 r[UPT];
-            philox_block(r, blk);
+            Philox6 nx[UPT];
+            step(r, 0);
+            philox_block(nx, blk + 1u);
 #pragma unroll
-            for (int s = 0; s < 6; ++s) step(r, s);
+            for (int s = 1; s < 6; ++s) step(r, s);
+#pragma unroll
+            for (int k = 0; k < UPT; ++k) r[k] = nx[k];
         }
         if (j0 < steps) {
-            Philox6 r[UPT];
-            philox_block(r, blk);
             const int32_t m = steps - j0;
 #pragma unroll
             for (int s = 0; s < 5; ++s)
@@ -433,19 +438,26 @@ __device__ __forceinline__ void sim_heston_form(const McOption& o, uint32_t unit
     if constexpr (SU == 1) {
         // whole blocks of three steps with no branch between the steps (so
         // one step's special-function work can be scheduled among the next
-        // step's arithmetic), then the one or two steps left
+        // step's arithmetic), then the one or two steps left.  The next
+        // block's Philox call is issued after the block's first step, so its
+        // integer work interleaves with the other steps' special-function
+        // work (the same words: the same bits); the loop is unrolled twice
+        // so that the two sets of words swap without copies.
         const int32_t full = steps - steps % 3;
         int32_t j0 = 0;
+        Philox6 r[UPT];
+        philox_block(r, 0u);
+#pragma unroll 2
         for (; j0 < full; j0 += 3, ++blk) {
-            Philox6 r[UPT];
-            philox_block(r, blk);
+            Philox6 nx[UPT];
             step(r, 0, j0 == 0);
+            philox_block(nx, blk + 1u);
             step(r, 1, false);
             step(r, 2, false);
+#pragma unroll
+            for (int k = 0; k < UPT; ++k) r[k] = nx[k];
         }
         if (j0 < steps) {
-            Philox6 r[UPT];
-            philox_block(r, blk);
             step(r, 0, j0 == 0);
             if (j0 + 1 < steps) step(r, 1, false);
         }
