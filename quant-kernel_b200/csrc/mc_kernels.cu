@@ -439,10 +439,11 @@ __device__ __forceinline__ void sim_heston_form(const McOption& o, uint32_t unit
         // whole blocks of three steps with no branch between the steps (so
         // one step's special-function work can be scheduled among the next
         // step's arithmetic), then the one or two steps left.  The next
-        // block's Philox call is issued after the block's first step, so its
-        // integer work interleaves with the other steps' special-function
-        // work (the same words: the same bits); the loop is unrolled twice
-        // so that the two sets of words swap without copies.
+        // block's Philox calls are issued inside the block -- the first half
+        // of the units' after the block's first step, the rest after its
+        // second -- so their integer work interleaves with the steps'
+        // special-function work (the same words: the same bits); the loop is
+        // unrolled twice so that the two sets of words swap without copies.
         const int32_t full = steps - steps % 3;
         int32_t j0 = 0;
         Philox6 r[UPT];
@@ -451,8 +452,13 @@ __device__ __forceinline__ void sim_heston_form(const McOption& o, uint32_t unit
         for (; j0 < full; j0 += 3, ++blk) {
             Philox6 nx[UPT];
             step(r, 0, j0 == 0);
-            philox_block(nx, blk + 1u);
+#pragma unroll
+            for (int k = 0; k < UPT / 2; ++k)
+                nx[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk + 1u, 0u, c3, k0, k1);
             step(r, 1, false);
+#pragma unroll
+            for (int k = UPT / 2; k < UPT; ++k)
+                nx[k].x = philox4x32_10(unit0 + (uint32_t)k * stride, blk + 1u, 0u, c3, k0, k1);
             step(r, 2, false);
 #pragma unroll
             for (int k = 0; k < UPT; ++k) r[k] = nx[k];
