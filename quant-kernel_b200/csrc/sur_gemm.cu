@@ -66,6 +66,14 @@ __device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
            (static_cast<uint64_t>(2) << 61);
 }
 
+// The same for 32-byte rows (K = 16 bf16): 32-byte swizzle, 8-row groups 256
+// B apart, layout type 6 (SWIZZLE_32B).
+__device__ __forceinline__ uint64_t desc_sw32(uint32_t addr) {
+    return static_cast<uint64_t>((addr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(1) << 16) |
+           (static_cast<uint64_t>(256 >> 4) << 32) | (static_cast<uint64_t>(1) << 46) |
+           (static_cast<uint64_t>(6) << 61);
+}
+
 // Instruction descriptor, kind::f16: D fp32, A and B bf16, both K-major,
 // N >> 3 at bit 17, M >> 4 at bit 24.
 template <int BN>
@@ -419,16 +427,21 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 // layer 1's and layer 2's activations.  While the epilogue warps work on one
 // slot's layer, the tensor core computes the other slot's, so neither waits
 // for the other's tail.  Four warp roles:
-//   warp 16 (one lane)  weight producer: the 32 KiB weight k-blocks in the
-//                       order the MMA issuer takes them (per tile pair: W1 for
-//                       A, W1 for B, W2[0..3] for A, for B, W3[0..3] for A,
-//                       for B) through a 2-slot ring;
+//   warp 16 (one lane)  weight producer: W1's first 16 columns once (8 KiB,
+//                       resident), then the 32 KiB k-blocks of W2 and W3 in
+//                       the order the MMA issuer takes them (per tile pair:
+//                       W2[0..3] for A, for B, W3[0..3] for A, for B) through
+//                       a 2-slot ring;
 //   warp 17 (one lane)  MMA issuer: per tile pair, layer by layer, tile A's
-//                       then tile B's: layer 1 (K = 64) once the slot's input
-//                       rows have landed and its previous tile's head has
-//                       read the accumulator, layers 2 and 3 once the
-//                       epilogue has written the slot's previous layer;
-//   warp 18 (one lane)  input loader: a slot's next input rows once the MMAs
+//                       then tile B's: layer 1 (one K = 16 MMA: the 9
+//                       features and their zero padding; the rows' columns
+//                       16..63 are zeros too and would add exact zeros) once
+//                       the slot's input rows have landed and its previous
+//                       tile's head has read the accumulator, layers 2 and 3
+//                       once the epilogue has written the slot's previous
+//                       layer;
+//   warp 18 (one lane)  input loader: a slot's next input rows (their first
+//                       16 columns, 32-byte swizzled: 4 KiB) once the MMAs
 //                       of its previous tile's layer 3 (the last reader of
 //                       the slot's buffer) have completed;
 //   warps 0-15          epilogue, in the MMA issuer's order: warp w reads TMEM
@@ -455,7 +468,11 @@ constexpr int kIWSlots = 2;
 constexpr uint32_t kWBlock = 256 * kBK * 2;        // 32 KiB: 256 rows x 64 bf16
 constexpr uint32_t kHBytes = 4 * kABytes;          // 64 KiB: 128 rows x 256 bf16
 constexpr int kTileSlots = 2;
-constexpr size_t kInferSmem = kTileSlots * kHBytes + kIWSlots * kWBlock + 1024;
+// Layer 1 reads only K = 16 (the 9 features and their zero padding): input
+// rows of 32 bytes, and W1's first 16 columns held resident for the launch.
+constexpr uint32_t kXBytes = kBM * 16 * 2;         // 4 KiB: 128 rows x 16 bf16
+constexpr uint32_t kW1Bytes = 256 * 16 * 2;        // 8 KiB: 256 rows x 16 bf16
+constexpr size_t kInferSmem = kTileSlots * kHBytes + kIWSlots * kWBlock + kW1Bytes + 1024;
 constexpr int kInferEpiWarps = 16;                 // 4 per TMEM lane quarter
 constexpr int kInferThreads = (kInferEpiWarps + 3) * 32;
 constexpr int kProducerWarp = kInferEpiWarps, kMmaWarp = kInferEpiWarps + 1,
@@ -501,6 +518,8 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                                                ~static_cast<uintptr_t>(1023));
     uint8_t* hbufs = smem;  // [kTileSlots][kHBytes]: a slot's input rows, then its activations
     uint8_t* wbuf = smem + kTileSlots * kHBytes;
+    uint8_t* w1s = wbuf + kIWSlots * kWBlock;  // W1 [256][16], resident
+    __shared__ __align__(8) uint64_t w1full;
     __shared__ __align__(8) uint64_t xfull[kTileSlots], slotfree[kTileSlots], accfull[kTileSlots];
     __shared__ __align__(8) uint64_t hdone[kTileSlots], pready[kTileSlots];
     __shared__ __align__(8) uint64_t wfull[kIWSlots], wempty[kIWSlots], drain;
@@ -535,6 +554,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
             mbar_init(smem_u32(&wempty[s]), 1);
         }
         mbar_init(smem_u32(&drain), 1);
+        mbar_init(smem_u32(&w1full), 1);
         abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -557,6 +577,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
     // bookkeeping for the teardown drain
     int last_round[kIWSlots] = {-1, -1};
     int64_t x_last[kTileSlots] = {-1, -1};
+    bool w1_issued = false;
 
     if (warp == kProducerWarp) {
         if (lane == 0) {
@@ -570,12 +591,16 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 ++wl;
                 return true;
             };
+            if (my_tiles > 0) {  // W1's first 16 columns, once
+                mbar_expect_tx(smem_u32(&w1full), kW1Bytes);
+                tma_load_2d(smem_u32(w1s), &tw1, 0, 0, smem_u32(&w1full));
+                w1_issued = true;
+            }
             for (int64_t i0 = 0; i0 < my_tiles; i0 += 2) {
                 if (abort_flag) break;
                 const int nt = (my_tiles - i0) >= 2 ? 2 : 1;
-                // the MMA issuer's order: each layer for tile A, then tile B
+                // the MMA issuer's order: layers 2 and 3 for tile A, then tile B
                 bool ok = true;
-                for (int k = 0; ok && k < nt; ++k) ok = load_w(&tw1, 0);
                 for (int k = 0; ok && k < nt; ++k)
                     for (int kb = 0; ok && kb < 4; ++kb) ok = load_w(&tw2, kb * kBK);
                 for (int k = 0; ok && k < nt; ++k)
@@ -598,7 +623,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                     fail(21);
                     break;
                 }
-                mbar_expect_tx(smem_u32(&xfull[s]), kABytes);
+                mbar_expect_tx(smem_u32(&xfull[s]), kXBytes);
                 const int64_t t = blockIdx.x + i * gridDim.x;
                 tma_load_2d(smem_u32(hbufs + s * kHBytes), &tx, 0, static_cast<int>(t * kBM),
                             smem_u32(&xfull[s]));
@@ -623,7 +648,9 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                 ++wc;
                 return true;
             };
-            bool ok = true;
+            bool ok = my_tiles == 0 || mbar_wait(smem_u32(&w1full), 0u);
+            if (!ok) fail(25);
+            const uint64_t dw1 = desc_sw32(smem_u32(w1s));
             for (int64_t i0 = 0; ok && i0 < my_tiles; i0 += 2) {
                 if (abort_flag) break;
                 const int nt = (my_tiles - i0) >= 2 ? 2 : 1;
@@ -639,7 +666,8 @@ __global__ void __launch_bounds__(kInferThreads, 1)
                             if (ok && u > 0)
                                 ok = mbar_wait(smem_u32(&hdone[s]), static_cast<uint32_t>((3 * u - 1) & 1));
                             fence_after();
-                            if (ok) ok = mma_kblock(acc, smem_u32(hb), true);  // K = 64
+                            // K = 16: the input rows and the resident W1 slice
+                            if (ok) umma_bf16(acc, desc_sw32(smem_u32(hb)), dw1, idesc, 0u);
                         } else {
                             // layer l's activations written (and its
                             // accumulator read) by every epilogue warp
@@ -761,6 +789,7 @@ __global__ void __launch_bounds__(kInferThreads, 1)
         if (warp == kProducerWarp && lane == 0) {
             for (int s = 0; s < kIWSlots; ++s)
                 if (last_round[s] >= 0) mbar_wait(smem_u32(&wfull[s]), last_round[s] & 1);
+            if (w1_issued) mbar_wait(smem_u32(&w1full), 0u);
         } else if (warp == kXWarp && lane == 0) {
             for (int s = 0; s < kTileSlots; ++s)
                 if (x_last[s] >= 0) mbar_wait(smem_u32(&xfull[s]), static_cast<uint32_t>(x_last[s] & 1));
@@ -834,6 +863,30 @@ bool make_tmap_bf16(CUtensorMap* map, const void* base, uint64_t rows, uint64_t 
     const cuuint32_t estr[2] = {1, 1};
     return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+bool make_tmap_bf16_k16(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
+                        uint32_t box_rows) {
+    if (!make_tmap_bf16(map, base, rows, cols, box_rows)) return false;  // also loads the encoder
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!encode || box_rows == 0 || box_rows > 256) return false;
+    // 16 bf16 = 32 bytes: the inner box equals the 32-byte swizzle span
+    const cuuint64_t dims[2] = {cols, rows};
+    const cuuint64_t strides[1] = {cols * 2};
+    const cuuint32_t box[2] = {16, box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 

@@ -66,14 +66,19 @@ struct InferArgs {
     float* y;                // [n]
     int* err;                // error word (0 = ok)
 };
-// tx: x [n][64] (box 64 x 128); tw1: W1 [256][64]; tw2, tw3: [256][256]
-// (boxes 64 x 256).  ctas: persistent grid size (one CTA per SM).
+// tx: x [n][64] and tw1: W1 [256][64] read through their first 16 columns
+// (make_tmap_bf16_k16: the 9 features and their zero padding; boxes 16 x 128
+// and 16 x 256, 32-byte swizzle); tw2, tw3: [256][256] (boxes 64 x 256).
+// ctas: persistent grid size (one CTA per SM).
 cudaError_t launch_mlp_infer(const CUtensorMap& tx, const CUtensorMap& tw1, const CUtensorMap& tw2,
                              const CUtensorMap& tw3, const InferArgs& a, int ctas, cudaStream_t st);
 
 // Host side: tensor maps over bf16 row-major [rows][cols] (cols contiguous).
 bool make_tmap_bf16(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
                     uint32_t box_rows);
+// The same over columns 0..15 only (a 16 x box_rows box, 32-byte swizzle).
+bool make_tmap_bf16_k16(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
+                        uint32_t box_rows);
 cudaError_t launch_umma_gemm(int epi, int bn, const CUtensorMap& ta, const CUtensorMap& tb,
                              const GemmArgs& a, int splits, cudaStream_t st);
 

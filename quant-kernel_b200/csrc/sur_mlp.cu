@@ -631,7 +631,8 @@ cudaError_t SurModel::predict_device(const __nv_bfloat16* x, const float* base, 
         if (sm_count_ <= 0)
             QK_TRY(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device_));
         CUtensorMap tx, tw1, tw2, tw3;
-        if (!(tmap(&tx, x, n, kSurInPad, 128) && tmap(&tw1, W1b_, kSurHid, kSurInPad, 256) &&
+        if (!(make_tmap_bf16_k16(&tx, x, static_cast<uint64_t>(n), kSurInPad, 128) &&
+              make_tmap_bf16_k16(&tw1, W1b_, kSurHid, kSurInPad, 256) &&
               tmap(&tw2, W2b_, kSurHid, kSurHid, 256) && tmap(&tw3, W3b_, kSurHid, kSurHid, 256)))
             return cudaErrorInvalidValue;
         InferArgs ia{};
