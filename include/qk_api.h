@@ -487,7 +487,9 @@ QK_EXPORT int32_t qk_sur_heston_train(qk_sur_model* model, int32_t epochs, int32
 QK_EXPORT int32_t qk_sur_heston_predict(qk_sur_model* model, const double* features, int64_t n,
                                         double* out);
 /* Device-resident inference: x_rows = normalised bf16 rows [n][64] (DEVICE,
- * 16-byte aligned), base = the rows' base (DEVICE, fp32; NULL only for a
+ * 16-byte aligned) as qk_sur_heston_features(_device) writes them: the nine
+ * features in columns 0..8 and zeros in columns 9..63 (this call reads
+ * columns 0..15 only), base = the rows' base (DEVICE, fp32; NULL only for a
  * model loaded from a checkpoint without a base), y = price / S (DEVICE,
  * fp32); asynchronous on `stream` (NULL = model's). */
 QK_EXPORT int32_t qk_sur_heston_predict_device(qk_sur_model* model, const void* x_rows,

@@ -90,7 +90,9 @@ class HestonSurrogate:
         return out
 
     def predict_device(self, x_rows_ptr, base_ptr, n, y_ptr, stream=0, layered=False):
-        """Device rows and base in, device price/S out.  The fused kernel by
+        """Device rows and base in, device price/S out.  The rows are
+        features()/features_device() rows: features in columns 0..8, zeros
+        in 9..63 (the fused kernel reads columns 0..15).  The fused kernel by
         default; layered=True runs the layer-by-layer GEMMs it is tested
         against."""
         fn = (self.lib.qk_sur_heston_predict_device_layered if layered
